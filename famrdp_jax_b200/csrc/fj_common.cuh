@@ -1,0 +1,129 @@
+// fj_common.cuh -- shared host/device plumbing of libfamrdp_cuda.so: the
+// context, status handling and launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+
+#include "famrdp_cuda.h"
+
+struct fj_ctx {
+  int device = 0;
+  void* ws = nullptr;        // scratch owned by the context (stage buffers, fluxes)
+  size_t ws_bytes = 0;
+  void* red = nullptr;       // small reduction scratch (partials + counters)
+  size_t red_bytes = 0;
+  std::string last_error;
+  int64_t launches = 0;      // kernels launched through this context
+};
+
+namespace fj {
+
+constexpr int kThreads = 256;
+
+inline int set_err(fj_ctx* ctx, int status, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return status;
+}
+
+inline int cuda_status(fj_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return FJ_OK;
+  if (ctx) ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return FJ_ERR_CUDA;
+}
+
+// Status of the last launch (cudaGetLastError clears the sticky-free error).
+inline int launch_status(fj_ctx* ctx, const char* what) {
+  return cuda_status(ctx, cudaGetLastError(), what);
+}
+
+inline int grid_for(int64_t n, int threads = kThreads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > (1LL << 30)) b = (1LL << 30);
+  return (int)b;
+}
+
+// Grows the context's scratch to at least `bytes` (contents not preserved).
+inline int ensure_ws(fj_ctx* ctx, size_t bytes) {
+  if (ctx->ws_bytes >= bytes) return FJ_OK;
+  if (ctx->ws) {
+    cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&ctx->ws, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, FJ_ERR_NO_MEMORY,
+                   "scratch allocation of " + std::to_string(bytes) + " bytes failed: " +
+                       cudaGetErrorString(e));
+  }
+  ctx->ws_bytes = bytes;
+  return FJ_OK;
+}
+
+inline int ensure_red(fj_ctx* ctx, size_t bytes) {
+  if (ctx->red_bytes >= bytes) return FJ_OK;
+  if (ctx->red) {
+    cudaFree(ctx->red);
+    ctx->red = nullptr;
+    ctx->red_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&ctx->red, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, FJ_ERR_NO_MEMORY, "reduction scratch allocation failed");
+  }
+  ctx->red_bytes = bytes;
+  return FJ_OK;
+}
+
+inline int check_params(fj_ctx* ctx, const fj_params* p) {
+  if (!p) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "params is NULL");
+  if (p->ghost != 2)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "the kernels require ghost == 2");
+  if (p->limiter != FJ_LIM_MINMOD && p->limiter != FJ_LIM_VANLEER)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown limiter");
+  if (p->visc_law != FJ_VISC_SUTHERLAND && p->visc_law != FJ_VISC_CONSTANT)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown viscosity law");
+  if (p->precision != FJ_PREC_F64 && p->precision != FJ_PREC_F32FLUX)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown precision");
+  return FJ_OK;
+}
+
+inline int check_dims(fj_ctx* ctx, int ni, int nj, int nk) {
+  // The widest stencil (MUSCL + face difference) needs 5 cells per axis.
+  if (ni < 5 || nj < 5 || nk < 5)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "every padded extent must be >= 5");
+  if ((int64_t)ni * nj * nk > (int64_t)INT32_MAX / 9)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "block too large for 32-bit cell indexing");
+  return FJ_OK;
+}
+
+// Physics constants passed by value to kernels.
+struct Phys {
+  double gm1, eps_entropy, R, mu0, T0, Ts, cp, Pr;
+  int limiter, visc_law;
+};
+
+inline Phys make_phys(const fj_params* p) {
+  Phys f;
+  f.gm1 = p->gamma - 1.0;
+  f.eps_entropy = p->eps_entropy;
+  f.R = p->R;
+  f.mu0 = p->mu0;
+  f.T0 = p->T0;
+  f.Ts = p->Ts;
+  // kappa = cp * mu / Pr with cp = gamma R / (gamma - 1) (rhs/viscous.py:38-39)
+  f.cp = p->gamma * p->R / (p->gamma - 1.0);
+  f.Pr = p->Pr;
+  f.limiter = p->limiter;
+  f.visc_law = p->visc_law;
+  return f;
+}
+
+}  // namespace fj

@@ -1,0 +1,320 @@
+// fj_halo.cu -- inter-block halo fill (mesh/halo.py:36-92) and physical
+// boundary conditions (physics/bc/*.py), in place on the blocks' q arrays.
+//
+// Halo semantics kept from the reference:
+//   * every CUT1TO1 link copies the source block's 2-layer slab next to the
+//     source face ([g, 2g) or [n-2g, n-g) along its axis, FULL extent along the
+//     other two axes) into the target's ghost slab ([0, g) or [n-g, n) along
+//     the target face's axis, full extent along the others), element by
+//     element in array order (mesh/halo.py:36-53);
+//   * all sources are read from the PRE-exchange arrays (mesh/halo.py:89-90):
+//     one kernel gathers every source slab into scratch before any target is
+//     written;
+//   * links apply in list order, so where two target slabs overlap (edges and
+//     corners) the later link wins: the scatter kernel skips a cell that a
+//     later link of the same target block also writes.
+// Boundary conditions run after the halo, one launch per face in Face enum
+// order (physics/bc/dispatch.py:15), each launch covering that face of every
+// block (blocks are independent).
+#include <vector>
+
+#include "fj_common.cuh"
+#include "fj_rhs.cuh"
+
+namespace fj {
+
+namespace {
+
+constexpr int kMaxLinksPerLaunch = 128;
+constexpr int kMaxBcPerLaunch = 128;
+
+struct HaloDesc {
+  double* tgt;
+  const double* src;
+  long long off;   // slab offset in scratch (doubles)
+  int tn[3], sn[3];
+  int tlo[3], slo[3], ext[3];
+  int tgt_block;
+};
+
+struct HaloTable {
+  int n;
+  HaloDesc d[kMaxLinksPerLaunch];
+};
+
+struct BcDesc {
+  double* q;
+  double qinf[5];
+  double T_wall;
+  int n[3];
+  int face, type, iso;
+};
+
+struct BcTable {
+  int n;
+  double gamma, R;
+  BcDesc d[kMaxBcPerLaunch];
+};
+
+__device__ __forceinline__ int64_t cell_index(const int n[3], int i, int j, int k) {
+  return ((int64_t)i * n[1] + j) * n[2] + k;
+}
+
+__global__ void k_halo_gather(const HaloTable tab, double* __restrict__ scratch) {
+  const HaloDesc& d = tab.d[blockIdx.y];
+  const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
+  const int64_t NS = (int64_t)d.sn[0] * d.sn[1] * d.sn[2];
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 5 * V;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int v = (int)(t / V);
+    const int64_t r = t - v * V;
+    const int c = (int)(r % d.ext[2]);
+    const int b = (int)((r / d.ext[2]) % d.ext[1]);
+    const int a = (int)(r / ((int64_t)d.ext[2] * d.ext[1]));
+    scratch[d.off + t] =
+        d.src[v * NS + cell_index(d.sn, d.slo[0] + a, d.slo[1] + b, d.slo[2] + c)];
+  }
+}
+
+__global__ void k_halo_scatter(const HaloTable tab, const double* __restrict__ scratch) {
+  const int L = blockIdx.y;
+  const HaloDesc& d = tab.d[L];
+  const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
+  const int64_t NT = (int64_t)d.tn[0] * d.tn[1] * d.tn[2];
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < V;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(r % d.ext[2]);
+    const int b = (int)((r / d.ext[2]) % d.ext[1]);
+    const int a = (int)(r / ((int64_t)d.ext[2] * d.ext[1]));
+    const int ti = d.tlo[0] + a, tj = d.tlo[1] + b, tk = d.tlo[2] + c;
+    bool later = false;
+    for (int L2 = L + 1; L2 < tab.n; ++L2) {
+      const HaloDesc& e = tab.d[L2];
+      if (e.tgt_block != d.tgt_block) continue;
+      if (ti >= e.tlo[0] && ti < e.tlo[0] + e.ext[0] && tj >= e.tlo[1] &&
+          tj < e.tlo[1] + e.ext[1] && tk >= e.tlo[2] && tk < e.tlo[2] + e.ext[2]) {
+        later = true;
+        break;
+      }
+    }
+    if (later) continue;
+    const int64_t tc = cell_index(d.tn, ti, tj, tk);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) d.tgt[v * NT + tc] = scratch[d.off + v * V + r];
+  }
+}
+
+// physics/bc/base.py:15-27 ghost_indices: outer layer o (0..g-1 counted from
+// the face) pairs with the mirrored inner layer.
+__device__ __forceinline__ void bc_layers(int face, int n, int g, int o, int& outer,
+                                          int& inner) {
+  if ((face & 1) == 0) {
+    outer = o;
+    inner = 2 * g - 1 - o;
+  } else {
+    outer = n - 1 - o;
+    inner = n - 2 * g + o;
+  }
+}
+
+__global__ void k_bc(const BcTable tab, int g) {
+  const BcDesc& d = tab.d[blockIdx.y];
+  const int ax = d.face >> 1;
+  const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;  // the two other axes
+  const int64_t NT = (int64_t)d.n[0] * d.n[1] * d.n[2];
+  const int64_t V = (int64_t)g * d.n[oa] * d.n[ob];
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < V;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(r % d.n[ob]);
+    const int x = (int)((r / d.n[ob]) % d.n[oa]);
+    const int o = (int)(r / ((int64_t)d.n[ob] * d.n[oa]));
+    int outer, inner;
+    bc_layers(d.face, d.n[ax], g, o, outer, inner);
+    int io[3], ii[3];
+    io[ax] = outer; ii[ax] = inner;
+    io[oa] = x; ii[oa] = x;
+    io[ob] = y; ii[ob] = y;
+    const int64_t co = cell_index(d.n, io[0], io[1], io[2]);
+    const int64_t ci = cell_index(d.n, ii[0], ii[1], ii[2]);
+    if (d.type == FJ_BC_FARFIELD) {  // physics/bc/farfield.py:7-21
+#pragma unroll
+      for (int v = 0; v < 5; ++v) d.q[v * NT + co] = d.qinf[v];
+    } else if (d.type == FJ_BC_WALL && d.iso) {  // physics/bc/wall.py:32-55
+      const double r0 = d.q[ci], r1 = d.q[NT + ci], r2 = d.q[2 * NT + ci],
+                   r3 = d.q[3 * NT + ci], r4 = d.q[4 * NT + ci];
+      const double gm1 = tab.gamma - 1.0;
+      const double ke_i = 0.5 * (r1 * r1 + r2 * r2 + r3 * r3) / r0;
+      const double p_g = gm1 * (r4 - ke_i);
+      const double rho_g = p_g / (tab.R * d.T_wall);
+      const double scale = rho_g / r0;
+      const double u_g = -r1 * scale, v_g = -r2 * scale, w_g = -r3 * scale;
+      const double ke_g = 0.5 * (u_g * u_g + v_g * v_g + w_g * w_g) / rho_g;
+      d.q[co] = rho_g;
+      d.q[NT + co] = u_g;
+      d.q[2 * NT + co] = v_g;
+      d.q[3 * NT + co] = w_g;
+      d.q[4 * NT + co] = p_g / gm1 + ke_g;
+    } else {  // mirror: adiabatic wall (wall.py:27-29) or symmetry (symmetry.py:8-11)
+      double s[5] = {1.0, 1.0, 1.0, 1.0, 1.0};
+      if (d.type == FJ_BC_WALL) {
+        s[1] = s[2] = s[3] = -1.0;
+      } else {
+        s[1 + ax] = -1.0;
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v) d.q[v * NT + co] = d.q[v * NT + ci] * s[v];
+    }
+  }
+}
+
+bool face_box(int face, const int n[3], int g, bool source, int lo[3], int ext[3]) {
+  if (face < 0 || face > 5) return false;
+  const int ax = face >> 1;
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = 0;
+    ext[a] = n[a];
+  }
+  ext[ax] = g;
+  if (source)
+    lo[ax] = (face & 1) == 0 ? g : n[ax] - 2 * g;
+  else
+    lo[ax] = (face & 1) == 0 ? 0 : n[ax] - g;
+  return true;
+}
+
+int build_links(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
+                int nlinks, int ghost, std::vector<HaloDesc>& out, size_t& scratch_doubles) {
+  out.clear();
+  scratch_doubles = 0;
+  for (int L = 0; L < nlinks; ++L) {
+    const fj_link& l = links[L];
+    if (l.tgt_block < 0 || l.tgt_block >= nblocks || l.src_block < 0 || l.src_block >= nblocks)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "link block index out of range");
+    if (l.tgt_face < 0 || l.tgt_face > 5 || l.src_face < 0 || l.src_face > 5)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "link face out of range");
+    if (l.orient != 0)
+      return set_err(ctx, FJ_ERR_NOT_IMPLEMENTED,
+                     "orient=" + std::to_string(l.orient) + " not supported in stage 1");
+    const fj_block& tb = blocks[l.tgt_block];
+    const fj_block& sb = blocks[l.src_block];
+    HaloDesc d;
+    d.tgt = tb.q;
+    d.src = sb.q;
+    d.tn[0] = tb.ni; d.tn[1] = tb.nj; d.tn[2] = tb.nk;
+    d.sn[0] = sb.ni; d.sn[1] = sb.nj; d.sn[2] = sb.nk;
+    int sext[3];
+    face_box(l.tgt_face, d.tn, ghost, false, d.tlo, d.ext);
+    face_box(l.src_face, d.sn, ghost, true, d.slo, sext);
+    if (sext[0] != d.ext[0] || sext[1] != d.ext[1] || sext[2] != d.ext[2])
+      return set_err(ctx, FJ_ERR_SHAPE,
+                     "halo slab shape mismatch: target (5," + std::to_string(d.ext[0]) + "," +
+                         std::to_string(d.ext[1]) + "," + std::to_string(d.ext[2]) +
+                         ") vs source (5," + std::to_string(sext[0]) + "," +
+                         std::to_string(sext[1]) + "," + std::to_string(sext[2]) + ")");
+    d.tgt_block = l.tgt_block;
+    d.off = (long long)scratch_doubles;
+    scratch_doubles += 5ull * d.ext[0] * d.ext[1] * d.ext[2];
+    scratch_doubles = (scratch_doubles + 31) & ~31ull;  // 256-byte aligned slabs
+    out.push_back(d);
+  }
+  return FJ_OK;
+}
+
+}  // namespace
+
+size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, int ghost) {
+  size_t total = 0;
+  for (int L = 0; L < nlinks; ++L) {
+    const fj_block& tb = blocks[links[L].tgt_block];
+    int n[3] = {tb.ni, tb.nj, tb.nk}, lo[3], ext[3];
+    if (!face_box(links[L].tgt_face, n, ghost, false, lo, ext)) return 0;
+    total += 5ull * ext[0] * ext[1] * ext[2];
+    total = (total + 31) & ~31ull;
+  }
+  return total * sizeof(double);
+}
+
+int halo_exchange(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
+                  int nlinks, int ghost, double* scratch, size_t scratch_bytes,
+                  cudaStream_t st) {
+  if (nlinks == 0) return FJ_OK;
+  std::vector<HaloDesc> descs;
+  size_t nd = 0;
+  int s = build_links(ctx, blocks, nblocks, links, nlinks, ghost, descs, nd);
+  if (s != FJ_OK) return s;
+  if (scratch_bytes < nd * sizeof(double))
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "halo scratch too small");
+  const int nl = (int)descs.size();
+  // gather all sources first (pre-exchange values), then scatter in order
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int base = 0; base < nl; base += kMaxLinksPerLaunch) {
+      HaloTable tab;
+      tab.n = std::min(kMaxLinksPerLaunch, nl - base);
+      int64_t vmax = 0;
+      for (int t = 0; t < tab.n; ++t) {
+        tab.d[t] = descs[base + t];
+        vmax = std::max<int64_t>(vmax, (int64_t)tab.d[t].ext[0] * tab.d[t].ext[1] * tab.d[t].ext[2]);
+      }
+      dim3 grid((unsigned)std::min<int64_t>(grid_for(pass == 0 ? 5 * vmax : vmax), 4096), tab.n);
+      if (pass == 0)
+        k_halo_gather<<<grid, kThreads, 0, st>>>(tab, scratch);
+      else
+        k_halo_scatter<<<grid, kThreads, 0, st>>>(tab, scratch);
+      ctx->launches += 1;
+      s = launch_status(ctx, "halo launch");
+      if (s != FJ_OK) return s;
+    }
+  }
+  return FJ_OK;
+}
+
+int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs, int nbcs,
+             const fj_params* p, cudaStream_t st) {
+  for (int b = 0; b < nbcs; ++b) {
+    const fj_bc& e = bcs[b];
+    if (e.block < 0 || e.block >= nblocks)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bc block index out of range");
+    if (e.face < 0 || e.face > 5)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bc face out of range");
+    if (e.type != FJ_BC_WALL && e.type != FJ_BC_SYMMETRY && e.type != FJ_BC_FARFIELD)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unsupported bc type");
+  }
+  for (int face = 0; face < 6; ++face) {
+    std::vector<BcDesc> ds;
+    for (int b = 0; b < nbcs; ++b) {
+      const fj_bc& e = bcs[b];
+      if (e.face != face) continue;
+      const fj_block& blk = blocks[e.block];
+      BcDesc d;
+      d.q = blk.q;
+      d.n[0] = blk.ni; d.n[1] = blk.nj; d.n[2] = blk.nk;
+      d.face = face;
+      d.type = e.type;
+      d.iso = e.isothermal;
+      d.T_wall = e.T_wall;
+      for (int v = 0; v < 5; ++v) d.qinf[v] = e.q_inf[v];
+      ds.push_back(d);
+    }
+    for (size_t base = 0; base < ds.size(); base += kMaxBcPerLaunch) {
+      BcTable tab;
+      tab.n = (int)std::min<size_t>(kMaxBcPerLaunch, ds.size() - base);
+      tab.gamma = p->gamma;
+      tab.R = p->R;
+      int64_t vmax = 0;
+      for (int t = 0; t < tab.n; ++t) {
+        tab.d[t] = ds[base + t];
+        const int ax = face >> 1;
+        int64_t area = (int64_t)tab.d[t].n[0] * tab.d[t].n[1] * tab.d[t].n[2] / tab.d[t].n[ax];
+        vmax = std::max<int64_t>(vmax, area * p->ghost);
+      }
+      dim3 grid((unsigned)std::min<int64_t>(grid_for(vmax), 4096), tab.n);
+      k_bc<<<grid, kThreads, 0, st>>>(tab, p->ghost);
+      ctx->launches += 1;
+      int s = launch_status(ctx, "bc launch");
+      if (s != FJ_OK) return s;
+    }
+  }
+  return FJ_OK;
+}
+
+}  // namespace fj

@@ -1,0 +1,35 @@
+// fj_rhs.cuh -- internal interfaces between the C ABI (fj_capi.cu) and the
+// RHS / step kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fj_common.cuh"
+
+namespace fj {
+
+// Which parts of the RHS a call evaluates (solver/step.py:10-15 = both).
+constexpr int kRhsInvscd = 1;
+constexpr int kRhsViscous = 2;
+
+// Staged pipeline (fj_rhs_staged.cu).  stage 0 writes the RHS to `out`;
+// stages 1..3 write the TVD-RK3 stage value (solver/step.py:45-53) computed
+// from q (the stage input), q0 (the step's start state) and dt.
+template <typename T>
+size_t staged_ws_bytes(int ni, int nj, int nk);
+template <typename T>
+int staged_rhs(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
+               const double* q0, double* out, int ni, int nj, int nk, const Phys& ph,
+               int flags, int stage, double dt, void* ws, cudaStream_t st);
+
+// Halo fill + boundary conditions (fj_halo.cu), in place on blocks[].q.
+// `scratch` holds the gathered source slabs (halo_ws_bytes of them).
+int halo_exchange(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
+                  int nlinks, int ghost, double* scratch, size_t scratch_bytes,
+                  cudaStream_t st);
+int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs, int nbcs,
+             const fj_params* p, cudaStream_t st);
+// Bytes of scratch the halo gather needs for these links (0 on shape errors).
+size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, int ghost);
+
+}  // namespace fj

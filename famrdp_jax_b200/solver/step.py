@@ -1,0 +1,81 @@
+"""The time step (famrdp_jax ``solver/step.py``) on the GPU.
+
+``step(state, cfg, dt)`` keeps the reference's signature and semantics: halo
+fill and boundary conditions once per step, then three Shu-Osher TVD-RK3
+stages over all padded cells of every block, returning a new State with
+t + dt and step + 1 (the input state is not modified).  The whole step is one
+call into libfamrdp_cuda.so (fj_step_f64).
+"""
+from __future__ import annotations
+
+import torch
+
+from famrdp_jax_b200 import _capi, _topology
+from famrdp_jax_b200.core.types import Block, Config, Metrics, State
+
+
+def _params(cfg: Config):
+    return _capi.params(cfg.gas, limiter=cfg.scheme.limiter, ghost=cfg.ghost,
+                        precision=getattr(cfg, "precision", "f64"))
+
+
+def _rhs_block(q: torch.Tensor, metrics: Metrics, cfg: Config) -> torch.Tensor:
+    """Inviscid + viscous RHS of one block (solver/step.py:10-15)."""
+    p = _params(cfg)
+    rhs = torch.empty_like(q)
+    ni, nj, nk = q.shape[1:]
+    c = _capi.ctx(q.device)
+    _capi.check(_capi.lib().fj_rhs_f64(c, _capi.dev_ptr(q, "q"), _capi.dev_ptr(metrics.kxyz, "kxyz"),
+                                       _capi.dev_ptr(metrics.vol, "vol"), _capi.dev_ptr(rhs, "rhs"),
+                                       ni, nj, nk, p, _capi.stream(q.device)), "fj_rhs_f64", c)
+    return rhs
+
+
+def rk_stage(q: torch.Tensor, q0: torch.Tensor | None, metrics: Metrics, cfg: Config, dt: float,
+             stage: int, out: torch.Tensor | None = None) -> torch.Tensor:
+    """One TVD-RK3 stage of one block, RHS and combine in one call
+    (solver/step.py:45-53 without the halo fill).  ``out`` may be ``q0``."""
+    p = _params(cfg)
+    out = torch.empty_like(q) if out is None else out
+    ni, nj, nk = q.shape[1:]
+    c = _capi.ctx(q.device)
+    q0p = _capi.dev_ptr(q0, "q0") if q0 is not None else None
+    _capi.check(_capi.lib().fj_rk_stage_f64(c, _capi.dev_ptr(q, "q"), q0p, _capi.dev_ptr(metrics.kxyz, "kxyz"),
+                                            _capi.dev_ptr(metrics.vol, "vol"), _capi.dev_ptr(out, "out"),
+                                            ni, nj, nk, p, float(dt), int(stage), _capi.stream(q.device)),
+                "fj_rk_stage_f64", c)
+    return out
+
+
+class StepPlan:
+    """The marshalled tables of one (state layout, cfg) pair, reusable across
+    steps whose blocks keep their shapes, metrics and device."""
+
+    def __init__(self, state: State, cfg: Config):
+        if len(state.blocks) != len(cfg.topology):
+            raise ValueError("state.blocks and cfg.topology differ in length")
+        self.cfg = cfg
+        self.params = _params(cfg)
+        self.links = _topology.links(cfg.topology)
+        self.bcs = _topology.bcs(cfg.topology, cfg)
+        self.link_arr = _topology.link_array(self.links)
+        self.bc_arr = _topology.bc_array(self.bcs)
+        self.metrics = state.metrics
+        self.device = state.blocks[0].q.device
+
+    def run(self, qs, outs, dt: float) -> None:
+        c = _capi.ctx(self.device)
+        blocks = _topology.block_array(qs, self.metrics)
+        _capi.check(_capi.lib().fj_step_f64(c, blocks, _topology.ptr_array(outs), len(qs), self.link_arr,
+                                            len(self.links), self.bc_arr, len(self.bcs), self.params,
+                                            float(dt), _capi.stream(self.device)), "fj_step_f64", c)
+
+
+def step(state: State, cfg: Config, dt: float, *, plan: StepPlan | None = None) -> State:
+    """Advance by dt with TVD-RK3 (solver/step.py:18-56)."""
+    plan = plan or StepPlan(state, cfg)
+    qs = [b.q for b in state.blocks]
+    outs = [torch.empty_like(q) for q in qs]
+    plan.run(qs, outs, dt)
+    new_blocks = tuple(Block(q=o, xyz=b.xyz) for o, b in zip(outs, state.blocks))
+    return State(blocks=new_blocks, metrics=state.metrics, t=state.t + dt, step=state.step + 1)

@@ -1,0 +1,195 @@
+/*
+ * famrdp_cuda.h -- C ABI of libfamrdp_cuda.so, the sm_100a kernels behind the
+ * famrdp_jax RHS + TVD-RK3 step path.
+ *
+ * Conventions
+ *   - Every array argument is a DEVICE pointer to contiguous float64 data in
+ *     the reference's C-order layout (famrdp_jax core/types.py:26-89):
+ *       q    (5, ni, nj, nk)   [rho, rho*u, rho*v, rho*w, rho*E], ghosts embedded
+ *       xyz  (3, ni, nj, nk)
+ *       kxyz (3, 3, ni, nj, nk)  kxyz[l][m] = d xi_l / d x_m
+ *       jac, vol (ni, nj, nk)
+ *     so k is the contiguous axis.  The caller owns all of them.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls are stream-ordered and asynchronous unless stated otherwise.
+ *   - Every entry point returns an int status (FJ_OK = 0).  A context-taking
+ *     call records a message retrievable with fj_last_error(ctx).  No C++
+ *     exception crosses this boundary.
+ *   - A context (fj_ctx) owns only scratch memory (stage buffers and
+ *     intermediate fluxes) and must be used from one host thread and one stream
+ *     at a time.
+ *
+ * The reference is pure Python/JAX and has no FFI; each entry point replaces
+ * one Python function of famrdp_jax (cited beside it, path:line relative to
+ * that project), and the Python shim in famrdp_jax_b200 keeps that function's
+ * name, signature and error behaviour.
+ */
+#ifndef FAMRDP_CUDA_H
+#define FAMRDP_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FJ_ABI_VERSION 1
+
+enum fj_status {
+  FJ_OK = 0,
+  FJ_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad enum value   */
+  FJ_ERR_CUDA = 2,             /* a CUDA runtime call or launch failed      */
+  FJ_ERR_NOT_IMPLEMENTED = 3,  /* e.g. orient != 0 (mesh/halo.py:86-87)     */
+  FJ_ERR_SHAPE = 4,            /* halo slab extents differ (mesh/halo.py:53) */
+  FJ_ERR_NONFINITE = 5,        /* a reduction found NaN/Inf                  */
+  FJ_ERR_NO_MEMORY = 6         /* scratch allocation failed                  */
+};
+
+enum fj_visc_law { FJ_VISC_SUTHERLAND = 0, FJ_VISC_CONSTANT = 1 };
+enum fj_limiter { FJ_LIM_MINMOD = 0, FJ_LIM_VANLEER = 1 };
+enum fj_precision { FJ_PREC_F64 = 0, FJ_PREC_F32FLUX = 1 };
+enum fj_face { FJ_IMIN = 0, FJ_IMAX = 1, FJ_JMIN = 2, FJ_JMAX = 3, FJ_KMIN = 4, FJ_KMAX = 5 };
+enum fj_bc_type { FJ_BC_WALL = 2, FJ_BC_SYMMETRY = 3, FJ_BC_FARFIELD = 4 };
+
+/* Gas model + scheme (GasModel core/types.py:159-167, SchemeChoice :170-176). */
+typedef struct fj_params {
+  double gamma;
+  double R;
+  double mu0;
+  double T0;
+  double Ts;
+  double Pr;            /* GasModel.Pr_lam                                  */
+  double eps_entropy;   /* Harten parameter; the reference always uses 0.1  */
+  int visc_law;         /* enum fj_visc_law                                 */
+  int limiter;          /* enum fj_limiter                                  */
+  int ghost;            /* ghost layers; the kernels require 2              */
+  int precision;        /* enum fj_precision                                */
+} fj_params;
+
+/* One block of a multi-block state. */
+typedef struct fj_block {
+  double* q;            /* (5, ni, nj, nk)                                  */
+  const double* kxyz;   /* (3, 3, ni, nj, nk)                               */
+  const double* vol;    /* (ni, nj, nk)                                     */
+  int ni, nj, nk;       /* padded extents                                   */
+} fj_block;
+
+/* One CUT1TO1 face (a BlockTopology.neighbors entry, mesh/halo.py:79-90).
+ * Links are applied in array order; the caller lists them in the reference's
+ * (block, neighbors-dict) iteration order. */
+typedef struct fj_link {
+  int tgt_block, tgt_face;
+  int src_block, src_face;
+  int orient;           /* must be 0 */
+} fj_link;
+
+/* One physical boundary face (physics/bc/dispatch.py:11-32).  The caller lists
+ * them per block in Face enum order; blocks are independent. */
+typedef struct fj_bc {
+  int block, face, type;   /* type: enum fj_bc_type                         */
+  int isothermal;          /* WALL only: 1 = isothermal, 0 = adiabatic      */
+  double T_wall;           /* WALL isothermal only                          */
+  double q_inf[5];         /* FARFIELD only                                 */
+} fj_bc;
+
+typedef struct fj_ctx fj_ctx;
+
+/* ---- library / context --------------------------------------------------- */
+int fj_abi_version(void);
+const char* fj_status_string(int status);
+int fj_ctx_create(fj_ctx** out);             /* on the current CUDA device  */
+int fj_ctx_destroy(fj_ctx* ctx);
+const char* fj_last_error(const fj_ctx* ctx);
+/* Number of kernels launched through this context so far (instrumentation;
+ * the reference has no counterpart). */
+int fj_launch_count(const fj_ctx* ctx, int64_t* out);
+
+/* ---- pointwise building blocks ------------------------------------------- */
+/* physics/eos.py:12-17 cons_to_prim over ncell cells, (5, ncell) -> (5, ncell) */
+int fj_cons_to_prim_f64(const double* q, double* pv, int64_t ncell, double gamma,
+                        void* stream);
+/* physics/eos.py:5-9 prim_to_cons */
+int fj_prim_to_cons_f64(const double* pv, double* q, int64_t ncell, double gamma,
+                        void* stream);
+/* flux/roe.py:21-85 roe_flux: UL, UR (5, nface), nxyz (3, nface) -> F (5, nface) */
+int fj_roe_flux_f64(const double* UL, const double* UR, const double* nxyz, double* F,
+                    int64_t nface, double gamma, double eps_entropy, void* stream);
+/* physics/reconstruct/muscl2.py:5-12 minmod / vanleer elementwise over n values */
+int fj_limiter_f64(const double* a, const double* b, double* out, int64_t n, int limiter,
+                   void* stream);
+/* physics/reconstruct/muscl2.py:18-37 on pv (nv, n1, n2, n3) along axis 1..3;
+ * pvL/pvR have extent n_axis-3 along that axis. */
+int fj_muscl2_f64(const double* pv, double* pvL, double* pvR, int nv, int n1, int n2,
+                  int n3, int axis, int limiter, void* stream);
+
+/* ---- right-hand side (one block) ------------------------------------------ */
+/* rhs/invscd.py:18-133 compute_invscd_rhs */
+int fj_invscd_rhs_f64(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
+                      double* rhs, int ni, int nj, int nk, const fj_params* p,
+                      void* stream);
+/* rhs/viscous.py:19-119 compute_viscous_rhs */
+int fj_viscous_rhs_f64(fj_ctx* ctx, const double* q, const double* kxyz, double* rhs,
+                       int ni, int nj, int nk, const fj_params* p, void* stream);
+/* solver/step.py:10-15 _rhs_block = inviscid + viscous */
+int fj_rhs_f64(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
+               double* rhs, int ni, int nj, int nk, const fj_params* p, void* stream);
+
+/* ---- halo fill and boundary conditions (in place) ------------------------- */
+/* mesh/halo.py:56-92 halo_exchange: every link reads its source slab from the
+ * pre-exchange arrays; later links overwrite earlier ones. */
+int fj_halo_exchange_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks,
+                         const fj_link* links, int nlinks, int ghost, void* stream);
+/* physics/bc/dispatch.py:11-32 apply_bc for all blocks */
+int fj_apply_bc_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs,
+                    int nbcs, const fj_params* p, void* stream);
+
+/* ---- the time step ------------------------------------------------------- */
+/* solver/step.py:18-56 step: halo + BC once, then three TVD-RK3 stages.
+ * Reads blocks[b].q (unchanged) and writes the new state to q_out[b], which
+ * must not alias any blocks[b].q. */
+int fj_step_f64(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int nblocks,
+                const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs,
+                const fj_params* p, double dt, void* stream);
+
+/* One TVD-RK3 stage of one block, RHS and combine together (solver/step.py:
+ * 45-53 for a single block, without the halo fill):
+ *   stage 1: out = q + dt*L(q)
+ *   stage 2: out = 0.75*q0 + 0.25*(q + dt*L(q))
+ *   stage 3: out = (1/3)*q0 + (2/3)*(q + dt*L(q))
+ * `out` must not alias `q`; it may alias `q0` (each cell of q0 is read only by
+ * the thread that writes the same cell of out). */
+int fj_rk_stage_f64(fj_ctx* ctx, const double* q, const double* q0, const double* kxyz,
+                    const double* vol, double* out, int ni, int nj, int nk, const fj_params* p,
+                    double dt, int stage, void* stream);
+
+/* time/rk.py:5-20 one Shu-Osher stage combine, elementwise over n values:
+ *   stage 1: out = qs + dt*L
+ *   stage 2: out = 0.75*q0 + 0.25*(qs + dt*L)
+ *   stage 3: out = (1/3)*q0 + (2/3)*(qs + dt*L)                               */
+int fj_rk3_combine_f64(const double* q0, const double* qs, const double* L, double* out,
+                       int64_t n, double dt, int stage, void* stream);
+
+/* ---- grid metrics --------------------------------------------------------- */
+/* mesh/metric.py:31-70 compute_metrics (4th-order central, roll wrap) */
+int fj_metrics_f64(const double* xyz, double* jac, double* kxyz, double* vol, int ni,
+                   int nj, int nk, void* stream);
+
+/* ---- reductions (FP64; block until the host result is ready) ------------- */
+/* Global dt = cfl / max_interior sum_a (|u.n_a| + c) |kxyz[a,:]| / vol. */
+int fj_cfl_dt_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_params* p,
+                  double cfl, double* dt_out, void* stream);
+/* J = sum_interior vol * 0.5 * (q1^2 + q2^2 + q3^2) / q0 over all blocks. */
+int fj_kinetic_energy_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, int ghost,
+                          double* out, void* stream);
+/* Counts non-finite values of q over all padded cells of all blocks and the
+ * minimum density and pressure; returns FJ_ERR_NONFINITE when count > 0 or
+ * min rho <= 0 or min p <= 0. */
+int fj_check_state_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, double gamma,
+                       int64_t* nonfinite_out, double* min_rho_out, double* min_p_out,
+                       void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FAMRDP_CUDA_H */
