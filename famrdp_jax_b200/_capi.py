@@ -25,6 +25,8 @@ FJ_ERR_NOT_IMPLEMENTED = 3
 FJ_ERR_SHAPE = 4
 FJ_ERR_NONFINITE = 5
 FJ_ERR_NO_MEMORY = 6
+FJ_ERR_SCRATCH_LIMIT = 7  # block too large for fj_rhs_noalloc_f64's fixed scratch
+NOALLOC_SCRATCH_BYTES = 64 << 20
 
 VISC_LAWS = {"sutherland": 0, "constant": 1}
 LIMITERS = {"minmod": 0, "vanleer": 1}
@@ -76,6 +78,7 @@ SIGNATURES = {
     "fj_invscd_rhs_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _P]),
     "fj_viscous_rhs_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _P]),
     "fj_rhs_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _P]),
+    "fj_rhs_noalloc_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _P]),
     "fj_halo_exchange_f64": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjLink), _I, _I, _P]),
     "fj_apply_bc_f64": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjBc), _I,
                              ctypes.POINTER(FjParams), _P]),
@@ -158,6 +161,8 @@ def _raise(status: int, c, what: str):
         raise FloatingPointError(text)
     if status == FJ_ERR_NO_MEMORY:
         raise MemoryError(text)
+    if status == FJ_ERR_SCRATCH_LIMIT:
+        raise ValueError(text)
     raise RuntimeError(text)
 
 

@@ -93,6 +93,7 @@ const char* fj_status_string(int status) {
     case FJ_ERR_SHAPE: return "shape mismatch";
     case FJ_ERR_NONFINITE: return "non-finite or non-physical state";
     case FJ_ERR_NO_MEMORY: return "out of device memory";
+    case FJ_ERR_SCRATCH_LIMIT: return "block exceeds the fixed scratch of the no-allocation entry point";
     default: return "unknown status";
   }
 }

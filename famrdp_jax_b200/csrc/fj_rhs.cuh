@@ -22,6 +22,13 @@ int staged_rhs(fj_ctx* ctx, const double* q, const double* kxyz, const double* v
                const double* q0, double* out, int ni, int nj, int nk, const Phys& ph,
                int flags, int stage, double dt, void* ws, cudaStream_t st);
 
+// The RHS (stage 0) launch sequence without a context, on caller-given scratch
+// of staged_ws_bytes<T> bytes.
+template <typename T>
+cudaError_t staged_rhs_noctx(const double* q, const double* kxyz, const double* vol,
+                             double* out, int ni, int nj, int nk, const Phys& ph, void* ws,
+                             cudaStream_t st);
+
 // Halo fill + boundary conditions (fj_halo.cu), in place on blocks[].q.
 // `scratch` holds the gathered source slabs (halo_ws_bytes of them).
 int halo_exchange(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,

@@ -280,6 +280,39 @@ int staged_rhs(fj_ctx* ctx, const double* q, const double* kxyz, const double* v
   return launch_status(ctx, "staged rhs launch");
 }
 
+// The same RHS launch sequence without a context (no launch counting, no
+// error text): used by the entry point whose scratch is a static device array.
+template <typename T>
+cudaError_t staged_rhs_noctx(const double* q, const double* kxyz, const double* vol,
+                             double* out, int ni, int nj, int nk, const Phys& ph, void* ws,
+                             cudaStream_t st) {
+  const int N = ni * nj * nk;
+  const size_t fI = (size_t)(ni - 3) * nj * nk, fJ = (size_t)ni * (nj - 3) * nk,
+               fK = (size_t)ni * nj * (nk - 3);
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  char* p = (char*)ws;
+  T* pv = (T*)p;  p += al(5 * (size_t)N * sizeof(T));
+  T* G = (T*)p;   p += al(9 * (size_t)N * sizeof(T));
+  T* Fi = (T*)p;  p += al(5 * fI * sizeof(T));
+  T* Fj = (T*)p;  p += al(5 * fJ * sizeof(T));
+  T* Fk = (T*)p;
+  k_prim<T><<<grid_for(N), kThreads, 0, st>>>(q, pv, N, ph.gm1);
+  k_vflux<T><<<grid_for(N), kThreads, 0, st>>>(pv, kxyz, G, ni, nj, nk, ph);
+  k_iflux<T, 0><<<grid_for(fI), kThreads, 0, st>>>(pv, kxyz, Fi, ni, nj, nk, ph);
+  k_iflux<T, 1><<<grid_for(fJ), kThreads, 0, st>>>(pv, kxyz, Fj, ni, nj, nk, ph);
+  k_iflux<T, 2><<<grid_for(fK), kThreads, 0, st>>>(pv, kxyz, Fk, ni, nj, nk, ph);
+  k_combine<T><<<grid_for(N), kThreads, 0, st>>>(Fi, Fj, Fk, G, kxyz, vol, q, nullptr, out, ni,
+                                                 nj, nk, kRhsInvscd | kRhsViscous, 0, 0.0);
+  return cudaGetLastError();
+}
+
+template cudaError_t staged_rhs_noctx<double>(const double*, const double*, const double*,
+                                              double*, int, int, int, const Phys&, void*,
+                                              cudaStream_t);
+template cudaError_t staged_rhs_noctx<float>(const double*, const double*, const double*,
+                                             double*, int, int, int, const Phys&, void*,
+                                             cudaStream_t);
+
 template size_t staged_ws_bytes<double>(int, int, int);
 template size_t staged_ws_bytes<float>(int, int, int);
 template int staged_rhs<double>(fj_ctx*, const double*, const double*, const double*,

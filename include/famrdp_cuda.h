@@ -42,8 +42,13 @@ enum fj_status {
   FJ_ERR_NOT_IMPLEMENTED = 3,  /* e.g. orient != 0 (mesh/halo.py:86-87)     */
   FJ_ERR_SHAPE = 4,            /* halo slab extents differ (mesh/halo.py:53) */
   FJ_ERR_NONFINITE = 5,        /* a reduction found NaN/Inf                  */
-  FJ_ERR_NO_MEMORY = 6         /* scratch allocation failed                  */
+  FJ_ERR_NO_MEMORY = 6,        /* scratch allocation failed                  */
+  FJ_ERR_SCRATCH_LIMIT = 7     /* block too large for the fixed scratch of
+                                  fj_rhs_noalloc_f64                         */
 };
+
+/* Size of the fixed device scratch behind fj_rhs_noalloc_f64 (64 MiB). */
+#define FJ_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 enum fj_visc_law { FJ_VISC_SUTHERLAND = 0, FJ_VISC_CONSTANT = 1 };
 enum fj_limiter { FJ_LIM_MINMOD = 0, FJ_LIM_VANLEER = 1 };
@@ -133,6 +138,26 @@ int fj_viscous_rhs_f64(fj_ctx* ctx, const double* q, const double* kxyz, double*
 /* solver/step.py:10-15 _rhs_block = inviscid + viscous */
 int fj_rhs_f64(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
                double* rhs, int ni, int nj, int nk, const fj_params* p, void* stream);
+
+/* The same result as fj_rhs_f64 for callers that cannot allocate device
+ * memory.  No counterpart in the reference.  It takes no context and never
+ * calls cudaMalloc/cudaFree: its intermediates live in one fixed device array
+ * of FJ_NOALLOC_SCRATCH_BYTES inside the library, which each device that runs
+ * it keeps until the process exits.  Meant for callers whose device memory is
+ * owned by a framework (e.g. an XLA custom call under JAX, whose allocator has
+ * reserved most of the GPU) or by a fixed start-up budget.
+ *   - Limit: the intermediates need about 232 bytes per padded cell in FP64
+ *     (116 with precision FJ_PREC_F32FLUX), so blocks of up to ~289,000 padded
+ *     cells (e.g. 66^3) in FP64; larger blocks return FJ_ERR_SCRATCH_LIMIT
+ *     before any device work.
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current); make that first call before any stream capture.
+ *   - All calls share the one array: calls that can run at the same time on
+ *     one device (different streams, or different host threads) race on it
+ *     and must be ordered by the caller.  The array keeps the last call's
+ *     contents; no call depends on them. */
+int fj_rhs_noalloc_f64(const double* q, const double* kxyz, const double* vol, double* rhs,
+                       int ni, int nj, int nk, const fj_params* p, void* stream);
 
 /* ---- halo fill and boundary conditions (in place) ------------------------- */
 /* mesh/halo.py:56-92 halo_exchange: every link reads its source slab from the
