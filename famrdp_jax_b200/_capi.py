@@ -69,6 +69,7 @@ SIGNATURES = {
     "fj_ctx_destroy": (_I, [_P]),
     "fj_last_error": (ctypes.c_char_p, [_P]),
     "fj_launch_count": (_I, [_P, ctypes.POINTER(_I64)]),
+    "fj_ctx_set_pipeline": (_I, [_P, _I, _I]),
     "fj_rk_stage_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _D, _I, _P]),
     "fj_cons_to_prim_f64": (_I, [_P, _P, _I64, _D, _P]),
     "fj_prim_to_cons_f64": (_I, [_P, _P, _I64, _D, _P]),
@@ -132,6 +133,16 @@ def ctx(device: torch.device | int | None = None) -> int:
             h = p.value
             _ctxs[dev] = h
     return h
+
+
+PIPELINES = {"fused": 0, "staged": 1}
+
+
+def set_pipeline(pipeline: str = "fused", seg: int = 0, device=None) -> None:
+    """Fused single-kernel stages (default) or the staged four-kernel pipeline;
+    ``seg`` = planes per CTA along i for the fused kernel (0 = automatic)."""
+    c = ctx(device)
+    check(lib().fj_ctx_set_pipeline(c, PIPELINES[pipeline], int(seg)), "fj_ctx_set_pipeline", c)
 
 
 def launch_count(device=None) -> int:

@@ -8,6 +8,7 @@
 #include "famrdp_cuda.h"
 #include "fj_common.cuh"
 #include "fj_rhs.cuh"
+#include "fj_stage.cuh"
 
 namespace fj {
 int metrics(const double* xyz, double* jac, double* kxyz, double* vol, int ni, int nj, int nk,
@@ -38,7 +39,10 @@ inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-size_t rhs_scratch_bytes(int precision, int ni, int nj, int nk) {
+// Scratch of one RHS/stage evaluation: none for the fused kernel, the
+// intermediates for the staged pipeline.
+size_t rhs_scratch_bytes(const fj_ctx* ctx, int precision, int ni, int nj, int nk) {
+  if (ctx->pipeline == FJ_PIPELINE_FUSED) return 0;
   return precision == FJ_PREC_F32FLUX ? staged_ws_bytes<float>(ni, nj, nk)
                                       : staged_ws_bytes<double>(ni, nj, nk);
 }
@@ -47,6 +51,23 @@ int run_rhs(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
             const double* q0, double* out, int ni, int nj, int nk, const fj_params* p, int flags,
             int stage, double dt, void* ws, cudaStream_t st) {
   Phys ph = make_phys(p);
+  if (ctx->pipeline == FJ_PIPELINE_FUSED) {
+    StageArgs a{};
+    a.q = q;
+    a.q0 = q0;
+    a.kxyz = kxyz;
+    a.kxyz32 = nullptr;
+    a.vol = vol;
+    a.out = out;
+    a.ni = ni;
+    a.nj = nj;
+    a.nk = nk;
+    a.flags = flags;
+    a.stage = stage;
+    a.dt = dt;
+    a.ph = ph;
+    return fused_stage(ctx, a, ctx->seg, p->precision, st);
+  }
   if (p->precision == FJ_PREC_F32FLUX)
     return staged_rhs<float>(ctx, q, kxyz, vol, q0, out, ni, nj, nk, ph, flags, stage, dt, ws, st);
   return staged_rhs<double>(ctx, q, kxyz, vol, q0, out, ni, nj, nk, ph, flags, stage, dt, ws, st);
@@ -61,7 +82,7 @@ int rhs_entry(fj_ctx* ctx, const double* q, const double* kxyz, const double* vo
   if (s != FJ_OK) return s;
   if (!q || !kxyz || !rhs || ((flags & kRhsInvscd) && !vol))
     return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "NULL array argument");
-  s = ensure_ws(ctx, rhs_scratch_bytes(p->precision, ni, nj, nk));
+  s = ensure_ws(ctx, rhs_scratch_bytes(ctx, p->precision, ni, nj, nk));
   if (s != FJ_OK) return s;
   return run_rhs(ctx, q, kxyz, vol, nullptr, rhs, ni, nj, nk, p, flags, 0, 0.0, ctx->ws, S(stream));
 }
@@ -121,6 +142,16 @@ int fj_ctx_destroy(fj_ctx* ctx) {
 
 const char* fj_last_error(const fj_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
+int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg) {
+  if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
+  if (pipeline != FJ_PIPELINE_FUSED && pipeline != FJ_PIPELINE_STAGED)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown pipeline");
+  if (seg < 0) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "segment length must be >= 0");
+  ctx->pipeline = pipeline;
+  ctx->seg = seg;
+  return FJ_OK;
+}
+
 int fj_launch_count(const fj_ctx* ctx, int64_t* out) {
   if (!ctx || !out) return FJ_ERR_INVALID_ARGUMENT;
   *out = ctx->launches;
@@ -139,7 +170,7 @@ int fj_rk_stage_f64(fj_ctx* ctx, const double* q, const double* q0, const double
   if (!q || !kxyz || !vol || !out || (stage > 1 && !q0))
     return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "NULL array argument");
   if (out == q) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "out must not alias q");
-  s = ensure_ws(ctx, rhs_scratch_bytes(p->precision, ni, nj, nk));
+  s = ensure_ws(ctx, rhs_scratch_bytes(ctx, p->precision, ni, nj, nk));
   if (s != FJ_OK) return s;
   return run_rhs(ctx, q, kxyz, vol, q0, out, ni, nj, nk, p, kRhsInvscd | kRhsViscous, stage, dt,
                  ctx->ws, S(stream));
@@ -247,7 +278,7 @@ int fj_step_f64(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int n
   for (int b = 0; b < nblocks; ++b) {
     if (!q_out[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "q_out entry is NULL");
     maxN = std::max(maxN, (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk);
-    rhs_b = std::max(rhs_b, rhs_scratch_bytes(p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
+    rhs_b = std::max(rhs_b, rhs_scratch_bytes(ctx, p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
   }
   const size_t stage_b = align256(5 * maxN * sizeof(double));
   const size_t halo_b = halo_ws_bytes(blocks, links, nlinks, p->ghost);

@@ -18,6 +18,8 @@ struct fj_ctx {
   size_t red_bytes = 0;
   std::string last_error;
   int64_t launches = 0;      // kernels launched through this context
+  int pipeline = FJ_PIPELINE_FUSED;
+  int seg = 0;               // fused kernel: planes per CTA along i (0 = automatic)
 };
 
 namespace fj {

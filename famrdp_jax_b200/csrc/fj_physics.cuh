@@ -204,6 +204,139 @@ __device__ __forceinline__ void invscd_face(const Prim<T> c[4], T kl0, T kl1, T 
   for (int v = 0; v < 5; ++v) F[v] = F[v] * nmag;
 }
 
+// ---------------------------------------------------------------------------
+// Reformulated face flux for the fused kernels.  Same mathematics as
+// roe_flux + prim_to_cons above, rearranged to cut divisions and recomputation:
+//   * the face states stay primitive (the reference rebuilds u = (rho u)/rho,
+//     p = (g-1)(rhoE - rho ke) from the conserved states it just built, which
+//     returns the same values up to rounding);
+//   * one reciprocal per divisor (1/(sqL+sqR), 1/c^2, 1/eps, 1/rho);
+//   * the shear term rho_h (du_t - (du_t . n) n) of flux/roe.py:69-79 equals
+//     (dU_m - u_h,m dU_0) - dun n_m with dun the normal-velocity jump of
+//     flux/roe.py:57, so it needs no division by rho_h.
+// For T = float the reciprocals and square roots use the fast MUFU-based
+// intrinsics (__fdividef, rsqrtf); the FP32-flux path's tolerance is 1e-5.
+// ---------------------------------------------------------------------------
+template <typename T> struct FastMath;
+template <> struct FastMath<double> {
+  static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+  static __device__ __forceinline__ double sqrt_pos(double x) { return sqrt(x); }
+};
+template <> struct FastMath<float> {
+  static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
+  // x must be > 0
+  static __device__ __forceinline__ float sqrt_pos(float x) { return x * rsqrtf(x); }
+};
+
+// minmod(a, b) of muscl2.py:5-7 without sign products: the smaller-magnitude
+// argument when both have the same strict sign, else 0.
+template <typename T> __device__ __forceinline__ T minmod_sel(T a, T b) {
+  return (a > T(0) && b > T(0)) ? fj_min(a, b) : ((a < T(0) && b < T(0)) ? fj_max(a, b) : T(0));
+}
+
+template <typename T>
+__device__ __forceinline__ void muscl2_fast(T c0, T c1, T c2, T c3, int limiter, T& L, T& R) {
+  const T d0 = c1 - c0, d1 = c2 - c1, d2 = c3 - c2;
+  T sL, sR;
+  if (limiter == 0) {
+    sL = minmod_sel(d0, d1);
+    sR = minmod_sel(d1, d2);
+  } else {
+    sL = vanleer(d0, d1);
+    sR = vanleer(d1, d2);
+  }
+  L = c1 + T(0.5) * sL;
+  R = c2 - T(0.5) * sR;
+}
+
+// Roe flux (flux/roe.py:21-85) of the primitive face states L, R along the unit
+// normal n; inv_gm1 = 1/(gamma-1).
+template <typename T>
+__device__ __forceinline__ void roe_prim(const Prim<T>& L, const Prim<T>& R, T n0, T n1, T n2,
+                                         T gm1, T inv_gm1, T eps_entropy, T F[5]) {
+  using M = FastMath<T>;
+  const T rhoL = fj_max(L.rho, Tiny<T>::rho()), rhoR = fj_max(R.rho, Tiny<T>::rho());
+  const T keL = T(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
+  const T keR = T(0.5) * (R.u * R.u + R.v * R.v + R.w * R.w);
+  const T EL = L.p * inv_gm1 + L.rho * keL;  // conserved energies (eos.py:8)
+  const T ER = R.p * inv_gm1 + R.rho * keR;
+  const T HL = (EL + L.p) * M::rcp(rhoL);
+  const T HR = (ER + R.p) * M::rcp(rhoR);
+  const T sqL = M::sqrt_pos(rhoL), sqR = M::sqrt_pos(rhoR);
+  const T inv_ss = M::rcp(fj_max(sqL + sqR, Tiny<T>::ss()));
+  const T wl = sqL * inv_ss, wr = sqR * inv_ss;
+  const T u_h = wl * L.u + wr * R.u;
+  const T v_h = wl * L.v + wr * R.v;
+  const T w_h = wl * L.w + wr * R.w;
+  const T H_h = wl * HL + wr * HR;
+  const T q2 = u_h * u_h + v_h * v_h + w_h * w_h;
+  const T c2 = fj_max(gm1 * (H_h - T(0.5) * q2), Tiny<T>::c2());
+  const T c_h = M::sqrt_pos(c2);
+  const T inv_c2 = M::rcp(c2);
+  const T un_h = u_h * n0 + v_h * n1 + w_h * n2;
+  const T rho_h = sqL * sqR;
+
+  const T eps = eps_entropy * (fj_abs(un_h) + c_h);
+  const T inv_eps = M::rcp(eps);
+  const T lam1 = un_h - c_h, lam5 = un_h + c_h;
+  const T al1 = fj_abs(lam1) >= eps ? fj_abs(lam1) : T(0.5) * (lam1 * lam1 * inv_eps + eps);
+  const T al5 = fj_abs(lam5) >= eps ? fj_abs(lam5) : T(0.5) * (lam5 * lam5 * inv_eps + eps);
+  const T al2 = fj_abs(un_h);
+
+  const T d0 = R.rho - L.rho;
+  const T d1 = R.rho * R.u - L.rho * L.u;
+  const T d2 = R.rho * R.v - L.rho * L.v;
+  const T d3 = R.rho * R.w - L.rho * L.w;
+  const T d4 = ER - EL;
+  const T dp = gm1 * (d4 - u_h * d1 - v_h * d2 - w_h * d3 + T(0.5) * q2 * d0);
+  const T dun = (d1 * n0 + d2 * n1 + d3 * n2) - un_h * d0;
+  const T rcd = rho_h * c_h * dun;
+  const T hc2 = T(0.5) * inv_c2;
+  const T a1 = (dp - rcd) * hc2;
+  const T a5 = (dp + rcd) * hc2;
+  const T a23 = d0 - dp * inv_c2;
+  const T t1 = (d1 - u_h * d0) - dun * n0;
+  const T t2 = (d2 - v_h * d0) - dun * n1;
+  const T t3 = (d3 - w_h * d0) - dun * n2;
+  const T t4 = u_h * t1 + v_h * t2 + w_h * t3;
+
+  const T s1 = al1 * a1, s5 = al5 * a5;
+  const T cn0 = c_h * n0, cn1 = c_h * n1, cn2 = c_h * n2, cun = c_h * un_h;
+  const T unL = L.u * n0 + L.v * n1 + L.w * n2;
+  const T unR = R.u * n0 + R.v * n1 + R.w * n2;
+  const T mL = rhoL * unL, mR = rhoR * unR;
+  F[0] = T(0.5) * (mL + mR) - T(0.5) * (s1 + s5 + al2 * a23);
+  F[1] = T(0.5) * ((mL * L.u + L.p * n0) + (mR * R.u + R.p * n0)) -
+         T(0.5) * (s1 * (u_h - cn0) + s5 * (u_h + cn0) + al2 * (a23 * u_h + t1));
+  F[2] = T(0.5) * ((mL * L.v + L.p * n1) + (mR * R.v + R.p * n1)) -
+         T(0.5) * (s1 * (v_h - cn1) + s5 * (v_h + cn1) + al2 * (a23 * v_h + t2));
+  F[3] = T(0.5) * ((mL * L.w + L.p * n2) + (mR * R.w + R.p * n2)) -
+         T(0.5) * (s1 * (w_h - cn2) + s5 * (w_h + cn2) + al2 * (a23 * w_h + t3));
+  F[4] = T(0.5) * (mL * HL + mR * HR) -
+         T(0.5) * (s1 * (H_h - cun) + s5 * (H_h + cun) + al2 * (a23 * (T(0.5) * q2) + t4));
+}
+
+// One inviscid face (rhs/invscd.py:62-100) in the reformulated arithmetic:
+// MUSCL on the four cells' primitives, face normal from the two adjacent
+// cells' kxyz rows, Roe, times |n|.
+template <typename T>
+__device__ __forceinline__ void invscd_face_fast(const Prim<T> c[4], T kl0, T kl1, T kl2, T kr0,
+                                                 T kr1, T kr2, T gm1, T inv_gm1, T eps_entropy,
+                                                 int limiter, T F[5]) {
+  Prim<T> L, R;
+  muscl2_fast(c[0].rho, c[1].rho, c[2].rho, c[3].rho, limiter, L.rho, R.rho);
+  muscl2_fast(c[0].u, c[1].u, c[2].u, c[3].u, limiter, L.u, R.u);
+  muscl2_fast(c[0].v, c[1].v, c[2].v, c[3].v, limiter, L.v, R.v);
+  muscl2_fast(c[0].w, c[1].w, c[2].w, c[3].w, limiter, L.w, R.w);
+  muscl2_fast(c[0].p, c[1].p, c[2].p, c[3].p, limiter, L.p, R.p);
+  const T nf0 = T(0.5) * (kl0 + kr0), nf1 = T(0.5) * (kl1 + kr1), nf2 = T(0.5) * (kl2 + kr2);
+  const T nmag = fj_sqrt(nf0 * nf0 + nf1 * nf1 + nf2 * nf2) + Tiny<T>::nmag();
+  const T inv = FastMath<T>::rcp(nmag);
+  roe_prim(L, R, nf0 * inv, nf1 * inv, nf2 * inv, gm1, inv_gm1, eps_entropy, F);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) F[v] = F[v] * nmag;
+}
+
 // physics/eos.py:24-25 (or the constant law)
 template <typename T>
 __device__ __forceinline__ T viscosity(T Tt, int law, T mu0, T T0, T Ts) {

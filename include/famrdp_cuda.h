@@ -50,6 +50,7 @@ enum fj_status {
 /* Size of the fixed device scratch behind fj_rhs_noalloc_f64 (64 MiB). */
 #define FJ_NOALLOC_SCRATCH_BYTES (64u << 20)
 
+enum fj_pipeline { FJ_PIPELINE_FUSED = 0, FJ_PIPELINE_STAGED = 1 };
 enum fj_visc_law { FJ_VISC_SUTHERLAND = 0, FJ_VISC_CONSTANT = 1 };
 enum fj_limiter { FJ_LIM_MINMOD = 0, FJ_LIM_VANLEER = 1 };
 enum fj_precision { FJ_PREC_F64 = 0, FJ_PREC_F32FLUX = 1 };
@@ -105,6 +106,12 @@ const char* fj_status_string(int status);
 int fj_ctx_create(fj_ctx** out);             /* on the current CUDA device  */
 int fj_ctx_destroy(fj_ctx* ctx);
 const char* fj_last_error(const fj_ctx* ctx);
+/* Selects how the context evaluates RHS / RK stages (no counterpart in the
+ * reference): FJ_PIPELINE_FUSED (default) runs one fused kernel per stage and
+ * block; FJ_PIPELINE_STAGED runs the four-kernel pipeline through scratch
+ * (kept as a cross-check).  `seg` = planes per CTA along i for the fused
+ * kernel, 0 = chosen from the block size and the SM count. */
+int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg);
 /* Number of kernels launched through this context so far (instrumentation;
  * the reference has no counterpart). */
 int fj_launch_count(const fj_ctx* ctx, int64_t* out);

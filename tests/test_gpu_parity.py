@@ -38,6 +38,15 @@ pytestmark = pytest.mark.gpu
 GAS = GasModel(gamma=1.4, R=1.0, mu0=2e-3, T0=1 / 1.4, Ts=0.27, Pr_lam=0.72)
 
 
+@pytest.fixture(params=["fused", "staged"])
+def pipeline(request, cuda_device):
+    """Runs a test on the fused single-kernel stage and on the staged pipeline."""
+    from famrdp_jax_b200 import _capi
+    _capi.set_pipeline(request.param)
+    yield request.param
+    _capi.set_pipeline("fused")
+
+
 def _cfg(topology=(), bc_params=None, limiter="minmod", gas=GAS, precision="f64"):
     return Config(gas=gas, scheme=SchemeChoice("muscl2", "roe", 3, limiter), bc_params=bc_params or {},
                   topology=topology, ghost=2, nan_check=False, precision=precision)
@@ -103,7 +112,7 @@ def test_limiters_and_muscl(cuda_device):
 # ---------------------------------------------------------------- RHS
 @pytest.mark.parametrize("shape,seed", [((12, 10, 9), 0), ((7, 16, 6), 1), ((9, 5, 21), 2)])
 @pytest.mark.parametrize("limiter", ["minmod", "vanleer"])
-def test_invscd_rhs_parity(cuda_device, shape, seed, limiter):
+def test_invscd_rhs_parity(cuda_device, pipeline, shape, seed, limiter):
     q, kxyz, vol = random_block(shape, seed)
     m = Metrics(jac=dev(vol), kxyz=dev(kxyz), vol=dev(vol))
     got = host(compute_invscd_rhs(dev(q), m, ghost=2, gamma=1.4, reconstruct="muscl2", flux="roe",
@@ -114,7 +123,7 @@ def test_invscd_rhs_parity(cuda_device, shape, seed, limiter):
 
 @pytest.mark.parametrize("visc_law", ["sutherland", "constant"])
 @pytest.mark.parametrize("shape,seed", [((12, 10, 9), 0), ((5, 7, 6), 4)])
-def test_viscous_rhs_parity(cuda_device, shape, seed, visc_law):
+def test_viscous_rhs_parity(cuda_device, pipeline, shape, seed, visc_law):
     q, kxyz, vol = random_block(shape, seed)
     gas = GasModel(gamma=1.4, R=1.0, mu0=2e-3, T0=1 / 1.4, Ts=0.27, Pr_lam=0.72, visc_law=visc_law)
     m = Metrics(jac=dev(vol), kxyz=dev(kxyz), vol=dev(vol))
@@ -124,7 +133,7 @@ def test_viscous_rhs_parity(cuda_device, shape, seed, visc_law):
     assert rel_l2(got, ref) <= 1e-11
 
 
-def test_rhs_block_parity_and_reference_invariants(cuda_device):
+def test_rhs_block_parity_and_reference_invariants(cuda_device, pipeline):
     q, kxyz, vol = random_block((11, 9, 13), 7)
     m = Metrics(jac=dev(vol), kxyz=dev(kxyz), vol=dev(vol))
     cfg = _cfg()
@@ -148,6 +157,26 @@ def test_rhs_block_parity_and_reference_invariants(cuda_device):
     qs[0], qs[4] = rho, p / 0.4
     r = host(compute_viscous_rhs(dev(qs), mi, gas=GasModel(), ghost=2))
     np.testing.assert_allclose(r[:, 4:-4, 4:-4, 4:-4], 0.0, atol=1e-10)
+
+
+@pytest.mark.parametrize("seg", [1, 2, 5, 0])
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_fused_segments_and_ragged_tiles(cuda_device, seg, precision):
+    """Segment lengths along i and tiles that overhang the block in j and k."""
+    from famrdp_jax_b200 import _capi
+    q, kxyz, vol = random_block((13, 19, 41), 9)
+    m = Metrics(jac=dev(vol), kxyz=dev(kxyz), vol=dev(vol))
+    cfg = _cfg(precision=precision)
+    _capi.set_pipeline("staged")
+    ref = host(_rhs_block(dev(q), m, cfg))
+    _capi.set_pipeline("fused", seg=seg)
+    try:
+        got = host(_rhs_block(dev(q), m, cfg))
+    finally:
+        _capi.set_pipeline("fused")
+    assert rel_l2(got, ref) <= (1e-12 if precision == "f64" else 1e-5)
+    if precision == "f64":
+        assert rel_l2(got, NP.rhs_block(q, kxyz, vol, cfg)) <= 1e-11
 
 
 # ---------------------------------------------------------------- halo + BC
@@ -255,7 +284,7 @@ def _run_steps(case, nsteps, dt, tol_fp64=1e-12):
     return errs, st
 
 
-def test_step_tgv32_ten_steps_fp64(cuda_device):
+def test_step_tgv32_ten_steps_fp64(cuda_device, pipeline):
     """Config: 32^3 TGV, M0 = 0.1, Re = 1600, constant viscosity, CFL 0.5, 10 steps."""
     c = cases.tgv(n=32)
     dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], c.cfg.gas.gamma, c.cfl, 2)
@@ -264,21 +293,21 @@ def test_step_tgv32_ten_steps_fp64(cuda_device):
     assert st.step == 10 and abs(st.t - 10 * dt) < 1e-15
 
 
-def test_step_wavy4_fp64(cuda_device):
+def test_step_wavy4_fp64(cuda_device, pipeline):
     c = cases.wavy4(n=12, metrics_fn=lambda x: NP.compute_metrics(x, ghost=2))
     dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], c.cfg.gas.gamma, c.cfl, 2)
     errs, _ = _run_steps(c, 3, dt)
     assert max(errs) <= 1e-12, errs
 
 
-def test_step_tree_with_farfield_fp64(cuda_device):
+def test_step_tree_with_farfield_fp64(cuda_device, pipeline):
     c = cases.tree24(nblocks=6, lo=6, hi=12, seed=1)
     dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], c.cfg.gas.gamma, c.cfl, 2)
     errs, _ = _run_steps(c, 3, dt)
     assert max(errs) <= 1e-12, errs
 
 
-def test_step_fp32_flux_tgv(cuda_device):
+def test_step_fp32_flux_tgv(cuda_device, pipeline):
     c = cases.tgv(n=32, precision="f32")
     dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], c.cfg.gas.gamma, c.cfl, 2)
     errs, _ = _run_steps(c, 10, dt)

@@ -51,7 +51,9 @@ def test_noalloc_rhs_matches_context_rhs_twice(cuda_device, precision):
         assert status == _capi.FJ_OK, _capi.lib().fj_status_string(status)
         ref = _rhs_with_context(qd, kd, vd, p)
         torch.cuda.synchronize()
-        assert rel_l2(host(got), host(ref)) <= 1e-11
+        # the RHS tolerances of the parity tests: FP64 fluxes agree to 1e-11; two
+        # FP32-flux evaluations differ by FP32 rounding, bounded like FP32 vs FP64
+        assert rel_l2(host(got), host(ref)) <= (1e-11 if precision == "f64" else 1e-5)
 
 
 def test_noalloc_rejects_blocks_beyond_capacity(cuda_device):
