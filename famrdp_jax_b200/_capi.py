@@ -69,7 +69,11 @@ SIGNATURES = {
     "fj_ctx_destroy": (_I, [_P]),
     "fj_last_error": (ctypes.c_char_p, [_P]),
     "fj_launch_count": (_I, [_P, ctypes.POINTER(_I64)]),
-    "fj_ctx_set_pipeline": (_I, [_P, _I, _I]),
+    "fj_ctx_set_pipeline": (_I, [_P, _I, _I, _I]),
+    "fj_plan_create": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjLink), _I, ctypes.POINTER(FjBc), _I,
+                            ctypes.POINTER(FjParams), ctypes.POINTER(_P)]),
+    "fj_plan_step": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
+    "fj_plan_destroy": (_I, [_P]),
     "fj_rk_stage_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _D, _I, _P]),
     "fj_cons_to_prim_f64": (_I, [_P, _P, _I64, _D, _P]),
     "fj_prim_to_cons_f64": (_I, [_P, _P, _I64, _D, _P]),
@@ -135,14 +139,24 @@ def ctx(device: torch.device | int | None = None) -> int:
     return h
 
 
-PIPELINES = {"fused": 0, "staged": 1}
+PIPELINES = {"fused": 0, "staged": 1, "split": 2}
 
 
-def set_pipeline(pipeline: str = "fused", seg: int = 0, device=None) -> None:
-    """Fused single-kernel stages (default) or the staged four-kernel pipeline;
-    ``seg`` = planes per CTA along i for the fused kernel (0 = automatic)."""
+TILES = {"8x32": 0, "4x32": 1, "6x32": 2, "8x16": 3, "16x32": 4, "8x64": 5, "16x16": 6}
+
+
+DEFAULT_PIPELINE = "split"
+
+
+def set_pipeline(pipeline: str = DEFAULT_PIPELINE, seg: int = 0, tile: str | int = 0, device=None) -> None:
+    """How RHS / RK stages are evaluated: "split" (default: three barrier-free
+    kernels per stage over all blocks), "fused" (one shared-memory streaming
+    kernel per stage and block) or "staged" (the six-kernel cross-check); for
+    the fused kernel ``seg`` = planes per CTA along i (0 = automatic) and
+    ``tile`` the (j, k) tile shape."""
     c = ctx(device)
-    check(lib().fj_ctx_set_pipeline(c, PIPELINES[pipeline], int(seg)), "fj_ctx_set_pipeline", c)
+    t = TILES[tile] if isinstance(tile, str) else int(tile)
+    check(lib().fj_ctx_set_pipeline(c, PIPELINES[pipeline], int(seg), t), "fj_ctx_set_pipeline", c)
 
 
 def launch_count(device=None) -> int:

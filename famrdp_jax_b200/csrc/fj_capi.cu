@@ -8,6 +8,7 @@
 #include "famrdp_cuda.h"
 #include "fj_common.cuh"
 #include "fj_rhs.cuh"
+#include "fj_split.cuh"
 #include "fj_stage.cuh"
 
 namespace fj {
@@ -23,6 +24,7 @@ int pw_rk3_combine(const double* q0, const double* qs, const double* Lr, double*
                    double dt, int stage, cudaStream_t st);
 int pw_limiter(const double* a, const double* b, double* out, int64_t n, int limiter,
                cudaStream_t st);
+int convert_f64_f32(const double* in, float* out, int64_t n, cudaStream_t st);
 int reduce_cfl_dt(fj_ctx* ctx, const fj_block* blocks, int nblocks, double gamma, int g,
                   double cfl, double* dt_out, cudaStream_t st);
 int reduce_kinetic_energy(fj_ctx* ctx, const fj_block* blocks, int nblocks, int g, double* res,
@@ -39,24 +41,46 @@ inline cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// Scratch of one RHS/stage evaluation: none for the fused kernel, the
-// intermediates for the staged pipeline.
+// Scratch of one RHS/stage evaluation of one block: none for the fused
+// kernel, the intermediates for the split and staged pipelines.
 size_t rhs_scratch_bytes(const fj_ctx* ctx, int precision, int ni, int nj, int nk) {
   if (ctx->pipeline == FJ_PIPELINE_FUSED) return 0;
+  if (ctx->pipeline == FJ_PIPELINE_SPLIT) return split_scratch_bytes(precision, (int64_t)ni * nj * nk);
   return precision == FJ_PREC_F32FLUX ? staged_ws_bytes<float>(ni, nj, nk)
                                       : staged_ws_bytes<double>(ni, nj, nk);
 }
 
+SplitBlock split_block(const double* q, const double* q0, double* out, const double* kxyz,
+                       const float* kxyz32, const double* vol, int ni, int nj, int nk) {
+  SplitBlock b{};
+  b.q = q;
+  b.q0 = q0;
+  b.out = out;
+  b.kxyz = kxyz;
+  b.kxyz32 = kxyz32;
+  b.vol = vol;
+  b.ni = ni;
+  b.nj = nj;
+  b.nk = nk;
+  return b;
+}
+
 int run_rhs(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
             const double* q0, double* out, int ni, int nj, int nk, const fj_params* p, int flags,
-            int stage, double dt, void* ws, cudaStream_t st) {
+            int stage, double dt, void* ws, cudaStream_t st, const float* kxyz32 = nullptr) {
   Phys ph = make_phys(p);
+  if (ctx->pipeline == FJ_PIPELINE_SPLIT) {
+    SplitBlock b = split_block(q, q0, out, kxyz, p->precision == FJ_PREC_F32FLUX ? kxyz32 : nullptr,
+                               vol, ni, nj, nk);
+    split_assign_scratch(p->precision, &b, 1, ws);
+    return split_stage(ctx, &b, 1, ph, flags, stage, dt, p->precision, st);
+  }
   if (ctx->pipeline == FJ_PIPELINE_FUSED) {
     StageArgs a{};
     a.q = q;
     a.q0 = q0;
     a.kxyz = kxyz;
-    a.kxyz32 = nullptr;
+    a.kxyz32 = p->precision == FJ_PREC_F32FLUX ? kxyz32 : nullptr;
     a.vol = vol;
     a.out = out;
     a.ni = ni;
@@ -66,7 +90,7 @@ int run_rhs(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
     a.stage = stage;
     a.dt = dt;
     a.ph = ph;
-    return fused_stage(ctx, a, ctx->seg, p->precision, st);
+    return fused_stage(ctx, a, ctx->seg, p->precision, ctx->tile, st);
   }
   if (p->precision == FJ_PREC_F32FLUX)
     return staged_rhs<float>(ctx, q, kxyz, vol, q0, out, ni, nj, nk, ph, flags, stage, dt, ws, st);
@@ -94,6 +118,114 @@ int check_blockset(fj_ctx* ctx, const fj_block* blocks, int nblocks, bool need_m
     if (need_metrics && (!blocks[b].kxyz || !blocks[b].vol))
       return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "block metrics are NULL");
     int s = check_dims(ctx, blocks[b].ni, blocks[b].nj, blocks[b].nk);
+    if (s != FJ_OK) return s;
+  }
+  return FJ_OK;
+}
+
+
+int check_step_args(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int nblocks,
+                    const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs, const fj_params* p) {
+  int s = check_params(ctx, p);
+  if (s != FJ_OK) return s;
+  s = check_blockset(ctx, blocks, nblocks, true);
+  if (s != FJ_OK) return s;
+  if (!q_out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "q_out is NULL");
+  if (nlinks < 0 || (nlinks > 0 && !links) || nbcs < 0 || (nbcs > 0 && !bcs))
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bad link or bc list");
+  for (int L = 0; L < nlinks; ++L)
+    if (links[L].tgt_block < 0 || links[L].tgt_block >= nblocks || links[L].tgt_face < 0 ||
+        links[L].tgt_face > 5)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "link target out of range");
+  for (int b = 0; b < nblocks; ++b)
+    if (!q_out[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "q_out entry is NULL");
+  return FJ_OK;
+}
+
+// Scratch layout of one step: [q1 | q2 | tail].  The split pipeline runs all
+// blocks per launch, so q1/q2 hold every block and the tail every block's
+// intermediates; the other pipelines run block by block and size everything
+// for the largest block.  The halo slabs reuse the tail (the halo runs first).
+size_t step_layout(const fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
+                   int nlinks, const fj_params* p, size_t* stage_b, size_t* tail_b) {
+  size_t maxN = 0, sumStage = 0, rhs_b = 0;
+  int64_t cells = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    const size_t N = (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
+    maxN = std::max(maxN, N);
+    sumStage += align256(5 * N * sizeof(double));
+    cells += (int64_t)N;
+    rhs_b = std::max(rhs_b, rhs_scratch_bytes(ctx, p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
+  }
+  const bool split = ctx->pipeline == FJ_PIPELINE_SPLIT;
+  *stage_b = split ? sumStage : align256(5 * maxN * sizeof(double));
+  const size_t work = split ? split_scratch_bytes(p->precision, cells) : rhs_b;
+  *tail_b = align256(std::max(std::max(work, halo_ws_bytes(blocks, links, nlinks, p->ghost)), (size_t)256));
+  return 2 * *stage_b + *tail_b;
+}
+
+// solver/step.py:18-56 on the device: q_out := q, halo + BC in place on q_out,
+// then the three stages of each block (blocks do not interact between the halo
+// fill and the end of the step, solver/step.py:40-53).
+int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int nblocks,
+              const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs, const fj_params* p,
+              double dt, float* const* kxyz32, double* q1, double* q2, void* tail, size_t tail_b,
+              cudaStream_t st) {
+  std::vector<fj_block> out(blocks, blocks + nblocks);
+  int s;
+  for (int b = 0; b < nblocks; ++b) {
+    out[b].q = q_out[b];
+    if (q_out[b] != blocks[b].q) {
+      const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
+      s = cuda_status(ctx, cudaMemcpyAsync(q_out[b], blocks[b].q, bytes, cudaMemcpyDeviceToDevice, st),
+                      "state copy");
+      if (s != FJ_OK) return s;
+    }
+  }
+  s = halo_exchange(ctx, out.data(), nblocks, links, nlinks, p->ghost, (double*)tail, tail_b, st);
+  if (s != FJ_OK) return s;
+  s = apply_bc(ctx, out.data(), nblocks, bcs, nbcs, p, st);
+  if (s != FJ_OK) return s;
+  const int flags = kRhsInvscd | kRhsViscous;
+  if (ctx->pipeline == FJ_PIPELINE_SPLIT) {
+    // all blocks per launch: q1/q2 hold every block (step_layout), the tail
+    // holds the intermediates of every block
+    std::vector<SplitBlock> sb(nblocks);
+    std::vector<double*> b1(nblocks), b2(nblocks);
+    size_t off = 0;
+    for (int b = 0; b < nblocks; ++b) {
+      const fj_block& B = out[b];
+      b1[b] = (double*)((char*)q1 + off);
+      b2[b] = (double*)((char*)q2 + off);
+      off += align256(5 * (size_t)B.ni * B.nj * B.nk * sizeof(double));
+      sb[b] = split_block(B.q, B.q, b1[b], B.kxyz,
+                          (p->precision == FJ_PREC_F32FLUX && kxyz32) ? kxyz32[b] : nullptr, B.vol, B.ni,
+                          B.nj, B.nk);
+    }
+    split_assign_scratch(p->precision, sb.data(), nblocks, tail);
+    const Phys ph = make_phys(p);
+    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 1, dt, p->precision, st);
+    if (s != FJ_OK) return s;
+    for (int b = 0; b < nblocks; ++b) {
+      sb[b].q = b1[b];
+      sb[b].out = b2[b];
+    }
+    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 2, dt, p->precision, st);
+    if (s != FJ_OK) return s;
+    for (int b = 0; b < nblocks; ++b) {
+      sb[b].q = b2[b];
+      sb[b].out = out[b].q;
+    }
+    return split_stage(ctx, sb.data(), nblocks, ph, flags, 3, dt, p->precision, st);
+  }
+  for (int b = 0; b < nblocks; ++b) {
+    const fj_block& B = out[b];
+    const float* k32 = kxyz32 ? kxyz32[b] : nullptr;
+    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, q1, B.ni, B.nj, B.nk, p, flags, 1, dt, tail, st, k32);
+    if (s != FJ_OK) return s;
+    s = run_rhs(ctx, q1, B.kxyz, B.vol, B.q, q2, B.ni, B.nj, B.nk, p, flags, 2, dt, tail, st, k32);
+    if (s != FJ_OK) return s;
+    s = run_rhs(ctx, q2, B.kxyz, B.vol, B.q, B.q, B.ni, B.nj, B.nk, p, flags, 3, dt, tail, st, k32);
     if (s != FJ_OK) return s;
   }
   return FJ_OK;
@@ -142,13 +274,15 @@ int fj_ctx_destroy(fj_ctx* ctx) {
 
 const char* fj_last_error(const fj_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
-int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg) {
+int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg, int tile) {
   if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
-  if (pipeline != FJ_PIPELINE_FUSED && pipeline != FJ_PIPELINE_STAGED)
+  if (pipeline != FJ_PIPELINE_FUSED && pipeline != FJ_PIPELINE_STAGED && pipeline != FJ_PIPELINE_SPLIT)
     return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown pipeline");
   if (seg < 0) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "segment length must be >= 0");
+  if (tile < 0 || tile >= FJ_NUM_TILES) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown tile shape");
   ctx->pipeline = pipeline;
   ctx->seg = seg;
+  ctx->tile = tile;
   return FJ_OK;
 }
 
@@ -262,60 +396,96 @@ int fj_step_f64(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int n
                 const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs, const fj_params* p,
                 double dt, void* stream) {
   if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
-  int s = check_params(ctx, p);
+  int s = check_step_args(ctx, blocks, q_out, nblocks, links, nlinks, bcs, nbcs, p);
   if (s != FJ_OK) return s;
-  s = check_blockset(ctx, blocks, nblocks, true);
-  if (s != FJ_OK) return s;
-  if (!q_out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "q_out is NULL");
-  if (nlinks < 0 || (nlinks > 0 && !links) || nbcs < 0 || (nbcs > 0 && !bcs))
-    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bad link or bc list");
-  for (int L = 0; L < nlinks; ++L)
-    if (links[L].tgt_block < 0 || links[L].tgt_block >= nblocks || links[L].tgt_face < 0 ||
-        links[L].tgt_face > 5)
-      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "link target out of range");
-  cudaStream_t st = S(stream);
-  size_t maxN = 0, rhs_b = 0;
-  for (int b = 0; b < nblocks; ++b) {
-    if (!q_out[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "q_out entry is NULL");
-    maxN = std::max(maxN, (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk);
-    rhs_b = std::max(rhs_b, rhs_scratch_bytes(ctx, p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
-  }
-  const size_t stage_b = align256(5 * maxN * sizeof(double));
-  const size_t halo_b = halo_ws_bytes(blocks, links, nlinks, p->ghost);
-  s = ensure_ws(ctx, 2 * stage_b + std::max(rhs_b, halo_b));
+  size_t stage_b = 0, tail_b = 0;
+  s = ensure_ws(ctx, step_layout(ctx, blocks, nblocks, links, nlinks, p, &stage_b, &tail_b));
   if (s != FJ_OK) return s;
   double* q1 = (double*)ctx->ws;
   double* q2 = (double*)((char*)ctx->ws + stage_b);
   void* tail = (char*)ctx->ws + 2 * stage_b;
-  const size_t tail_b = ctx->ws_bytes - 2 * stage_b;
+  return step_body(ctx, blocks, q_out, nblocks, links, nlinks, bcs, nbcs, p, dt, nullptr, q1, q2, tail,
+                   tail_b, S(stream));
+}
 
-  // q0 := q (the functional copy), then halo + BC in place on q0
-  std::vector<fj_block> out(blocks, blocks + nblocks);
-  for (int b = 0; b < nblocks; ++b) {
-    out[b].q = q_out[b];
-    if (q_out[b] != blocks[b].q) {
-      const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
-      s = cuda_status(ctx, cudaMemcpyAsync(q_out[b], blocks[b].q, bytes, cudaMemcpyDeviceToDevice, st),
-                      "state copy");
-      if (s != FJ_OK) return s;
+int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                   const fj_bc* bcs, int nbcs, const fj_params* p, fj_plan** out) {
+  if (!ctx || !out) return FJ_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  std::vector<double*> dummy_out(nblocks > 0 ? nblocks : 1, nullptr);
+  for (int b = 0; b < nblocks; ++b) dummy_out[b] = blocks ? blocks[b].q : nullptr;
+  int s = check_step_args(ctx, blocks, dummy_out.data(), nblocks, links, nlinks, bcs, nbcs, p);
+  if (s != FJ_OK) return s;
+  fj_plan* pl = new (std::nothrow) fj_plan();
+  if (!pl) return FJ_ERR_NO_MEMORY;
+  pl->ctx = ctx;
+  pl->blocks.assign(blocks, blocks + nblocks);
+  pl->links.assign(links, links + nlinks);
+  pl->bcs.assign(bcs, bcs + nbcs);
+  pl->p = *p;
+  // the plan keeps the context's pipeline choice of its creation time
+  pl->pipeline = ctx->pipeline;
+  const size_t total = step_layout(ctx, blocks, nblocks, links, nlinks, p, &pl->stage_bytes, &pl->halo_bytes);
+  cudaError_t e = cudaMalloc(&pl->scratch, total);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete pl;
+    return set_err(ctx, FJ_ERR_NO_MEMORY, "plan scratch allocation failed");
+  }
+  if (p->precision == FJ_PREC_F32FLUX) {
+    pl->kxyz32.assign(nblocks, nullptr);
+    for (int b = 0; b < nblocks; ++b) {
+      const size_t n9 = 9 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
+      e = cudaMalloc(&pl->kxyz32[b], n9 * sizeof(float));
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        fj_plan_destroy(pl);
+        return set_err(ctx, FJ_ERR_NO_MEMORY, "plan FP32 metric allocation failed");
+      }
+      s = convert_f64_f32(blocks[b].kxyz, pl->kxyz32[b], (int64_t)n9, nullptr);
+      if (s != FJ_OK) {
+        fj_plan_destroy(pl);
+        return set_err(ctx, s, "plan FP32 metric conversion failed");
+      }
+    }
+    e = cudaStreamSynchronize(nullptr);
+    if (e != cudaSuccess) {
+      fj_plan_destroy(pl);
+      return cuda_status(ctx, e, "plan metric conversion");
     }
   }
-  s = halo_exchange(ctx, out.data(), nblocks, links, nlinks, p->ghost, (double*)tail, tail_b, st);
-  if (s != FJ_OK) return s;
-  s = apply_bc(ctx, out.data(), nblocks, bcs, nbcs, p, st);
-  if (s != FJ_OK) return s;
-  // Blocks do not interact between the halo fill and the end of the step
-  // (solver/step.py:40-53), so each block runs its three stages back to back.
-  const int flags = kRhsInvscd | kRhsViscous;
-  for (int b = 0; b < nblocks; ++b) {
-    const fj_block& B = out[b];
-    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, q1, B.ni, B.nj, B.nk, p, flags, 1, dt, tail, st);
-    if (s != FJ_OK) return s;
-    s = run_rhs(ctx, q1, B.kxyz, B.vol, B.q, q2, B.ni, B.nj, B.nk, p, flags, 2, dt, tail, st);
-    if (s != FJ_OK) return s;
-    s = run_rhs(ctx, q2, B.kxyz, B.vol, B.q, B.q, B.ni, B.nj, B.nk, p, flags, 3, dt, tail, st);
-    if (s != FJ_OK) return s;
+  *out = pl;
+  return FJ_OK;
+}
+
+int fj_plan_step(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, void* stream) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  fj_ctx* ctx = pl->ctx;
+  const int nb = (int)pl->blocks.size();
+  if (!q_in || !q_out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "q_in/q_out is NULL");
+  std::vector<fj_block> in(pl->blocks);
+  for (int b = 0; b < nb; ++b) {
+    if (!q_in[b] || !q_out[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "state pointer is NULL");
+    in[b].q = q_in[b];
   }
+  double* q1 = (double*)pl->scratch;
+  double* q2 = (double*)((char*)pl->scratch + pl->stage_bytes);
+  void* tail = (char*)pl->scratch + 2 * pl->stage_bytes;
+  const int saved = ctx->pipeline;
+  ctx->pipeline = pl->pipeline;  // the scratch was laid out for this pipeline
+  int s = step_body(ctx, in.data(), q_out, nb, pl->links.data(), (int)pl->links.size(), pl->bcs.data(),
+                    (int)pl->bcs.size(), &pl->p, dt, pl->kxyz32.empty() ? nullptr : pl->kxyz32.data(), q1, q2,
+                    tail, pl->halo_bytes, S(stream));
+  ctx->pipeline = saved;
+  return s;
+}
+
+int fj_plan_destroy(fj_plan* pl) {
+  if (!pl) return FJ_OK;
+  for (float* k : pl->kxyz32)
+    if (k) cudaFree(k);
+  if (pl->scratch) cudaFree(pl->scratch);
+  delete pl;
   return FJ_OK;
 }
 

@@ -7,6 +7,7 @@
 #include <stdio.h>
 
 #include <string>
+#include <vector>
 
 #include "famrdp_cuda.h"
 
@@ -18,8 +19,23 @@ struct fj_ctx {
   size_t red_bytes = 0;
   std::string last_error;
   int64_t launches = 0;      // kernels launched through this context
-  int pipeline = FJ_PIPELINE_FUSED;
+  int pipeline = FJ_PIPELINE_SPLIT;
   int seg = 0;               // fused kernel: planes per CTA along i (0 = automatic)
+  int tile = 0;              // fused kernel: tile shape index (FJ_NUM_TILES shapes)
+};
+
+// A prepared step of one block set (fj_plan_create): tables, the metric
+// pointers, FP32 metric copies for the FP32-flux path, and owned scratch.
+struct fj_plan {
+  fj_ctx* ctx = nullptr;
+  std::vector<fj_block> blocks;
+  std::vector<fj_link> links;
+  std::vector<fj_bc> bcs;
+  fj_params p{};
+  std::vector<float*> kxyz32;
+  void* scratch = nullptr;   // q1 | q2 | tail (intermediates, halo slabs)
+  size_t stage_bytes = 0, halo_bytes = 0;  // halo_bytes: size of the tail
+  int pipeline = 0;
 };
 
 namespace fj {

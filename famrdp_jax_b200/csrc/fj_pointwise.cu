@@ -80,6 +80,16 @@ int pw_limiter(const double* a, const double* b, double* out, int64_t n, int lim
   return cudaGetLastError() == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
 }
 
+__global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c < n) out[c] = (float)in[c];
+}
+
+int convert_f64_f32(const double* in, float* out, int64_t n, cudaStream_t st) {
+  k_f64_to_f32<<<grid_for(n), kThreads, 0, st>>>(in, out, n);
+  return cudaGetLastError() == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
+}
+
 __global__ void k_rk3_combine(const double* __restrict__ q0, const double* __restrict__ qs,
                               const double* __restrict__ Lr, double* __restrict__ out, int64_t n,
                               double dt, int stage) {

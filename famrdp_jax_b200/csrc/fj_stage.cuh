@@ -22,7 +22,9 @@ struct StageArgs {
   Phys ph;
 };
 
-// One fused launch for one block.  `seg` = planes per CTA along i (0 = all).
-int fused_stage(fj_ctx* ctx, const StageArgs& a, int seg, int precision, cudaStream_t st);
+// One fused launch for one block.  `seg` = planes per CTA along i (0 =
+// automatic); `tile` selects the (TJ, TK) tile shape: 0 = 8x32, 1 = 4x32,
+// 2 = 6x32, 3 = 8x16.
+int fused_stage(fj_ctx* ctx, const StageArgs& a, int seg, int precision, int tile, cudaStream_t st);
 
 }  // namespace fj

@@ -8,20 +8,22 @@
 //   P   ring of 4 planes of primitives (rho, u, v, w, p, T) on the tile plus a
 //       2-cell halo in j and k (indices wrap around the padded block, as the
 //       reference's jnp.roll does for the viscous terms);
+//   K   ring of 2 planes of metrics kxyz on the tile plus a 1-cell halo;
 //   G   ring of 3 planes of viscous flux components (tau_00 tau_01 tau_02
 //       tau_11 tau_12 tau_22 Ge_0 Ge_1 Ge_2) on the tile plus a 1-cell halo;
-//   FI, FJ, FK the Roe face fluxes of the current plane along i, j and k.
+//   FJ, FK the Roe face fluxes of the current plane along j and k
+// (the i-face flux of a column stays in its thread's registers).
 // Iteration i (two barriers):
-//   A  primitives of plane i+2                                       | sync
+//   A  primitives of plane i+2, metrics of plane i+1                 | sync
 //   B  one balanced work list: i faces (i|i+1), j and k faces of plane i,
-//      G of plane i+1                                                | sync
+//      G of plane i+1; each thread also reads its own cell's metrics  | sync
 //   C  per-cell assembly + stage combine of plane i.
 // The segment's first two iterations only fill the rings (i = ib-2, ib-1).
 //
 // Inputs are read from HBM once per stage (halo re-reads hit L2); the only
 // write is the stage result.  T is the flux arithmetic type: double (the
 // drop-in FP64 path) or float (FP32-flux path: state, volume reciprocal,
-// accumulation and combine stay FP64).
+// accumulation and combine stay FP64; metrics may come as an FP32 copy).
 #include "fj_common.cuh"
 #include "fj_physics.cuh"
 #include "fj_rhs.cuh"
@@ -31,68 +33,130 @@ namespace fj {
 
 namespace {
 
+// x mod n for the small overshoots of halo indices (|x| < a few n).
 __device__ __forceinline__ int wrap(int x, int n) {
-  int r = x % n;
-  return r < 0 ? r + n : r;
+  while (x < 0) x += n;
+  while (x >= n) x -= n;
+  return x;
 }
 
-__device__ __forceinline__ int slot4(int p) { return p & 3; }  // p >= -2 always; & keeps it in 0..3
+__device__ __forceinline__ int slot4(int p) { return p & 3; }  // two's complement: p mod 4
 __device__ __forceinline__ int slot3(int p) { return ((p % 3) + 3) % 3; }
 
 template <typename T, int TJ, int TK>
 struct Tile {
   static constexpr int NT = TJ * TK;
   static constexpr int HJ = TJ + 4, HK = TK + 4, HN = HJ * HK;  // primitive plane
-  static constexpr int GJ = TJ + 2, GK = TK + 2, GN = GJ * GK;  // viscous-flux plane
+  static constexpr int GJ = TJ + 2, GK = TK + 2, GN = GJ * GK;  // viscous-flux / metric plane
   static constexpr int NFI = NT, NFJ = (TJ + 1) * TK, NFK = TJ * (TK + 1);
   static constexpr int NW = NFI + NFJ + NFK + GN;                // phase-B work items
   static constexpr size_t kP = (size_t)4 * 6 * HN;
   static constexpr size_t kG = (size_t)3 * 9 * GN;
-  static constexpr size_t bytes() { return (kP + kG + 5 * (NFI + NFJ + NFK)) * sizeof(T); }
+  static constexpr size_t kK = (size_t)2 * 9 * GN;
+  static constexpr size_t bytes() { return (kP + kG + kK + 5 * (NFJ + NFK)) * sizeof(T); }
+  // CTAs per SM the launch bounds ask the register allocator to allow
+  static constexpr int kMinBlocks = sizeof(T) == 8 ? 1 : (NT <= 128 ? 3 : (NT <= 256 ? 2 : 1));
+  // per-thread points of the next plane's loads held in registers
+  static constexpr int NPP = (HN + NT - 1) / NT, NKP = (GN + NT - 1) / NT;
 };
 
-template <typename T>
-__device__ __forceinline__ T metric(const StageArgs& a, int64_t N, int lm, int64_t c) {
-  return a.kxyz32 ? (T)a.kxyz32[lm * N + c] : (T)a.kxyz[lm * N + c];
-}
-
-// Primitives of plane p on the tile + 2-halo into ring slot slot4(p).
+// Raw state of plane p on the tile + 2-halo: each thread loads its points
+// (t, t + NT, ...) into registers; store_plane turns them into primitives.
 template <typename T, int TJ, int TK>
-__device__ __forceinline__ void load_plane(const StageArgs& a, T* __restrict__ P, int p, int j0,
-                                           int k0) {
+__device__ __forceinline__ void issue_plane(const StageArgs& a, int p, int j0, int k0,
+                                            double (&qr)[Tile<T, TJ, TK>::NPP][5]) {
   using TL = Tile<T, TJ, TK>;
   const int64_t N = (int64_t)a.ni * a.nj * a.nk;
-  const int pi = wrap(p, a.ni);
+  const int64_t base = (int64_t)wrap(p, a.ni) * a.nj * a.nk;
+#pragma unroll
+  for (int s = 0; s < TL::NPP; ++s) {
+    const int t = threadIdx.x + s * TL::NT;
+    if (t < TL::HN) {
+      const int hj = t / TL::HK, hk = t - (t / TL::HK) * TL::HK;
+      const int j = wrap(j0 - 2 + hj, a.nj), k = wrap(k0 - 2 + hk, a.nk);
+      const double* qc = a.q + base + (int64_t)j * a.nk + k;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) qr[s][v] = __ldg(qc + v * N);
+    }
+  }
+}
+
+// Primitives (rho, u, v, w, p, T) of the issued plane into P ring slot slot4(p)
+// (physics/eos.py:12-17; T = p / max(rho R, 1e-300), rhs/viscous.py:36).
+template <typename T, int TJ, int TK>
+__device__ __forceinline__ void store_plane(const StageArgs& a, T* __restrict__ P, int p,
+                                            const double (&qr)[Tile<T, TJ, TK>::NPP][5]) {
+  using TL = Tile<T, TJ, TK>;
   T* dst = P + (size_t)slot4(p) * 6 * TL::HN;
-  const double gm1 = a.ph.gm1, inv_R = 1.0 / a.ph.R;
-  for (int t = threadIdx.x; t < TL::HN; t += TL::NT) {
-    const int hj = t / TL::HK, hk = t - hj * TL::HK;
-    const int j = wrap(j0 - 2 + hj, a.nj), k = wrap(k0 - 2 + hk, a.nk);
-    const int64_t c = ((int64_t)pi * a.nj + j) * a.nk + k;
-    const double r = a.q[c];
-    const double ir = 1.0 / r;
-    const double u = a.q[N + c] * ir, v = a.q[2 * N + c] * ir, w = a.q[3 * N + c] * ir;
-    const double p_ = gm1 * (a.q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));  // eos.py:12-17
-    // T = p / max(rho R, 1e-300) (rhs/viscous.py:36)
-    const double Tt = r * a.ph.R > 1e-300 ? p_ * ir * inv_R : p_ / 1e-300;
-    dst[t] = (T)r;
-    dst[TL::HN + t] = (T)u;
-    dst[2 * TL::HN + t] = (T)v;
-    dst[3 * TL::HN + t] = (T)w;
-    dst[4 * TL::HN + t] = (T)p_;
-    dst[5 * TL::HN + t] = (T)Tt;
+  const double gm1 = a.ph.gm1, R = a.ph.R, inv_R = 1.0 / a.ph.R;
+#pragma unroll
+  for (int s = 0; s < TL::NPP; ++s) {
+    const int t = threadIdx.x + s * TL::NT;
+    if (t < TL::HN) {
+      const double r = qr[s][0];
+      const double ir = 1.0 / r;
+      const double u = qr[s][1] * ir, v = qr[s][2] * ir, w = qr[s][3] * ir;
+      const double p_ = gm1 * (qr[s][4] - r * (0.5 * (u * u + v * v + w * w)));
+      const double Tt = r * R > 1e-300 ? p_ * ir * inv_R : p_ * 1e300;
+      dst[t] = (T)r;
+      dst[TL::HN + t] = (T)u;
+      dst[2 * TL::HN + t] = (T)v;
+      dst[3 * TL::HN + t] = (T)w;
+      dst[4 * TL::HN + t] = (T)p_;
+      dst[5 * TL::HN + t] = (T)Tt;
+    }
+  }
+}
+
+// Metrics of plane p on the tile + 1-halo into registers, then into K ring
+// slot p & 1.
+template <typename T, int TJ, int TK>
+__device__ __forceinline__ void issue_metrics(const StageArgs& a, int p, int j0, int k0,
+                                              T (&kr)[Tile<T, TJ, TK>::NKP][9]) {
+  using TL = Tile<T, TJ, TK>;
+  const int64_t N = (int64_t)a.ni * a.nj * a.nk;
+  const int64_t base = (int64_t)wrap(p, a.ni) * a.nj * a.nk;
+#pragma unroll
+  for (int s = 0; s < TL::NKP; ++s) {
+    const int t = threadIdx.x + s * TL::NT;
+    if (t < TL::GN) {
+      const int gj = t / TL::GK, gk = t - (t / TL::GK) * TL::GK;
+      const int64_t c = base + (int64_t)wrap(j0 - 1 + gj, a.nj) * a.nk + wrap(k0 - 1 + gk, a.nk);
+      if (a.kxyz32) {
+#pragma unroll
+        for (int lm = 0; lm < 9; ++lm) kr[s][lm] = (T)__ldg(a.kxyz32 + lm * N + c);
+      } else {
+#pragma unroll
+        for (int lm = 0; lm < 9; ++lm) kr[s][lm] = (T)__ldg(a.kxyz + lm * N + c);
+      }
+    }
   }
 }
 
 template <typename T, int TJ, int TK>
-__global__ void __launch_bounds__(TJ* TK, 1) k_stage_fused(const StageArgs a) {
+__device__ __forceinline__ void store_metrics(T* __restrict__ K, int p,
+                                              const T (&kr)[Tile<T, TJ, TK>::NKP][9]) {
+  using TL = Tile<T, TJ, TK>;
+  T* dst = K + (size_t)(p & 1) * 9 * TL::GN;
+#pragma unroll
+  for (int s = 0; s < TL::NKP; ++s) {
+    const int t = threadIdx.x + s * TL::NT;
+    if (t < TL::GN) {
+#pragma unroll
+      for (int lm = 0; lm < 9; ++lm) dst[lm * TL::GN + t] = kr[s][lm];
+    }
+  }
+}
+
+template <typename T, int TJ, int TK>
+__global__ void __launch_bounds__(TJ* TK, (Tile<T, TJ, TK>::kMinBlocks)) k_stage_fused(const StageArgs a) {
   using TL = Tile<T, TJ, TK>;
   using M = FastMath<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* P = (T*)smem_raw;
   T* G = P + TL::kP;
-  T* FI = G + TL::kG;
-  T* FJ = FI + 5 * TL::NFI;
+  T* K = G + TL::kG;
+  T* FJ = K + TL::kK;
   T* FK = FJ + 5 * TL::NFJ;
 
   const int tile = blockIdx.x;
@@ -107,67 +171,165 @@ __global__ void __launch_bounds__(TJ* TK, 1) k_stage_fused(const StageArgs a) {
   const int ni = a.ni, nj = a.nj, nk = a.nk;
   const bool do_inv = (a.flags & kRhsInvscd) != 0, do_vis = (a.flags & kRhsViscous) != 0;
   const T gm1 = (T)a.ph.gm1, inv_gm1 = (T)(1.0 / a.ph.gm1), eps_e = (T)a.ph.eps_entropy;
-  const T mu0 = (T)a.ph.mu0, T0 = (T)a.ph.T0, Ts = (T)a.ph.Ts;
+  const T mu0 = (T)a.ph.mu0, Ts = (T)a.ph.Ts;
   const T inv_T0 = (T)(1.0 / a.ph.T0), sfac = (T)(a.ph.T0 + a.ph.Ts);
   const T kap_fac = (T)(a.ph.cp / a.ph.Pr);
   const T third = (T)(1.0 / 3.0);
-
-  load_plane<T, TJ, TK>(a, P, ib - 2, j0, k0);
-  load_plane<T, TJ, TK>(a, P, ib - 1, j0, k0);
+  const int gown = (lj + 1) * TL::GK + (lk + 1);
 
   T Fprev[5] = {T(0), T(0), T(0), T(0), T(0)};
+  T Fnext[5] = {T(0), T(0), T(0), T(0), T(0)};
+  T kown[9];
+
+  // C: assembly + stage combine of plane i (face fluxes from the previous
+  // phase B: Fnext = face i|i+1, Fprev = face i-1|i, FJ/FK, G ring, kown)
+  auto assemble = [&](const int i) {
+    if (active) {
+      const int64_t c = ((int64_t)i * nj + j) * nk + k;
+      double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      if (do_inv) {
+        // face-flux differences along i, j, k (cells [2, n-3] of each axis);
+        // summed in T, then scaled by 1/(vol + 1e-300) in FP64
+        const bool ii = i >= 2 && i <= ni - 3, jj = j >= 2 && j <= nj - 3, kk = k >= 2 && k <= nk - 3;
+        const int jR = (lj + 1) * TK + lk, jL = lj * TK + lk;
+        const int kR = lj * (TK + 1) + lk + 1, kL = lj * (TK + 1) + lk;
+        const double ivd = 1.0 / (a.vol[c] + 1e-300);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          double dsum;
+          if (sizeof(T) == sizeof(double)) {
+            // FP64: accumulate axis by axis like the reference
+            dsum = 0.0;
+            if (ii) dsum += (double)(Fnext[v] - Fprev[v]);
+            if (jj) dsum += (double)(FJ[v * TL::NFJ + jR] - FJ[v * TL::NFJ + jL]);
+            if (kk) dsum += (double)(FK[v * TL::NFK + kR] - FK[v * TL::NFK + kL]);
+          } else {
+            T s = T(0);
+            if (ii) s += Fnext[v] - Fprev[v];
+            if (jj) s += FJ[v * TL::NFJ + jR] - FJ[v * TL::NFJ + jL];
+            if (kk) s += FK[v * TL::NFK + kR] - FK[v * TL::NFK + kL];
+            dsum = (double)s;
+          }
+          r[v] = -dsum * ivd;
+        }
+      }
+      if (do_vis) {
+        const T* Gm = G + (size_t)slot3(i - 1) * 9 * TL::GN;
+        const T* Gc = G + (size_t)slot3(i) * 9 * TL::GN;
+        const T* Gp = G + (size_t)slot3(i + 1) * 9 * TL::GN;
+        // rows 0..2: momentum (tau row e), row 3: energy
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          T res = T(0);
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) {
+            int comp;
+            if (e == 3) {
+              comp = 6 + jj;
+            } else {
+              const int lo = e < jj ? e : jj, hi = e < jj ? jj : e;
+              comp = lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+            }
+            const size_t o = (size_t)comp * TL::GN + gown;
+            res += T(0.5) * ((Gp[o] - Gm[o]) * kown[jj] + (Gc[o + TL::GK] - Gc[o - TL::GK]) * kown[3 + jj] +
+                             (Gc[o + 1] - Gc[o - 1]) * kown[6 + jj]);
+          }
+          r[e + 1] += (double)res;
+        }
+      }
+      if (a.stage == 0) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) a.out[v * N + c] = r[v];
+      } else {
+        const double ca = a.stage == 2 ? 0.75 : 1.0 / 3.0;
+        const double cb = a.stage == 2 ? 0.25 : 2.0 / 3.0;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const int64_t o = v * N + c;
+          const double t = a.q[o] + a.dt * r[v];
+          a.out[o] = a.stage == 1 ? t : ca * a.q0[o] + cb * t;
+        }
+      }
+    }
+  };
+
+  {
+    double qr[TL::NPP][5];
+    T kr[TL::NKP][9];
+    issue_plane<T, TJ, TK>(a, ib - 2, j0, k0, qr);
+    store_plane<T, TJ, TK>(a, P, ib - 2, qr);
+    issue_plane<T, TJ, TK>(a, ib - 1, j0, k0, qr);
+    store_plane<T, TJ, TK>(a, P, ib - 1, qr);
+    issue_metrics<T, TJ, TK>(a, ib - 2, j0, k0, kr);
+    store_metrics<T, TJ, TK>(K, ib - 2, kr);
+  }
+
   for (int i = ib - 2; i < ie; ++i) {
-    // ---- A: primitives of plane i+2
-    load_plane<T, TJ, TK>(a, P, i + 2, j0, k0);
+    // ---- A: loads of plane i+2 (state) and i+1 (metrics) in flight while
+    //      the previous plane is assembled (C of plane i-1), then stored
+    {
+      double qr[TL::NPP][5];
+      T kr[TL::NKP][9];
+      issue_plane<T, TJ, TK>(a, i + 2, j0, k0, qr);
+      issue_metrics<T, TJ, TK>(a, i + 1, j0, k0, kr);
+      if (i - 1 >= ib) assemble(i - 1);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) Fprev[v] = Fnext[v];
+      store_plane<T, TJ, TK>(a, P, i + 2, qr);
+      store_metrics<T, TJ, TK>(K, i + 1, kr);
+    }
     __syncthreads();
 
     // ---- B: faces of plane i, viscous fluxes of plane i+1 (one work list)
+    const T* Ki = K + (size_t)(i & 1) * 9 * TL::GN;
+    const T* Kn = K + (size_t)((i + 1) & 1) * 9 * TL::GN;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Fnext[v] = T(0);
+#pragma unroll
+    for (int lm = 0; lm < 9; ++lm) kown[lm] = Ki[lm * TL::GN + gown];
     for (int w = threadIdx.x; w < TL::NW; w += TL::NT) {
       if (w < TL::NFI + TL::NFJ + TL::NFK) {
-        // face item: decode (cells c0..c3 in P, normal cells cl/cr, axis, output)
-        int ax, h0, hstep, ps0, fi_out;
-        int64_t cl;
+        // face item: cells c0..c3 in P, the two adjacent cells' metric rows in K
+        int ax, h0, hstep, ps0, gl, gstep, o_idx;
         bool valid;
-        T* out;
-        int ostride;
+        const T* Kl;
         if (w < TL::NFI) {  // i face between planes i and i+1, column w
           const int wj = w / TK, wk = w - (w / TK) * TK;
-          const int jj = j0 + wj, kk = k0 + wk;
-          valid = do_inv && jj < nj && kk < nk && i >= ib - 1 && i - 1 >= 0 && i - 1 <= ni - 4;
+          valid = do_inv && j0 + wj < nj && k0 + wk < nk && i >= ib - 1 && i - 1 >= 0 && i - 1 <= ni - 4;
           ax = 0;
           h0 = (wj + 2) * TL::HK + wk + 2;
           hstep = 0;
           ps0 = i - 1;
-          cl = ((int64_t)i * nj + jj) * nk + kk;
-          out = FI;
-          ostride = TL::NFI;
-          fi_out = w;
+          gl = (wj + 1) * TL::GK + wk + 1;
+          gstep = 0;
+          Kl = Ki;
+          o_idx = -1;
         } else if (w < TL::NFI + TL::NFJ) {  // j face between j0-1+fj and j0+fj
           const int t = w - TL::NFI;
           const int fj = t / TK, fk = t - (t / TK) * TK;
-          const int jl = j0 - 1 + fj, kc = k0 + fk;
-          valid = do_inv && i >= ib && jl - 1 >= 0 && jl - 1 <= nj - 4 && kc < nk;
+          const int jl = j0 - 1 + fj;
+          valid = do_inv && i >= ib && jl - 1 >= 0 && jl - 1 <= nj - 4 && k0 + fk < nk;
           ax = 1;
           h0 = fj * TL::HK + fk + 2;
           hstep = TL::HK;
           ps0 = i;
-          cl = ((int64_t)i * nj + jl) * nk + kc;
-          out = FJ;
-          ostride = TL::NFJ;
-          fi_out = t;
+          gl = fj * TL::GK + fk + 1;
+          gstep = TL::GK;
+          Kl = Ki;
+          o_idx = t;
         } else {  // k face between k0-1+fk and k0+fk
           const int t = w - TL::NFI - TL::NFJ;
           const int fj = t / (TK + 1), fk = t - (t / (TK + 1)) * (TK + 1);
-          const int kl = k0 - 1 + fk, jr = j0 + fj;
-          valid = do_inv && i >= ib && kl - 1 >= 0 && kl - 1 <= nk - 4 && jr < nj;
+          const int kl = k0 - 1 + fk;
+          valid = do_inv && i >= ib && kl - 1 >= 0 && kl - 1 <= nk - 4 && j0 + fj < nj;
           ax = 2;
           h0 = (fj + 2) * TL::HK + fk;
           hstep = 1;
           ps0 = i;
-          cl = ((int64_t)i * nj + jr) * nk + kl;
-          out = FK;
-          ostride = TL::NFK;
-          fi_out = t;
+          gl = (fj + 1) * TL::GK + fk;
+          gstep = 1;
+          Kl = Ki;
+          o_idx = t;
         }
         T F[5] = {T(0), T(0), T(0), T(0), T(0)};
         if (valid) {
@@ -182,14 +344,23 @@ __global__ void __launch_bounds__(TJ* TK, 1) k_stage_fused(const StageArgs a) {
             cell[s].w = ps[3 * TL::HN];
             cell[s].p = ps[4 * TL::HN];
           }
-          const int64_t cr = cl + (ax == 0 ? (int64_t)nj * nk : (ax == 1 ? nk : 1));
-          invscd_face_fast<T>(cell, metric<T>(a, N, 3 * ax, cl), metric<T>(a, N, 3 * ax + 1, cl),
-                              metric<T>(a, N, 3 * ax + 2, cl), metric<T>(a, N, 3 * ax, cr),
-                              metric<T>(a, N, 3 * ax + 1, cr), metric<T>(a, N, 3 * ax + 2, cr), gm1,
-                              inv_gm1, eps_e, a.ph.limiter, F);
+          const T* Kr = ax == 0 ? Kn : Kl;
+          const int gr = gl + gstep;
+          const int m0 = 3 * ax * TL::GN;
+          invscd_face_fast<T>(cell, Kl[m0 + gl], Kl[m0 + TL::GN + gl], Kl[m0 + 2 * TL::GN + gl], Kr[m0 + gr],
+                              Kr[m0 + TL::GN + gr], Kr[m0 + 2 * TL::GN + gr], gm1, inv_gm1, eps_e,
+                              a.ph.limiter, F);
         }
+        if (o_idx < 0) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) out[v * ostride + fi_out] = F[v];
+          for (int v = 0; v < 5; ++v) Fnext[v] = F[v];
+        } else if (ax == 1) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) FJ[v * TL::NFJ + o_idx] = F[v];
+        } else {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) FK[v * TL::NFK + o_idx] = F[v];
+        }
       } else if (do_vis) {
         // viscous flux components at plane i+1, point (j0-1+gj, k0-1+gk)
         const int t = w - TL::NFI - TL::NFJ - TL::NFK;
@@ -197,8 +368,6 @@ __global__ void __launch_bounds__(TJ* TK, 1) k_stage_fused(const StageArgs a) {
         if ((gj == 0 || gj == TL::GJ - 1) && (gk == 0 || gk == TL::GK - 1)) continue;
         const int p = i + 1;
         const int h = (gj + 1) * TL::HK + (gk + 1);
-        const int jj = wrap(j0 - 1 + gj, nj), kk = wrap(k0 - 1 + gk, nk);
-        const int64_t c = ((int64_t)wrap(p, ni) * nj + jj) * nk + kk;
         const T* Pm = P + (size_t)slot4(p - 1) * 6 * TL::HN;
         const T* Pc = P + (size_t)slot4(p) * 6 * TL::HN;
         const T* Pp = P + (size_t)slot4(p + 1) * 6 * TL::HN;
@@ -211,15 +380,13 @@ __global__ void __launch_bounds__(TJ* TK, 1) k_stage_fused(const StageArgs a) {
           d[s][1] = T(0.5) * (Pc[o + h + TL::HK] - Pc[o + h - TL::HK]);
           d[s][2] = T(0.5) * (Pc[o + h + 1] - Pc[o + h - 1]);
         }
-        T kk9[9];
-#pragma unroll
-        for (int lm = 0; lm < 9; ++lm) kk9[lm] = metric<T>(a, N, lm, c);
         T g[4][3];
 #pragma unroll
         for (int s = 0; s < 4; ++s)
 #pragma unroll
           for (int m = 0; m < 3; ++m)
-            g[s][m] = d[s][0] * kk9[m] + d[s][1] * kk9[3 + m] + d[s][2] * kk9[6 + m];
+            g[s][m] = d[s][0] * Kn[m * TL::GN + t] + d[s][1] * Kn[(3 + m) * TL::GN + t] +
+                      d[s][2] * Kn[(6 + m) * TL::GN + t];
         const T u = Pc[TL::HN + h], v = Pc[2 * TL::HN + h], wv = Pc[3 * TL::HN + h];
         T mu = mu0;
         if (a.ph.visc_law == 0) {  // Sutherland (physics/eos.py:24-25)
@@ -249,77 +416,8 @@ __global__ void __launch_bounds__(TJ* TK, 1) k_stage_fused(const StageArgs a) {
     }
     __syncthreads();
 
-    // ---- C: assembly + stage combine of plane i
-    if (i >= ib && active) {
-      const int64_t c = ((int64_t)i * nj + j) * nk + k;
-      double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-      if (do_inv) {
-        const double ivd = 1.0 / (a.vol[c] + 1e-300);
-        if (i >= 2 && i <= ni - 3) {
-#pragma unroll
-          for (int v = 0; v < 5; ++v)
-            r[v] -= ((double)FI[v * TL::NFI + threadIdx.x] - (double)Fprev[v]) * ivd;
-        }
-        if (j >= 2 && j <= nj - 3) {
-          const int tR = (lj + 1) * TK + lk, tL = lj * TK + lk;
-#pragma unroll
-          for (int v = 0; v < 5; ++v)
-            r[v] -= ((double)FJ[v * TL::NFJ + tR] - (double)FJ[v * TL::NFJ + tL]) * ivd;
-        }
-        if (k >= 2 && k <= nk - 3) {
-          const int tR = lj * (TK + 1) + lk + 1, tL = lj * (TK + 1) + lk;
-#pragma unroll
-          for (int v = 0; v < 5; ++v)
-            r[v] -= ((double)FK[v * TL::NFK + tR] - (double)FK[v * TL::NFK + tL]) * ivd;
-        }
-      }
-      if (do_vis) {
-        T kk9[9];
-#pragma unroll
-        for (int lm = 0; lm < 9; ++lm) kk9[lm] = metric<T>(a, N, lm, c);
-        const T* Gm = G + (size_t)slot3(i - 1) * 9 * TL::GN;
-        const T* Gc = G + (size_t)slot3(i) * 9 * TL::GN;
-        const T* Gp = G + (size_t)slot3(i + 1) * 9 * TL::GN;
-        const int g = (lj + 1) * TL::GK + (lk + 1);
-        // rows 0..2: momentum (tau row e), row 3: energy
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          T res = T(0);
-#pragma unroll
-          for (int jj = 0; jj < 3; ++jj) {
-            int comp;
-            if (e == 3) {
-              comp = 6 + jj;
-            } else {
-              const int lo = e < jj ? e : jj, hi = e < jj ? jj : e;
-              comp = lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
-            }
-            const size_t o = (size_t)comp * TL::GN + g;
-            res += T(0.5) * ((Gp[o] - Gm[o]) * kk9[jj] + (Gc[o + TL::GK] - Gc[o - TL::GK]) * kk9[3 + jj] +
-                             (Gc[o + 1] - Gc[o - 1]) * kk9[6 + jj]);
-          }
-          r[e + 1] += (double)res;
-        }
-      }
-      if (a.stage == 0) {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) a.out[v * N + c] = r[v];
-      } else {
-        const double ca = a.stage == 1 ? 0.0 : (a.stage == 2 ? 0.75 : 1.0 / 3.0);
-        const double cb = a.stage == 1 ? 1.0 : (a.stage == 2 ? 0.25 : 2.0 / 3.0);
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const int64_t o = v * N + c;
-          const double t = a.q[o] + a.dt * r[v];
-          a.out[o] = a.stage == 1 ? t : ca * a.q0[o] + cb * t;
-        }
-      }
-    }
-    if (i >= ib - 1) {
-#pragma unroll
-      for (int v = 0; v < 5; ++v) Fprev[v] = FI[v * TL::NFI + threadIdx.x];
-    }
   }
+  if (ie - 1 >= ib) assemble(ie - 1);
 }
 
 template <typename T, int TJ, int TK>
@@ -351,9 +449,25 @@ int launch_tiled(fj_ctx* ctx, StageArgs a, int seg, cudaStream_t st) {
 
 }  // namespace
 
-int fused_stage(fj_ctx* ctx, const StageArgs& a, int seg, int precision, cudaStream_t st) {
-  if (precision == FJ_PREC_F32FLUX) return launch_tiled<float, 8, 32>(ctx, a, seg, st);
-  return launch_tiled<double, 8, 32>(ctx, a, seg, st);
+int fused_stage(fj_ctx* ctx, const StageArgs& a, int seg, int precision, int tile, cudaStream_t st) {
+  if (precision == FJ_PREC_F32FLUX) {
+    switch (tile) {
+      case 1: return launch_tiled<float, 4, 32>(ctx, a, seg, st);
+      case 2: return launch_tiled<float, 6, 32>(ctx, a, seg, st);
+      case 3: return launch_tiled<float, 8, 16>(ctx, a, seg, st);
+      case 4: return launch_tiled<float, 16, 32>(ctx, a, seg, st);
+      case 5: return launch_tiled<float, 8, 64>(ctx, a, seg, st);
+      case 6: return launch_tiled<float, 16, 16>(ctx, a, seg, st);
+      default: return launch_tiled<float, 8, 32>(ctx, a, seg, st);
+    }
+  }
+  // FP64 tiles must fit 227 KB of shared memory: the 512-thread shapes do not
+  switch (tile) {
+    case 1: return launch_tiled<double, 4, 32>(ctx, a, seg, st);
+    case 2: return launch_tiled<double, 6, 32>(ctx, a, seg, st);
+    case 3: case 6: return launch_tiled<double, 8, 16>(ctx, a, seg, st);
+    default: return launch_tiled<double, 8, 32>(ctx, a, seg, st);
+  }
 }
 
 }  // namespace fj

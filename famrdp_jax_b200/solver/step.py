@@ -8,6 +8,8 @@ call into libfamrdp_cuda.so (fj_step_f64).
 """
 from __future__ import annotations
 
+import ctypes
+
 import torch
 
 from famrdp_jax_b200 import _capi, _topology
@@ -48,8 +50,10 @@ def rk_stage(q: torch.Tensor, q0: torch.Tensor | None, metrics: Metrics, cfg: Co
 
 
 class StepPlan:
-    """The marshalled tables of one (state layout, cfg) pair, reusable across
-    steps whose blocks keep their shapes, metrics and device."""
+    """A prepared step (fj_plan) for one (block layout, metrics, cfg): tables
+    checked and uploaded once, FP32 metric copies built once for the FP32-flux
+    precision, scratch owned by the plan.  Reusable while the metrics and block
+    shapes stay the same."""
 
     def __init__(self, state: State, cfg: Config):
         if len(state.blocks) != len(cfg.topology):
@@ -58,17 +62,30 @@ class StepPlan:
         self.params = _params(cfg)
         self.links = _topology.links(cfg.topology)
         self.bcs = _topology.bcs(cfg.topology, cfg)
-        self.link_arr = _topology.link_array(self.links)
-        self.bc_arr = _topology.bc_array(self.bcs)
         self.metrics = state.metrics
         self.device = state.blocks[0].q.device
+        self.shapes = [tuple(b.q.shape) for b in state.blocks]
+        self._handle = None
+        c = _capi.ctx(self.device)
+        blocks = _topology.block_array([b.q for b in state.blocks], self.metrics)
+        h = ctypes.c_void_p()
+        _capi.check(_capi.lib().fj_plan_create(c, blocks, len(state.blocks), _topology.link_array(self.links),
+                                               len(self.links), _topology.bc_array(self.bcs), len(self.bcs),
+                                               self.params, ctypes.byref(h)), "fj_plan_create", c)
+        self._handle = h.value
+        self._lib = _capi.lib()
 
     def run(self, qs, outs, dt: float) -> None:
+        if [tuple(q.shape) for q in qs] != self.shapes or [tuple(o.shape) for o in outs] != self.shapes:
+            raise ValueError("state shapes differ from the plan's")
         c = _capi.ctx(self.device)
-        blocks = _topology.block_array(qs, self.metrics)
-        _capi.check(_capi.lib().fj_step_f64(c, blocks, _topology.ptr_array(outs), len(qs), self.link_arr,
-                                            len(self.links), self.bc_arr, len(self.bcs), self.params,
-                                            float(dt), _capi.stream(self.device)), "fj_step_f64", c)
+        _capi.check(self._lib.fj_plan_step(self._handle, _topology.ptr_array(qs), _topology.ptr_array(outs),
+                                           float(dt), _capi.stream(self.device)), "fj_plan_step", c)
+
+    def __del__(self):
+        if getattr(self, "_handle", None):
+            self._lib.fj_plan_destroy(self._handle)
+            self._handle = None
 
 
 def step(state: State, cfg: Config, dt: float, *, plan: StepPlan | None = None) -> State:

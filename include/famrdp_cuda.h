@@ -50,7 +50,7 @@ enum fj_status {
 /* Size of the fixed device scratch behind fj_rhs_noalloc_f64 (64 MiB). */
 #define FJ_NOALLOC_SCRATCH_BYTES (64u << 20)
 
-enum fj_pipeline { FJ_PIPELINE_FUSED = 0, FJ_PIPELINE_STAGED = 1 };
+enum fj_pipeline { FJ_PIPELINE_FUSED = 0, FJ_PIPELINE_STAGED = 1, FJ_PIPELINE_SPLIT = 2 };
 enum fj_visc_law { FJ_VISC_SUTHERLAND = 0, FJ_VISC_CONSTANT = 1 };
 enum fj_limiter { FJ_LIM_MINMOD = 0, FJ_LIM_VANLEER = 1 };
 enum fj_precision { FJ_PREC_F64 = 0, FJ_PREC_F32FLUX = 1 };
@@ -107,11 +107,17 @@ int fj_ctx_create(fj_ctx** out);             /* on the current CUDA device  */
 int fj_ctx_destroy(fj_ctx* ctx);
 const char* fj_last_error(const fj_ctx* ctx);
 /* Selects how the context evaluates RHS / RK stages (no counterpart in the
- * reference): FJ_PIPELINE_FUSED (default) runs one fused kernel per stage and
- * block; FJ_PIPELINE_STAGED runs the four-kernel pipeline through scratch
- * (kept as a cross-check).  `seg` = planes per CTA along i for the fused
- * kernel, 0 = chosen from the block size and the SM count. */
-int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg);
+ * reference): FJ_PIPELINE_SPLIT (default) runs three barrier-free kernels per
+ * stage over all blocks at once (primitives; face fluxes + viscous fluxes;
+ * assembly + combine) through scratch; FJ_PIPELINE_FUSED runs one
+ * shared-memory streaming kernel per stage and block; FJ_PIPELINE_STAGED runs
+ * the six-kernel reference decomposition (kept as a cross-check).  A plan
+ * keeps the pipeline chosen when it was created.  For the fused kernel, `seg` = planes per CTA
+ * along i (0 = chosen from the block size and the SM count) and `tile` picks
+ * the (j, k) tile shape, 0 .. FJ_NUM_TILES-1: 8x32, 4x32, 6x32, 8x16, 16x32,
+ * 8x64, 16x16 (the last three FP32-flux only; FP64 maps them to 8x32/8x16). */
+#define FJ_NUM_TILES 7
+int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg, int tile);
 /* Number of kernels launched through this context so far (instrumentation;
  * the reference has no counterpart). */
 int fj_launch_count(const fj_ctx* ctx, int64_t* out);
@@ -193,6 +199,21 @@ int fj_step_f64(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int n
 int fj_rk_stage_f64(fj_ctx* ctx, const double* q, const double* q0, const double* kxyz,
                     const double* vol, double* out, int ni, int nj, int nk, const fj_params* p,
                     double dt, int stage, void* stream);
+
+/* A prepared step (solver/step.py:18-56 for a fixed block set): the link and
+ * boundary tables are copied and checked once, the metrics are bound (they
+ * must stay valid and unchanged while the plan lives) and, for the FP32-flux
+ * precision, an FP32 copy of every block's kxyz is built.  The plan owns its
+ * scratch, so fj_plan_step allocates nothing.  Creation synchronises the
+ * device. */
+typedef struct fj_plan fj_plan;
+int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
+                   int nlinks, const fj_bc* bcs, int nbcs, const fj_params* p, fj_plan** out);
+/* One step: reads q_in[b] (unchanged) and writes q_out[b]; q_out[b] may equal
+ * q_in[b] (in-place step), but must not partially overlap any state. */
+int fj_plan_step(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,
+                 void* stream);
+int fj_plan_destroy(fj_plan* plan);
 
 /* time/rk.py:5-20 one Shu-Osher stage combine, elementwise over n values:
  *   stage 1: out = qs + dt*L

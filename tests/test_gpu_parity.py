@@ -38,13 +38,13 @@ pytestmark = pytest.mark.gpu
 GAS = GasModel(gamma=1.4, R=1.0, mu0=2e-3, T0=1 / 1.4, Ts=0.27, Pr_lam=0.72)
 
 
-@pytest.fixture(params=["fused", "staged"])
+@pytest.fixture(params=["split", "fused", "staged"])
 def pipeline(request, cuda_device):
-    """Runs a test on the fused single-kernel stage and on the staged pipeline."""
+    """Runs a test on each RHS/stage pipeline (split is the default)."""
     from famrdp_jax_b200 import _capi
     _capi.set_pipeline(request.param)
     yield request.param
-    _capi.set_pipeline("fused")
+    _capi.set_pipeline()
 
 
 def _cfg(topology=(), bc_params=None, limiter="minmod", gas=GAS, precision="f64"):
@@ -173,7 +173,7 @@ def test_fused_segments_and_ragged_tiles(cuda_device, seg, precision):
     try:
         got = host(_rhs_block(dev(q), m, cfg))
     finally:
-        _capi.set_pipeline("fused")
+        _capi.set_pipeline()
     assert rel_l2(got, ref) <= (1e-12 if precision == "f64" else 1e-5)
     if precision == "f64":
         assert rel_l2(got, NP.rhs_block(q, kxyz, vol, cfg)) <= 1e-11
