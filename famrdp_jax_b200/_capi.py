@@ -74,6 +74,7 @@ SIGNATURES = {
                             ctypes.POINTER(FjParams), ctypes.POINTER(_P)]),
     "fj_plan_step": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_destroy": (_I, [_P]),
+    "fj_plan_stage": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _I, _P]),
     "fj_rk_stage_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _D, _I, _P]),
     "fj_cons_to_prim_f64": (_I, [_P, _P, _I64, _D, _P]),
     "fj_prim_to_cons_f64": (_I, [_P, _P, _I64, _D, _P]),

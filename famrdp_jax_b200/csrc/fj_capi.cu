@@ -480,6 +480,41 @@ int fj_plan_step(fj_plan* pl, double* const* q_in, double* const* q_out, double 
   return s;
 }
 
+int fj_plan_stage(fj_plan* pl, double* const* q, double* const* q0, double* const* out, double dt,
+                  int stage, void* stream) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  fj_ctx* ctx = pl->ctx;
+  const int nb = (int)pl->blocks.size();
+  if (!q || !out || (stage > 1 && !q0)) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "NULL state list");
+  if (stage < 1 || stage > 3) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "stage must be 1, 2 or 3");
+  for (int b = 0; b < nb; ++b)
+    if (!q[b] || !out[b] || (stage > 1 && !q0[b]) || out[b] == q[b])
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bad state pointer");
+  void* tail = (char*)pl->scratch + 2 * pl->stage_bytes;
+  const int flags = kRhsInvscd | kRhsViscous;
+  const int saved = ctx->pipeline;
+  ctx->pipeline = pl->pipeline;
+  int s = FJ_OK;
+  if (pl->pipeline == FJ_PIPELINE_SPLIT) {
+    std::vector<SplitBlock> sb(nb);
+    for (int b = 0; b < nb; ++b) {
+      const fj_block& B = pl->blocks[b];
+      sb[b] = split_block(q[b], stage > 1 ? q0[b] : q[b], out[b], B.kxyz,
+                          pl->kxyz32.empty() ? nullptr : pl->kxyz32[b], B.vol, B.ni, B.nj, B.nk);
+    }
+    split_assign_scratch(pl->p.precision, sb.data(), nb, tail);
+    s = split_stage(ctx, sb.data(), nb, make_phys(&pl->p), flags, stage, dt, pl->p.precision, S(stream));
+  } else {
+    for (int b = 0; b < nb && s == FJ_OK; ++b) {
+      const fj_block& B = pl->blocks[b];
+      s = run_rhs(ctx, q[b], B.kxyz, B.vol, stage > 1 ? q0[b] : q[b], out[b], B.ni, B.nj, B.nk, &pl->p, flags,
+                  stage, dt, tail, S(stream), pl->kxyz32.empty() ? nullptr : pl->kxyz32[b]);
+    }
+  }
+  ctx->pipeline = saved;
+  return s;
+}
+
 int fj_plan_destroy(fj_plan* pl) {
   if (!pl) return FJ_OK;
   for (float* k : pl->kxyz32)

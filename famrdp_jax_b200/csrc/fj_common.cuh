@@ -125,6 +125,8 @@ inline int check_dims(fj_ctx* ctx, int ni, int nj, int nk) {
 // Physics constants passed by value to kernels.
 struct Phys {
   double gm1, eps_entropy, R, mu0, T0, Ts, cp, Pr;
+  // derived once on the host: 1/(gamma-1), 1/T0, T0+Ts, cp/Pr
+  double inv_gm1, inv_T0, sfac, kap_fac;
   int limiter, visc_law;
 };
 
@@ -139,6 +141,10 @@ inline Phys make_phys(const fj_params* p) {
   // kappa = cp * mu / Pr with cp = gamma R / (gamma - 1) (rhs/viscous.py:38-39)
   f.cp = p->gamma * p->R / (p->gamma - 1.0);
   f.Pr = p->Pr;
+  f.inv_gm1 = 1.0 / f.gm1;
+  f.inv_T0 = 1.0 / f.T0;
+  f.sfac = f.T0 + f.Ts;
+  f.kap_fac = f.cp / f.Pr;
   f.limiter = p->limiter;
   f.visc_law = p->visc_law;
   return f;

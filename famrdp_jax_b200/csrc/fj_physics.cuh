@@ -221,17 +221,23 @@ template <typename T> struct FastMath;
 template <> struct FastMath<double> {
   static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
   static __device__ __forceinline__ double sqrt_pos(double x) { return sqrt(x); }
+  static __device__ __forceinline__ double sqrt_nn(double x) { return sqrt(x); }
 };
 template <> struct FastMath<float> {
   static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
   // x must be > 0
   static __device__ __forceinline__ float sqrt_pos(float x) { return x * rsqrtf(x); }
+  // x >= 0
+  static __device__ __forceinline__ float sqrt_nn(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
 };
 
 // minmod(a, b) of muscl2.py:5-7 without sign products: the smaller-magnitude
-// argument when both have the same strict sign, else 0.
+// argument when both have the same strict sign (a*b > 0), else 0.  (For
+// |a*b| below the smallest normal the product rounds to 0 and the result is
+// 0 where the reference returns the tiny min(|a|, |b|).)
 template <typename T> __device__ __forceinline__ T minmod_sel(T a, T b) {
-  return (a > T(0) && b > T(0)) ? fj_min(a, b) : ((a < T(0) && b < T(0)) ? fj_max(a, b) : T(0));
+  const T m = fj_abs(a) < fj_abs(b) ? a : b;
+  return a * b > T(0) ? m : T(0);
 }
 
 template <typename T>
@@ -330,7 +336,7 @@ __device__ __forceinline__ void invscd_face_fast(const Prim<T> c[4], T kl0, T kl
   muscl2_fast(c[0].w, c[1].w, c[2].w, c[3].w, limiter, L.w, R.w);
   muscl2_fast(c[0].p, c[1].p, c[2].p, c[3].p, limiter, L.p, R.p);
   const T nf0 = T(0.5) * (kl0 + kr0), nf1 = T(0.5) * (kl1 + kr1), nf2 = T(0.5) * (kl2 + kr2);
-  const T nmag = fj_sqrt(nf0 * nf0 + nf1 * nf1 + nf2 * nf2) + Tiny<T>::nmag();
+  const T nmag = FastMath<T>::sqrt_nn(nf0 * nf0 + nf1 * nf1 + nf2 * nf2) + Tiny<T>::nmag();
   const T inv = FastMath<T>::rcp(nmag);
   roe_prim(L, R, nf0 * inv, nf1 * inv, nf2 * inv, gm1, inv_gm1, eps_entropy, F);
 #pragma unroll

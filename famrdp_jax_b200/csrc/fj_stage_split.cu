@@ -110,6 +110,51 @@ __device__ __forceinline__ T metric(const SplitBlock& B, int64_t N, int lm, int6
   return B.kxyz32 ? (T)__ldg(B.kxyz32 + lm * N + c) : (T)__ldg(B.kxyz + lm * N + c);
 }
 
+// Primitives (rho, u, v, w, p[, T]) of one cell from the field-major scratch.
+template <typename T>
+struct Cell6 {
+  T r, u, v, w, p, t;
+};
+
+template <typename T, bool WITH_T>
+__device__ __forceinline__ Cell6<T> load_cell(const T* __restrict__ P, int32_t N, int32_t c) {
+  Cell6<T> x;
+  x.r = P[c];
+  x.u = P[N + c];
+  x.v = P[2 * N + c];
+  x.w = P[3 * N + c];
+  x.p = P[4 * N + c];
+  x.t = WITH_T ? P[5 * N + c] : T(0);
+  return x;
+}
+
+// Roe face c | c+e_a from the primitives of c-e_a, c, c+e_a, c+2e_a and the
+// kxyz rows of c and c+e_a (rhs/invscd.py:62-100).
+template <typename T>
+__device__ __forceinline__ void face_from_cells(const Cell6<T>& a0, const Cell6<T>& a1, const Cell6<T>& a2,
+                                                const Cell6<T>& a3, const T kl[3], const T kr[3],
+                                                const Phys& ph, T F[5]) {
+  Prim<T> cell[4] = {{a0.r, a0.u, a0.v, a0.w, a0.p}, {a1.r, a1.u, a1.v, a1.w, a1.p},
+                     {a2.r, a2.u, a2.v, a2.w, a2.p}, {a3.r, a3.u, a3.v, a3.w, a3.p}};
+  invscd_face_fast<T>(cell, kl[0], kl[1], kl[2], kr[0], kr[1], kr[2], (T)ph.gm1, (T)ph.inv_gm1,
+                      (T)ph.eps_entropy, ph.limiter, F);
+}
+
+template <typename T>
+__device__ __forceinline__ void metric_row(const SplitBlock& B, int32_t N, int row, int32_t c, T k[3]) {
+  if (B.kxyz32) {
+    const float* K = B.kxyz32 + 3 * row * N;
+    k[0] = (T)__ldg(K + c);
+    k[1] = (T)__ldg(K + N + c);
+    k[2] = (T)__ldg(K + 2 * N + c);
+  } else {
+    const double* K = B.kxyz + 3 * row * N;
+    k[0] = (T)__ldg(K + c);
+    k[1] = (T)__ldg(K + N + c);
+    k[2] = (T)__ldg(K + 2 * N + c);
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kSplitThreads) k_split_fluxes(const Table tab, const Phys ph,
                                                                const int flags) {
@@ -118,44 +163,48 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_fluxes(const Table tab,
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
-  const int64_t N = x.N, c = x.c;
-  const int64_t si = (int64_t)x.nj * x.nk, sj = x.nk;
-  const T* P = (const T*)B.prim;
-  const int n[3] = {x.ni, x.nj, x.nk};
-  const int idx[3] = {x.i, x.j, x.k};
-  const int64_t st[3] = {si, sj, 1};
+  // 32-bit offsets: 15 N < 2^31 is checked on the host
+  const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
+  const int32_t si = x.nj * x.nk, sj = x.nk;
+  const T* __restrict__ P = (const T*)B.prim;
+  const bool vis = (flags & kRhsViscous) != 0, inv = (flags & kRhsInvscd) != 0;
 
-  if (flags & kRhsViscous) {
+  // neighbour offsets with the padded-array wrap (jnp.roll) for the viscous
+  // stencil; faces exist only where no wrap is involved
+  const int32_t ip = x.i + 1 == x.ni ? c - (x.ni - 1) * si : c + si;
+  const int32_t im = x.i == 0 ? c + (x.ni - 1) * si : c - si;
+  const int32_t jp = x.j + 1 == x.nj ? c - (x.nj - 1) * sj : c + sj;
+  const int32_t jm = x.j == 0 ? c + (x.nj - 1) * sj : c - sj;
+  const int32_t kp = x.k + 1 == x.nk ? c - (x.nk - 1) : c + 1;
+  const int32_t km = x.k == 0 ? c + (x.nk - 1) : c - 1;
+
+  const Cell6<T> C0 = load_cell<T, true>(P, N, c);
+  const Cell6<T> Im = load_cell<T, true>(P, N, im), Ip = load_cell<T, true>(P, N, ip);
+  const Cell6<T> Jm = load_cell<T, true>(P, N, jm), Jp = load_cell<T, true>(P, N, jp);
+  const Cell6<T> Km = load_cell<T, true>(P, N, km), Kp = load_cell<T, true>(P, N, kp);
+
+  if (vis) {
     // viscous flux components at c (rhs/viscous.py:36-105)
-    int64_t cp[3], cm[3];
-#pragma unroll
-    for (int l = 0; l < 3; ++l) {
-      cp[l] = idx[l] + 1 == n[l] ? c - (int64_t)(n[l] - 1) * st[l] : c + st[l];
-      cm[l] = idx[l] == 0 ? c + (int64_t)(n[l] - 1) * st[l] : c - st[l];
-    }
-    T d[4][3];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int64_t o = (int64_t)(s < 3 ? s + 1 : 5) * N;  // u, v, w, T
-#pragma unroll
-      for (int l = 0; l < 3; ++l) d[s][l] = T(0.5) * (P[o + cp[l]] - P[o + cm[l]]);
-    }
+    const T h = T(0.5);
+    const T d[4][3] = {{h * (Ip.u - Im.u), h * (Jp.u - Jm.u), h * (Kp.u - Km.u)},
+                       {h * (Ip.v - Im.v), h * (Jp.v - Jm.v), h * (Kp.v - Km.v)},
+                       {h * (Ip.w - Im.w), h * (Jp.w - Jm.w), h * (Kp.w - Km.w)},
+                       {h * (Ip.t - Im.t), h * (Jp.t - Jm.t), h * (Kp.t - Km.t)}};
     T kk[9];
-#pragma unroll
-    for (int lm = 0; lm < 9; ++lm) kk[lm] = metric<T>(B, N, lm, c);
+    metric_row<T>(B, N, 0, c, kk);
+    metric_row<T>(B, N, 1, c, kk + 3);
+    metric_row<T>(B, N, 2, c, kk + 6);
     T g[4][3];
 #pragma unroll
     for (int s = 0; s < 4; ++s)
 #pragma unroll
       for (int m = 0; m < 3; ++m) g[s][m] = d[s][0] * kk[m] + d[s][1] * kk[3 + m] + d[s][2] * kk[6 + m];
-    const T u = P[N + c], v = P[2 * N + c], w = P[3 * N + c];
     T mu = (T)ph.mu0;
     if (ph.visc_law == 0) {  // Sutherland (physics/eos.py:24-25)
-      const T Tt = P[5 * N + c];
-      const T r = Tt * (T)(1.0 / ph.T0);
-      mu = (T)ph.mu0 * (r * M::sqrt_pos(r)) * (T)(ph.T0 + ph.Ts) * M::rcp(Tt + (T)ph.Ts);
+      const T r = C0.t * (T)ph.inv_T0;
+      mu = (T)ph.mu0 * (r * M::sqrt_pos(r)) * (T)ph.sfac * M::rcp(C0.t + (T)ph.Ts);
     }
-    const T kappa = (T)(ph.cp / ph.Pr) * mu;
+    const T kappa = (T)ph.kap_fac * mu;
     const T third = (T)(1.0 / 3.0);
     const T div_u = g[0][0] + g[1][1] + g[2][2];
     const T t00 = T(2) * mu * (g[0][0] - div_u * third);
@@ -164,42 +213,44 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_fluxes(const Table tab,
     const T t11 = T(2) * mu * (g[1][1] - div_u * third);
     const T t12 = mu * (g[1][2] + g[2][1]);
     const T t22 = T(2) * mu * (g[2][2] - div_u * third);
-    T* G = (T*)B.G;
+    T* __restrict__ G = (T*)B.G;
     G[c] = t00;
     G[N + c] = t01;
     G[2 * N + c] = t02;
     G[3 * N + c] = t11;
     G[4 * N + c] = t12;
     G[5 * N + c] = t22;
-    G[6 * N + c] = u * t00 + v * t01 + w * t02 + kappa * g[3][0];
-    G[7 * N + c] = u * t01 + v * t11 + w * t12 + kappa * g[3][1];
-    G[8 * N + c] = u * t02 + v * t12 + w * t22 + kappa * g[3][2];
+    G[6 * N + c] = C0.u * t00 + C0.v * t01 + C0.w * t02 + kappa * g[3][0];
+    G[7 * N + c] = C0.u * t01 + C0.v * t11 + C0.w * t12 + kappa * g[3][1];
+    G[8 * N + c] = C0.u * t02 + C0.v * t12 + C0.w * t22 + kappa * g[3][2];
   }
-  if (flags & kRhsInvscd) {
-    const T gm1 = (T)ph.gm1, inv_gm1 = (T)(1.0 / ph.gm1), eps_e = (T)ph.eps_entropy;
-    T* F = (T*)B.F;
-#pragma unroll 1
-    for (int a = 0; a < 3; ++a) {
-      // face c | c+e_a (face index c_a - 1 of rhs/invscd.py:62-100)
-      if (idx[a] < 1 || idx[a] > n[a] - 3) continue;
-      Prim<T> cell[4];
+  if (inv) {
+    // the three faces c | c+e_a with face index c_a - 1 in [0, n_a - 4]
+    T* __restrict__ F = (T*)B.F;
+    T kc[3], kn[3], Fo[5];
+    if (x.i >= 1 && x.i <= x.ni - 3) {
+      const Cell6<T> I2 = load_cell<T, false>(P, N, c + 2 * si);
+      metric_row<T>(B, N, 0, c, kc);
+      metric_row<T>(B, N, 0, c + si, kn);
+      face_from_cells<T>(Im, C0, Ip, I2, kc, kn, ph, Fo);
 #pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        const int64_t cc = c + (int64_t)(s - 1) * st[a];
-        cell[s].rho = P[cc];
-        cell[s].u = P[N + cc];
-        cell[s].v = P[2 * N + cc];
-        cell[s].w = P[3 * N + cc];
-        cell[s].p = P[4 * N + cc];
-      }
-      const int64_t cr = c + st[a];
-      T Fo[5];
-      invscd_face_fast<T>(cell, metric<T>(B, N, 3 * a, c), metric<T>(B, N, 3 * a + 1, c),
-                          metric<T>(B, N, 3 * a + 2, c), metric<T>(B, N, 3 * a, cr),
-                          metric<T>(B, N, 3 * a + 1, cr), metric<T>(B, N, 3 * a + 2, cr), gm1, inv_gm1,
-                          eps_e, ph.limiter, Fo);
+      for (int v = 0; v < 5; ++v) F[v * N + c] = Fo[v];
+    }
+    if (x.j >= 1 && x.j <= x.nj - 3) {
+      const Cell6<T> J2 = load_cell<T, false>(P, N, c + 2 * sj);
+      metric_row<T>(B, N, 1, c, kc);
+      metric_row<T>(B, N, 1, c + sj, kn);
+      face_from_cells<T>(Jm, C0, Jp, J2, kc, kn, ph, Fo);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) F[(int64_t)(a * 5 + v) * N + c] = Fo[v];
+      for (int v = 0; v < 5; ++v) F[(5 + v) * N + c] = Fo[v];
+    }
+    if (x.k >= 1 && x.k <= x.nk - 3) {
+      const Cell6<T> K2 = load_cell<T, false>(P, N, c + 2);
+      metric_row<T>(B, N, 2, c, kc);
+      metric_row<T>(B, N, 2, c + 1, kn);
+      face_from_cells<T>(Km, C0, Kp, K2, kc, kn, ph, Fo);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) F[(10 + v) * N + c] = Fo[v];
     }
   }
 }
@@ -300,6 +351,9 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
     tab.n = std::min(kMaxSplitBlocks, nblocks - base);
     int ctas = 0;
     for (int t = 0; t < tab.n; ++t) {
+      // the kernels index the 15 face-flux fields with 32-bit offsets
+      if (15 * (int64_t)blocks[base + t].ni * blocks[base + t].nj * blocks[base + t].nk > INT32_MAX)
+        return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "block too large for the split pipeline");
       tab.b[t].blk = blocks[base + t];
       tab.b[t].blk.cta_begin = ctas;
       tab.b[t].dk.init((uint32_t)blocks[base + t].nk);

@@ -82,6 +82,13 @@ class StepPlan:
         _capi.check(self._lib.fj_plan_step(self._handle, _topology.ptr_array(qs), _topology.ptr_array(outs),
                                            float(dt), _capi.stream(self.device)), "fj_plan_step", c)
 
+    def stage(self, qs, q0s, outs, dt: float, stage: int) -> None:
+        """One TVD-RK3 stage of every block (no halo fill)."""
+        c = _capi.ctx(self.device)
+        q0p = _topology.ptr_array(q0s) if q0s is not None else None
+        _capi.check(self._lib.fj_plan_stage(self._handle, _topology.ptr_array(qs), q0p, _topology.ptr_array(outs),
+                                            float(dt), int(stage), _capi.stream(self.device)), "fj_plan_stage", c)
+
     def __del__(self):
         if getattr(self, "_handle", None):
             self._lib.fj_plan_destroy(self._handle)

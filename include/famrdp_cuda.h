@@ -214,6 +214,12 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
 int fj_plan_step(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,
                  void* stream);
 int fj_plan_destroy(fj_plan* plan);
+/* One TVD-RK3 stage (1..3) of every block of the plan, without the halo fill
+ * (solver/step.py:45-53): out[b] from q[b] (stage input) and q0[b] (step start
+ * state); out[b] may alias q0[b], never q[b].  With the split pipeline this is
+ * three launches over all blocks. */
+int fj_plan_stage(fj_plan* plan, double* const* q, double* const* q0, double* const* out,
+                  double dt, int stage, void* stream);
 
 /* time/rk.py:5-20 one Shu-Osher stage combine, elementwise over n values:
  *   stage 1: out = qs + dt*L
