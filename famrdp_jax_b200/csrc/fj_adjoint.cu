@@ -1,0 +1,417 @@
+// fj_adjoint.cu -- hand-written reverse mode of the RHS and of the TVD-RK3
+// step (the reference differentiates its step with jax.grad,
+// tests/solver/test_grad.py:30-35; there is no hand-written adjoint there).
+//
+// RHS vector-Jacobian product lam -> (dL/dq)^T lam for one block, four kernels:
+//   k_adj_prims    primitives (rho, u, v, w, p, T) of q                 (forward)
+//   k_adj_faces    per cell c and axis a with a face c | c+e_a: the face's
+//                  adjoint  lamF = -lam(c)/vol(c) [c in range] + lam(c+e_a)/
+//                  vol(c+e_a) [c+e_a in range]  (reverse of rhs/invscd.py:
+//                  119-131), then the reverse of MUSCL + Roe; the primitive
+//                  adjoints of the four cells are atomically added to lamP
+//   k_adj_visc     per cell y: lamG(y) gathered from the six neighbours'
+//                  lam and kxyz (reverse of the divergence, rhs/viscous.py:
+//                  86-117), then the reverse of the viscous fluxes at y:
+//                  lamD[s][l] (adjoint of the central difference of u, v, w, T
+//                  along l) and the local adjoints of u, v, w, T at y
+//   k_adj_final    per cell: lamP + local + the neighbours' lamD gathered back
+//                  through the central differences, the reverse of
+//                  T = p/(rho R) and of cons_to_prim (physics/eos.py:12-17)
+// All neighbour indices wrap around the padded block like the forward.
+//
+// The step adjoint recomputes q0' (copy + halo + BC), q1 and q2 with the
+// forward kernels, then applies the transposed stage combines and RHS VJPs
+// in reverse (solver/step.py:45-53) and finally the transposed boundary
+// conditions and halo fill (mesh/halo.py:56-92, physics/bc/*.py).
+#include <vector>
+
+#include "fj_adjoint.cuh"
+#include "fj_common.cuh"
+#include "fj_rhs.cuh"
+
+namespace fj {
+
+namespace {
+
+constexpr int kAT = 256;
+
+struct ADims {
+  int ni, nj, nk;
+};
+
+__device__ __forceinline__ void dec(int c, const ADims& d, int& i, int& j, int& k) {
+  k = c % d.nk;
+  const int t = c / d.nk;
+  j = t % d.nj;
+  i = t / d.nj;
+}
+
+__device__ __forceinline__ void wrapped(int c, int i, int j, int k, const ADims& d, int nb[6]) {
+  const int si = d.nj * d.nk, sj = d.nk;
+  nb[0] = i + 1 == d.ni ? c - (d.ni - 1) * si : c + si;
+  nb[1] = i == 0 ? c + (d.ni - 1) * si : c - si;
+  nb[2] = j + 1 == d.nj ? c - (d.nj - 1) * sj : c + sj;
+  nb[3] = j == 0 ? c + (d.nj - 1) * sj : c - sj;
+  nb[4] = k + 1 == d.nk ? c - (d.nk - 1) : c + 1;
+  nb[5] = k == 0 ? c + (d.nk - 1) : c - 1;
+}
+
+template <typename T>
+__global__ void k_adj_prims(const double* __restrict__ q, T* __restrict__ P, int N, double gm1,
+                            double R) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const double r = q[c], ir = 1.0 / r;
+  const double u = q[N + c] * ir, v = q[2 * N + c] * ir, w = q[3 * N + c] * ir;
+  const double p = gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
+  P[c] = (T)r;
+  P[N + c] = (T)u;
+  P[2 * N + c] = (T)v;
+  P[3 * N + c] = (T)w;
+  P[4 * N + c] = (T)p;
+  P[5 * N + c] = (T)(r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300);
+}
+
+__device__ __forceinline__ void atomic_add(float* a, float v) { atomicAdd(a, v); }
+__device__ __forceinline__ void atomic_add(double* a, double v) { atomicAdd(a, v); }
+
+template <typename T>
+__global__ void k_adj_faces(const T* __restrict__ P, const double* __restrict__ kxyz,
+                            const double* __restrict__ vol, const double* __restrict__ lam,
+                            T* __restrict__ lamP, ADims d, Phys ph) {
+  const int N = d.ni * d.nj * d.nk;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  int i, j, k;
+  dec(c, d, i, j, k);
+  const int idx[3] = {i, j, k}, n[3] = {d.ni, d.nj, d.nk};
+  const int st[3] = {d.nj * d.nk, d.nk, 1};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (idx[a] < 1 || idx[a] > n[a] - 3) continue;
+    const int cr = c + st[a];
+    const bool inL = idx[a] >= 2, inR = idx[a] + 1 <= n[a] - 3;
+    const double ivl = inL ? 1.0 / (vol[c] + 1e-300) : 0.0;
+    const double ivr = inR ? 1.0 / (vol[cr] + 1e-300) : 0.0;
+    T lF[5];
+    bool any = false;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double x = (inL ? -lam[v * N + c] * ivl : 0.0) + (inR ? lam[v * N + cr] * ivr : 0.0);
+      lF[v] = (T)x;
+      any |= x != 0.0;
+    }
+    if (!any) continue;
+    Prim<T> cell[4], lc[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int cc = c + (s - 1) * st[a];
+      cell[s] = Prim<T>{P[cc], P[N + cc], P[2 * N + cc], P[3 * N + cc], P[4 * N + cc]};
+      lc[s] = Prim<T>{T(0), T(0), T(0), T(0), T(0)};
+    }
+    const double* K = kxyz + (size_t)(3 * a) * N;
+    invscd_face_vjp<T>(cell, (T)K[c], (T)K[N + c], (T)K[2 * N + c], (T)K[cr], (T)K[N + cr],
+                       (T)K[2 * N + cr], (T)ph.gm1, (T)ph.inv_gm1, (T)ph.eps_entropy, ph.limiter, lF,
+                       lc);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int cc = c + (s - 1) * st[a];
+      atomic_add(lamP + cc, lc[s].rho);
+      atomic_add(lamP + N + cc, lc[s].u);
+      atomic_add(lamP + 2 * N + cc, lc[s].v);
+      atomic_add(lamP + 3 * N + cc, lc[s].w);
+      atomic_add(lamP + 4 * N + cc, lc[s].p);
+    }
+  }
+}
+
+// lamD: 12 x N (s-major: u, v, w, T; l = 0..2), lamL: 4 x N (local u, v, w, T)
+template <typename T>
+__global__ void k_adj_visc(const T* __restrict__ P, const double* __restrict__ kxyz,
+                           const double* __restrict__ lam, T* __restrict__ lamD,
+                           T* __restrict__ lamL, ADims d, Phys ph) {
+  using M = FastMath<T>;
+  const int N = d.ni * d.nj * d.nk;
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= N) return;
+  int i, j, k;
+  dec(y, d, i, j, k);
+  int nb[6];
+  wrapped(y, i, j, k, d, nb);
+  // ---- lamG(y): reverse of rhs_vis(c) = sum_jj sum_l 0.5 k[l][jj](c) (G(c+e_l) - G(c-e_l))
+  double lG[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      // side 0: c = y - e_l (y is its + neighbour, weight +0.5); side 1: c = y + e_l (-0.5)
+      const int c = side == 0 ? nb[2 * l + 1] : nb[2 * l];
+      const double wgt = side == 0 ? 0.5 : -0.5;
+      const double k0 = kxyz[(3 * l + 0) * N + c], k1 = kxyz[(3 * l + 1) * N + c],
+                   k2 = kxyz[(3 * l + 2) * N + c];
+      const double L1 = lam[N + c], L2 = lam[2 * N + c], L3 = lam[3 * N + c], L4 = lam[4 * N + c];
+      // comp(e, jj): tau_00 tau_01 tau_02 tau_11 tau_12 tau_22 Ge_0 Ge_1 Ge_2
+      lG[0] += wgt * (k0 * L1);
+      lG[1] += wgt * (k1 * L1 + k0 * L2);
+      lG[2] += wgt * (k2 * L1 + k0 * L3);
+      lG[3] += wgt * (k1 * L2);
+      lG[4] += wgt * (k2 * L2 + k1 * L3);
+      lG[5] += wgt * (k2 * L3);
+      lG[6] += wgt * (k0 * L4);
+      lG[7] += wgt * (k1 * L4);
+      lG[8] += wgt * (k2 * L4);
+    }
+  }
+  // ---- forward of the viscous fluxes at y (rhs/viscous.py:36-105)
+  const int fld[4] = {1, 2, 3, 5};
+  T dd[4][3];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int l = 0; l < 3; ++l)
+      dd[s][l] = T(0.5) * (P[fld[s] * N + nb[2 * l]] - P[fld[s] * N + nb[2 * l + 1]]);
+  T kk[9];
+#pragma unroll
+  for (int lm = 0; lm < 9; ++lm) kk[lm] = (T)kxyz[lm * N + y];
+  T g[4][3];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) g[s][m] = dd[s][0] * kk[m] + dd[s][1] * kk[3 + m] + dd[s][2] * kk[6 + m];
+  const T u = P[N + y], v = P[2 * N + y], w = P[3 * N + y], Tt = P[5 * N + y];
+  T mu = (T)ph.mu0, dmu_dT = T(0);
+  if (ph.visc_law == 0) {
+    const T r = Tt * (T)ph.inv_T0;
+    mu = (T)ph.mu0 * (r * M::sqrt_pos(r)) * (T)ph.sfac * M::rcp(Tt + (T)ph.Ts);
+    dmu_dT = mu * (T(1.5) * M::rcp(Tt) - M::rcp(Tt + (T)ph.Ts));
+  }
+  const T kap = (T)ph.kap_fac;
+  const T kappa = kap * mu;
+  const T third = (T)(1.0 / 3.0);
+  const T div_u = g[0][0] + g[1][1] + g[2][2];
+  const T t00 = T(2) * mu * (g[0][0] - div_u * third), t11 = T(2) * mu * (g[1][1] - div_u * third),
+          t22 = T(2) * mu * (g[2][2] - div_u * third);
+  const T t01 = mu * (g[0][1] + g[1][0]), t02 = mu * (g[0][2] + g[2][0]), t12 = mu * (g[1][2] + g[2][1]);
+  // ---- reverse
+  const T lGe0 = (T)lG[6], lGe1 = (T)lG[7], lGe2 = (T)lG[8];
+  T lt00 = (T)lG[0] + lGe0 * u, lt01 = (T)lG[1] + lGe0 * v + lGe1 * u, lt02 = (T)lG[2] + lGe0 * w + lGe2 * u;
+  T lt11 = (T)lG[3] + lGe1 * v, lt12 = (T)lG[4] + lGe1 * w + lGe2 * v, lt22 = (T)lG[5] + lGe2 * w;
+  const T lu = lGe0 * t00 + lGe1 * t01 + lGe2 * t02;
+  const T lv = lGe0 * t01 + lGe1 * t11 + lGe2 * t12;
+  const T lw = lGe0 * t02 + lGe1 * t12 + lGe2 * t22;
+  T lkappa = lGe0 * g[3][0] + lGe1 * g[3][1] + lGe2 * g[3][2];
+  T lg[4][3];
+  lg[3][0] = lGe0 * kappa;
+  lg[3][1] = lGe1 * kappa;
+  lg[3][2] = lGe2 * kappa;
+  T lmu = lt00 * T(2) * (g[0][0] - div_u * third) + lt11 * T(2) * (g[1][1] - div_u * third) +
+          lt22 * T(2) * (g[2][2] - div_u * third) + lt01 * (g[0][1] + g[1][0]) +
+          lt02 * (g[0][2] + g[2][0]) + lt12 * (g[1][2] + g[2][1]) + kap * lkappa;
+  const T ldiv = -(lt00 + lt11 + lt22) * T(2) * mu * third;
+  lg[0][0] = lt00 * T(2) * mu + ldiv;
+  lg[1][1] = lt11 * T(2) * mu + ldiv;
+  lg[2][2] = lt22 * T(2) * mu + ldiv;
+  lg[0][1] = lt01 * mu;
+  lg[1][0] = lt01 * mu;
+  lg[0][2] = lt02 * mu;
+  lg[2][0] = lt02 * mu;
+  lg[1][2] = lt12 * mu;
+  lg[2][1] = lt12 * mu;
+  const T lT = lmu * dmu_dT;
+  // g[s][m] = sum_l d[s][l] k[l][m]  ->  lamD[s][l] = sum_m lg[s][m] k[l][m]
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int l = 0; l < 3; ++l)
+      lamD[(s * 3 + l) * N + y] = lg[s][0] * kk[3 * l] + lg[s][1] * kk[3 * l + 1] + lg[s][2] * kk[3 * l + 2];
+  lamL[y] = lu;
+  lamL[N + y] = lv;
+  lamL[2 * N + y] = lw;
+  lamL[3 * N + y] = lT;
+}
+
+template <typename T>
+__global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ lamP,
+                            const T* __restrict__ lamD, const T* __restrict__ lamL,
+                            double* __restrict__ out, ADims d, Phys ph, int flags) {
+  const int N = d.ni * d.nj * d.nk;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= N) return;
+  double lr = 0, lu = 0, lv = 0, lw = 0, lp = 0, lT = 0;
+  if (flags & kRhsInvscd) {
+    lr = lamP[x];
+    lu = lamP[N + x];
+    lv = lamP[2 * N + x];
+    lw = lamP[3 * N + x];
+    lp = lamP[4 * N + x];
+  }
+  if (flags & kRhsViscous) {
+    int i, j, k;
+    dec(x, d, i, j, k);
+    int nb[6];
+    wrapped(x, i, j, k, d, nb);
+    double ls[4] = {(double)lamL[x], (double)lamL[N + x], (double)lamL[2 * N + x], (double)lamL[3 * N + x]};
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int l = 0; l < 3; ++l)
+        ls[s] += 0.5 * ((double)lamD[(s * 3 + l) * N + nb[2 * l + 1]] - (double)lamD[(s * 3 + l) * N + nb[2 * l]]);
+    lu += ls[0];
+    lv += ls[1];
+    lw += ls[2];
+    lT = ls[3];
+  }
+  // reverse of T = p / max(rho R, 1e-300) and of cons_to_prim
+  const double r = q[x], ir = 1.0 / r;
+  const double u = q[N + x] * ir, v = q[2 * N + x] * ir, w = q[3 * N + x] * ir;
+  const double ke = 0.5 * (u * u + v * v + w * w);
+  const double p = ph.gm1 * (q[4 * N + x] - r * ke);
+  if (r * ph.R > 1e-300) {
+    lp += lT * ir / ph.R;
+    lr -= lT * p * ir * ir / ph.R;
+  } else {
+    lp += lT * 1e300;
+  }
+  // p = gm1 (q4 - rho ke); ke = 0.5 |u|^2; u = q1 / rho
+  const double lq4 = ph.gm1 * lp;
+  lr -= ph.gm1 * lp * ke;
+  const double lke = -ph.gm1 * lp * r;
+  lu += lke * u;
+  lv += lke * v;
+  lw += lke * w;
+  out[N + x] = lu * ir;
+  out[2 * N + x] = lv * ir;
+  out[3 * N + x] = lw * ir;
+  out[4 * N + x] = lq4;
+  out[x] = lr - (lu * u + lv * v + lw * w) * ir;
+}
+
+// out = a x + b y + c z (y, z may be null)
+__global__ void k_axpy3(double* __restrict__ out, const double* __restrict__ x, double a,
+                        const double* __restrict__ y, double b, const double* __restrict__ z, double c,
+                        int64_t n) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double r = a * x[t];
+  if (y) r += b * y[t];
+  if (z) r += c * z[t];
+  out[t] = r;
+}
+
+// *acc += scale * sum(x * y) (FP64 warp-shuffle reduction + one atomic per CTA)
+__global__ void k_dot_acc(const double* __restrict__ x, const double* __restrict__ y, int64_t n,
+                          double scale, double* __restrict__ acc) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    s += x[t] * y[t];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) atomicAdd(acc, scale * s);
+  }
+}
+
+// dJ/dq of J = sum_interior vol * 0.5 |m|^2 / rho
+__global__ void k_ke_grad(const double* __restrict__ q, const double* __restrict__ vol,
+                          double* __restrict__ grad, int ni, int nj, int nk, int g) {
+  const int N = ni * nj * nk;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const int k = c % nk, j = (c / nk) % nj, i = c / (nk * nj);
+  const bool in = i >= g && i < ni - g && j >= g && j < nj - g && k >= g && k < nk - g;
+  if (!in) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) grad[v * N + c] = 0.0;
+    return;
+  }
+  const double r = q[c], m1 = q[N + c], m2 = q[2 * N + c], m3 = q[3 * N + c], V = vol[c];
+  const double ir = 1.0 / r;
+  grad[c] = -V * 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) * ir * ir;
+  grad[N + c] = V * m1 * ir;
+  grad[2 * N + c] = V * m2 * ir;
+  grad[3 * N + c] = V * m3 * ir;
+  grad[4 * N + c] = 0.0;
+}
+
+template <typename T>
+size_t vjp_ws(int64_t N) {
+  return ((6 + 5 + 12 + 4) * (size_t)N) * sizeof(T) + 4 * 256;
+}
+
+template <typename T>
+int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
+                 const double* lam, double* out, int ni, int nj, int nk, const Phys& ph, int flags,
+                 void* ws, cudaStream_t st) {
+  const int N = ni * nj * nk;
+  auto al = [](char* p) { return (char*)(((uintptr_t)p + 255) & ~(uintptr_t)255); };
+  char* p = al((char*)ws);
+  T* P = (T*)p;
+  p = al(p + 6 * (size_t)N * sizeof(T));
+  T* lamP = (T*)p;
+  p = al(p + 5 * (size_t)N * sizeof(T));
+  T* lamD = (T*)p;
+  p = al(p + 12 * (size_t)N * sizeof(T));
+  T* lamL = (T*)p;
+  const ADims d{ni, nj, nk};
+  const int grid = grid_for(N, kAT);
+  k_adj_prims<T><<<grid, kAT, 0, st>>>(q, P, N, ph.gm1, ph.R);
+  ctx->launches += 1;
+  if (flags & kRhsInvscd) {
+    cudaError_t e = cudaMemsetAsync(lamP, 0, 5 * (size_t)N * sizeof(T), st);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "vjp memset");
+    k_adj_faces<T><<<grid, kAT, 0, st>>>(P, kxyz, vol, lam, lamP, d, ph);
+    ctx->launches += 1;
+  }
+  if (flags & kRhsViscous) {
+    k_adj_visc<T><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph);
+    ctx->launches += 1;
+  }
+  k_adj_final<T><<<grid, kAT, 0, st>>>(q, lamP, lamD, lamL, out, d, ph, flags);
+  ctx->launches += 1;
+  return launch_status(ctx, "rhs vjp launch");
+}
+
+}  // namespace
+
+size_t rhs_vjp_ws_bytes(int precision, int ni, int nj, int nk) {
+  const int64_t N = (int64_t)ni * nj * nk;
+  return precision == FJ_PREC_F32FLUX ? vjp_ws<float>(N) : vjp_ws<double>(N);
+}
+
+int rhs_vjp(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol, const double* lam,
+            double* out, int ni, int nj, int nk, const fj_params* p, int flags, void* ws,
+            cudaStream_t st) {
+  const Phys ph = make_phys(p);
+  if (p->precision == FJ_PREC_F32FLUX)
+    return rhs_vjp_impl<float>(ctx, q, kxyz, vol, lam, out, ni, nj, nk, ph, flags, ws, st);
+  return rhs_vjp_impl<double>(ctx, q, kxyz, vol, lam, out, ni, nj, nk, ph, flags, ws, st);
+}
+
+int dot_acc(fj_ctx* ctx, const double* x, const double* y, int64_t n, double scale, double* acc,
+            cudaStream_t st) {
+  k_dot_acc<<<592, kThreads, 0, st>>>(x, y, n, scale, acc);
+  ctx->launches += 1;
+  return launch_status(ctx, "dot launch");
+}
+
+int ke_grad(fj_ctx* ctx, const double* q, const double* vol, double* grad, int ni, int nj, int nk, int g,
+            cudaStream_t st) {
+  k_ke_grad<<<grid_for((int64_t)ni * nj * nk), kThreads, 0, st>>>(q, vol, grad, ni, nj, nk, g);
+  ctx->launches += 1;
+  return launch_status(ctx, "ke grad launch");
+}
+
+int axpy3(fj_ctx* ctx, double* out, const double* x, double a, const double* y, double b,
+          const double* z, double c, int64_t n, cudaStream_t st) {
+  k_axpy3<<<grid_for(n), kThreads, 0, st>>>(out, x, a, y, b, z, c, n);
+  ctx->launches += 1;
+  return launch_status(ctx, "axpy launch");
+}
+
+}  // namespace fj

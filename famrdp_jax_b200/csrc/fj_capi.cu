@@ -515,6 +515,150 @@ int fj_plan_stage(fj_plan* pl, double* const* q, double* const* q0, double* cons
   return s;
 }
 
+int fj_rhs_vjp_f64(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
+                   const double* lam, double* out, int ni, int nj, int nk, const fj_params* p,
+                   void* stream) {
+  if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
+  int s = check_params(ctx, p);
+  if (s != FJ_OK) return s;
+  s = check_dims(ctx, ni, nj, nk);
+  if (s != FJ_OK) return s;
+  if (!q || !kxyz || !vol || !lam || !out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  s = ensure_ws(ctx, rhs_vjp_ws_bytes(p->precision, ni, nj, nk));
+  if (s != FJ_OK) return s;
+  return rhs_vjp(ctx, q, kxyz, vol, lam, out, ni, nj, nk, p, kRhsInvscd | kRhsViscous, ctx->ws, S(stream));
+}
+
+static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
+                         double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
+                         const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dmu,
+                         void* stream);
+
+int fj_step_vjp_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
+                    double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
+                    const fj_bc* bcs, int nbcs, const fj_params* p, double dt, void* stream) {
+  return step_vjp_impl(ctx, blocks, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt, nullptr, stream);
+}
+
+int fj_step_vjp_mu_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
+                       double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
+                       const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dJ_dmu0,
+                       void* stream) {
+  if (!dJ_dmu0) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "dJ_dmu0 is NULL");
+  return step_vjp_impl(ctx, blocks, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt, dJ_dmu0, stream);
+}
+
+int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* const* grad, int nblocks,
+                               int ghost, void* stream) {
+  if (!ctx || !blocks || !grad || nblocks <= 0 || ghost < 0) return FJ_ERR_INVALID_ARGUMENT;
+  for (int b = 0; b < nblocks; ++b) {
+    if (!blocks[b].q || !blocks[b].vol || !grad[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "NULL array");
+    int s = ke_grad(ctx, blocks[b].q, blocks[b].vol, grad[b], blocks[b].ni, blocks[b].nj, blocks[b].nk, ghost,
+                    S(stream));
+    if (s != FJ_OK) return s;
+  }
+  return FJ_OK;
+}
+
+static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
+                         double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
+                         const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dmu,
+                         void* stream) {
+  if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
+  if (!lam_in || !lam_out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "adjoint lists are NULL");
+  std::vector<double*> dummy(nblocks > 0 ? nblocks : 1, nullptr);
+  for (int b = 0; b < nblocks; ++b) dummy[b] = blocks ? blocks[b].q : nullptr;
+  int s = check_step_args(ctx, blocks, dummy.data(), nblocks, links, nlinks, bcs, nbcs, p);
+  if (s != FJ_OK) return s;
+  for (int b = 0; b < nblocks; ++b)
+    if (!lam_in[b] || !lam_out[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "adjoint pointer is NULL");
+  for (int b = 0; b < nbcs; ++b)
+    if (bcs[b].type == FJ_BC_WALL && bcs[b].isothermal)
+      return set_err(ctx, FJ_ERR_NOT_IMPLEMENTED, "the adjoint of the isothermal wall is not implemented");
+  cudaStream_t st = S(stream);
+  // layout: [Q0 all blocks][L0 all blocks][Q1][Q2][LA][LB][V][work]
+  size_t sum5 = 0, max5 = 0, work = 256;
+  for (int b = 0; b < nblocks; ++b) {
+    const size_t by = align256(5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double));
+    sum5 += by;
+    max5 = std::max(max5, by);
+    work = std::max(work, rhs_scratch_bytes(ctx, p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
+    work = std::max(work, rhs_vjp_ws_bytes(p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
+  }
+  work = std::max(work, halo_ws_bytes(blocks, links, nlinks, p->ghost));
+  work = align256(work);
+  s = ensure_ws(ctx, 2 * sum5 + 6 * max5 + work);
+  if (s != FJ_OK) return s;
+  char* base = (char*)ctx->ws;
+  std::vector<fj_block> q0(blocks, blocks + nblocks), l0(blocks, blocks + nblocks);
+  size_t off = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    q0[b].q = (double*)(base + off);
+    l0[b].q = (double*)(base + sum5 + off);
+    off += align256(5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double));
+  }
+  double* Q1 = (double*)(base + 2 * sum5);
+  double* Q2 = (double*)(base + 2 * sum5 + max5);
+  double* LA = (double*)(base + 2 * sum5 + 2 * max5);
+  double* LB = (double*)(base + 2 * sum5 + 3 * max5);
+  double* V = (double*)(base + 2 * sum5 + 4 * max5);
+  double* W = (double*)(base + 2 * sum5 + 5 * max5);  // viscous RHS for dJ/dmu0
+  void* wk = base + 2 * sum5 + 6 * max5;
+  const double inv_mu = p->mu0 != 0.0 ? 1.0 / p->mu0 : 0.0;
+  // c_s dt lam_{s+1} . L_vis(q_s) / mu0
+  auto mu_term = [&](const fj_block& B, const double* qs, const double* lam_next, double coef) -> int {
+    if (!dmu) return FJ_OK;
+    int r = run_rhs(ctx, qs, B.kxyz, B.vol, nullptr, W, B.ni, B.nj, B.nk, p, kRhsViscous, 0, 0.0, wk, st);
+    if (r != FJ_OK) return r;
+    return dot_acc(ctx, lam_next, W, 5 * (int64_t)B.ni * B.nj * B.nk, coef * dt * inv_mu, dmu, st);
+  };
+  // ---- forward recompute of q0' (copy + halo + BC)
+  for (int b = 0; b < nblocks; ++b) {
+    const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
+    s = cuda_status(ctx, cudaMemcpyAsync(q0[b].q, blocks[b].q, bytes, cudaMemcpyDeviceToDevice, st), "copy");
+    if (s != FJ_OK) return s;
+  }
+  s = halo_exchange(ctx, q0.data(), nblocks, links, nlinks, p->ghost, (double*)wk, work, st);
+  if (s != FJ_OK) return s;
+  s = apply_bc(ctx, q0.data(), nblocks, bcs, nbcs, p, st);
+  if (s != FJ_OK) return s;
+  // ---- per block: recompute q1, q2; reverse the three stages
+  const int flags = kRhsInvscd | kRhsViscous;
+  for (int b = 0; b < nblocks; ++b) {
+    const fj_block& B = q0[b];
+    const int64_t n5 = 5 * (int64_t)B.ni * B.nj * B.nk;
+    double* L0 = l0[b].q;
+    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, Q1, B.ni, B.nj, B.nk, p, flags, 1, dt, wk, st);
+    if (s == FJ_OK) s = run_rhs(ctx, Q1, B.kxyz, B.vol, B.q, Q2, B.ni, B.nj, B.nk, p, flags, 2, dt, wk, st);
+    // stage 3: q3 = 1/3 q0 + 2/3 (q2 + dt L(q2))
+    if (s == FJ_OK) s = mu_term(B, Q2, lam_in[b], 2.0 / 3.0);
+    if (s == FJ_OK) s = rhs_vjp(ctx, Q2, B.kxyz, B.vol, lam_in[b], V, B.ni, B.nj, B.nk, p, flags, wk, st);
+    if (s == FJ_OK) s = axpy3(ctx, LB, lam_in[b], 2.0 / 3.0, V, 2.0 / 3.0 * dt, nullptr, 0.0, n5, st);
+    if (s == FJ_OK) s = axpy3(ctx, L0, lam_in[b], 1.0 / 3.0, nullptr, 0.0, nullptr, 0.0, n5, st);
+    // stage 2: q2 = 3/4 q0 + 1/4 (q1 + dt L(q1))
+    if (s == FJ_OK) s = mu_term(B, Q1, LB, 0.25);
+    if (s == FJ_OK) s = rhs_vjp(ctx, Q1, B.kxyz, B.vol, LB, V, B.ni, B.nj, B.nk, p, flags, wk, st);
+    if (s == FJ_OK) s = axpy3(ctx, LA, LB, 0.25, V, 0.25 * dt, nullptr, 0.0, n5, st);
+    if (s == FJ_OK) s = axpy3(ctx, L0, L0, 1.0, LB, 0.75, nullptr, 0.0, n5, st);
+    // stage 1: q1 = q0 + dt L(q0)
+    if (s == FJ_OK) s = mu_term(B, B.q, LA, 1.0);
+    if (s == FJ_OK) s = rhs_vjp(ctx, B.q, B.kxyz, B.vol, LA, V, B.ni, B.nj, B.nk, p, flags, wk, st);
+    if (s == FJ_OK) s = axpy3(ctx, L0, L0, 1.0, LA, 1.0, V, dt, n5, st);
+    if (s != FJ_OK) return s;
+  }
+  // ---- transposed boundary conditions, then transposed halo fill
+  s = bc_transpose(ctx, l0.data(), nblocks, bcs, nbcs, p, st);
+  if (s != FJ_OK) return s;
+  s = halo_transpose(ctx, l0.data(), nblocks, links, nlinks, p->ghost, (double*)wk, work, st);
+  if (s != FJ_OK) return s;
+  for (int b = 0; b < nblocks; ++b) {
+    const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
+    s = cuda_status(ctx, cudaMemcpyAsync(lam_out[b], l0[b].q, bytes, cudaMemcpyDeviceToDevice, st), "copy");
+    if (s != FJ_OK) return s;
+  }
+  return FJ_OK;
+}
+
 int fj_plan_destroy(fj_plan* pl) {
   if (!pl) return FJ_OK;
   for (float* k : pl->kxyz32)

@@ -25,7 +25,7 @@ namespace fj {
 
 namespace {
 
-constexpr int kMaxLinksPerLaunch = 128;
+constexpr int kMaxLinksPerLaunch = 192;
 constexpr int kMaxBcPerLaunch = 128;
 
 struct HaloDesc {
@@ -311,6 +311,170 @@ int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs,
       k_bc<<<grid, kThreads, 0, st>>>(tab, p->ghost);
       ctx->launches += 1;
       int s = launch_status(ctx, "bc launch");
+      if (s != FJ_OK) return s;
+    }
+  }
+  return FJ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Transposes (adjoint) of the halo fill and of the linear boundary conditions,
+// applied in place to per-block adjoint arrays laid out like q.
+// ---------------------------------------------------------------------------
+namespace {
+
+// A target cell's value after the fill comes from its last writer's source
+// cell; the cell's own original value is discarded.
+__device__ __forceinline__ bool later_link_covers(const HaloTable& tab, int L, int ti, int tj, int tk) {
+  const HaloDesc& d = tab.d[L];
+  for (int L2 = L + 1; L2 < tab.n; ++L2) {
+    const HaloDesc& e = tab.d[L2];
+    if (e.tgt_block != d.tgt_block) continue;
+    if (ti >= e.tlo[0] && ti < e.tlo[0] + e.ext[0] && tj >= e.tlo[1] && tj < e.tlo[1] + e.ext[1] &&
+        tk >= e.tlo[2] && tk < e.tlo[2] + e.ext[2])
+      return true;
+  }
+  return false;
+}
+
+// pass 0: scratch := lam at last-writer target cells (else 0); pass 1: zero
+// every target cell; pass 2: lam[source] += scratch.
+__global__ void k_halo_transpose(const HaloTable tab, double* __restrict__ scratch, int pass) {
+  const int L = blockIdx.y;
+  const HaloDesc& d = tab.d[L];
+  const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
+  const int64_t NT = (int64_t)d.tn[0] * d.tn[1] * d.tn[2];
+  const int64_t NS = (int64_t)d.sn[0] * d.sn[1] * d.sn[2];
+  double* tgt = d.tgt;
+  double* src = const_cast<double*>(d.src);
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < V;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(r % d.ext[2]);
+    const int b = (int)((r / d.ext[2]) % d.ext[1]);
+    const int a = (int)(r / ((int64_t)d.ext[2] * d.ext[1]));
+    const int ti = d.tlo[0] + a, tj = d.tlo[1] + b, tk = d.tlo[2] + c;
+    const int64_t tc = cell_index(d.tn, ti, tj, tk);
+    if (pass == 0) {
+      const bool last = !later_link_covers(tab, L, ti, tj, tk);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) scratch[d.off + v * V + r] = last ? tgt[v * NT + tc] : 0.0;
+    } else if (pass == 1) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) tgt[v * NT + tc] = 0.0;
+    } else {
+      const int64_t sc = cell_index(d.sn, d.slo[0] + a, d.slo[1] + b, d.slo[2] + c);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) atomicAdd(src + v * NS + sc, scratch[d.off + v * V + r]);
+    }
+  }
+}
+
+// Transpose of one face's farfield (lam(outer) := 0) or mirror BC
+// (lam(inner) += s lam(outer); lam(outer) := 0).
+__global__ void k_bc_transpose(const BcTable tab, int g) {
+  const BcDesc& d = tab.d[blockIdx.y];
+  const int ax = d.face >> 1;
+  const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
+  const int64_t NT = (int64_t)d.n[0] * d.n[1] * d.n[2];
+  const int64_t V = (int64_t)d.n[oa] * d.n[ob];
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < V;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(r % d.n[ob]);
+    const int x = (int)(r / d.n[ob]);
+    // the layers of one (x, y) line in one thread: outer and inner sets are disjoint
+    for (int o = 0; o < g; ++o) {
+      int outer, inner;
+      bc_layers(d.face, d.n[ax], g, o, outer, inner);
+      int io[3], ii[3];
+      io[ax] = outer; ii[ax] = inner;
+      io[oa] = x; ii[oa] = x;
+      io[ob] = y; ii[ob] = y;
+      const int64_t co = cell_index(d.n, io[0], io[1], io[2]);
+      const int64_t ci = cell_index(d.n, ii[0], ii[1], ii[2]);
+      if (d.type != FJ_BC_FARFIELD) {
+        double s[5] = {1.0, 1.0, 1.0, 1.0, 1.0};
+        if (d.type == FJ_BC_WALL) {
+          s[1] = s[2] = s[3] = -1.0;
+        } else {
+          s[1 + ax] = -1.0;
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) d.q[v * NT + ci] += s[v] * d.q[v * NT + co];
+      }
+#pragma unroll
+      for (int v = 0; v < 5; ++v) d.q[v * NT + co] = 0.0;
+    }
+  }
+}
+
+}  // namespace
+
+int halo_transpose(fj_ctx* ctx, const fj_block* lam, int nblocks, const fj_link* links, int nlinks,
+                   int ghost, double* scratch, size_t scratch_bytes, cudaStream_t st) {
+  if (nlinks == 0) return FJ_OK;
+  if (nlinks > kMaxLinksPerLaunch)
+    return set_err(ctx, FJ_ERR_NOT_IMPLEMENTED, "adjoint halo limited to 192 links");
+  std::vector<HaloDesc> descs;
+  size_t nd = 0;
+  int s = build_links(ctx, lam, nblocks, links, nlinks, ghost, descs, nd);
+  if (s != FJ_OK) return s;
+  if (scratch_bytes < nd * sizeof(double))
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "halo scratch too small");
+  HaloTable tab;
+  tab.n = (int)descs.size();
+  int64_t vmax = 0;
+  for (int t = 0; t < tab.n; ++t) {
+    tab.d[t] = descs[t];
+    vmax = std::max<int64_t>(vmax, (int64_t)tab.d[t].ext[0] * tab.d[t].ext[1] * tab.d[t].ext[2]);
+  }
+  dim3 grid((unsigned)std::min<int64_t>(grid_for(vmax), 4096), tab.n);
+  for (int pass = 0; pass < 3; ++pass) {
+    k_halo_transpose<<<grid, kThreads, 0, st>>>(tab, scratch, pass);
+    ctx->launches += 1;
+    s = launch_status(ctx, "halo transpose launch");
+    if (s != FJ_OK) return s;
+  }
+  return FJ_OK;
+}
+
+int bc_transpose(fj_ctx* ctx, const fj_block* lam, int nblocks, const fj_bc* bcs, int nbcs,
+                 const fj_params* p, cudaStream_t st) {
+  for (int b = 0; b < nbcs; ++b) {
+    if (bcs[b].block < 0 || bcs[b].block >= nblocks || bcs[b].face < 0 || bcs[b].face > 5)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bc entry out of range");
+    if (bcs[b].type == FJ_BC_WALL && bcs[b].isothermal)
+      return set_err(ctx, FJ_ERR_NOT_IMPLEMENTED, "the adjoint of the isothermal wall is not implemented");
+  }
+  for (int face = 5; face >= 0; --face) {  // reverse of the Face-order application
+    std::vector<BcDesc> ds;
+    for (int b = 0; b < nbcs; ++b) {
+      if (bcs[b].face != face) continue;
+      const fj_block& blk = lam[bcs[b].block];
+      BcDesc d;
+      d.q = blk.q;
+      d.n[0] = blk.ni; d.n[1] = blk.nj; d.n[2] = blk.nk;
+      d.face = face;
+      d.type = bcs[b].type;
+      d.iso = 0;
+      d.T_wall = 0.0;
+      for (int v = 0; v < 5; ++v) d.qinf[v] = 0.0;
+      ds.push_back(d);
+    }
+    for (size_t base = 0; base < ds.size(); base += kMaxBcPerLaunch) {
+      BcTable tab;
+      tab.n = (int)std::min<size_t>(kMaxBcPerLaunch, ds.size() - base);
+      tab.gamma = p->gamma;
+      tab.R = p->R;
+      int64_t vmax = 0;
+      for (int t = 0; t < tab.n; ++t) {
+        tab.d[t] = ds[base + t];
+        const int ax = face >> 1;
+        vmax = std::max<int64_t>(vmax, (int64_t)tab.d[t].n[0] * tab.d[t].n[1] * tab.d[t].n[2] / tab.d[t].n[ax]);
+      }
+      dim3 grid((unsigned)std::min<int64_t>(grid_for(vmax), 4096), tab.n);
+      k_bc_transpose<<<grid, kThreads, 0, st>>>(tab, p->ghost);
+      ctx->launches += 1;
+      int s = launch_status(ctx, "bc transpose launch");
       if (s != FJ_OK) return s;
     }
   }

@@ -39,4 +39,26 @@ int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs,
 // Bytes of scratch the halo gather needs for these links (0 on shape errors).
 size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, int ghost);
 
+// ---- adjoint (fj_adjoint.cu, fj_halo.cu) ----
+// out = (dL/dq)^T lam for one block (L = the RHS parts selected by flags).
+size_t rhs_vjp_ws_bytes(int precision, int ni, int nj, int nk);
+int rhs_vjp(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol, const double* lam,
+            double* out, int ni, int nj, int nk, const fj_params* p, int flags, void* ws,
+            cudaStream_t st);
+// *acc (device) += scale * dot(x, y)
+int dot_acc(fj_ctx* ctx, const double* x, const double* y, int64_t n, double scale, double* acc,
+            cudaStream_t st);
+// grad = dJ/dq of the interior kinetic-energy integral
+int ke_grad(fj_ctx* ctx, const double* q, const double* vol, double* grad, int ni, int nj, int nk, int g,
+            cudaStream_t st);
+// out = a x + b y + c z elementwise (y, z may be null)
+int axpy3(fj_ctx* ctx, double* out, const double* x, double a, const double* y, double b,
+          const double* z, double c, int64_t n, cudaStream_t st);
+// In-place transposes of the halo fill and of the (linear) boundary conditions
+// on per-block adjoint arrays; the blocks' q pointers hold the adjoints.
+int halo_transpose(fj_ctx* ctx, const fj_block* lam, int nblocks, const fj_link* links, int nlinks,
+                   int ghost, double* scratch, size_t scratch_bytes, cudaStream_t st);
+int bc_transpose(fj_ctx* ctx, const fj_block* lam, int nblocks, const fj_bc* bcs, int nbcs,
+                 const fj_params* p, cudaStream_t st);
+
 }  // namespace fj

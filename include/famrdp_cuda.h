@@ -221,6 +221,35 @@ int fj_plan_destroy(fj_plan* plan);
 int fj_plan_stage(fj_plan* plan, double* const* q, double* const* q0, double* const* out,
                   double dt, int stage, void* stream);
 
+/* ---- adjoint (the reference differentiates step with jax.grad,
+ *      tests/solver/test_grad.py:30-35; these are hand-written reverse modes) -- */
+/* out = (dL/dq)^T lam for one block, L = _rhs_block (solver/step.py:10-15);
+ * lam and out are (5, ni, nj, nk).  Flux arithmetic follows p->precision. */
+int fj_rhs_vjp_f64(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
+                   const double* lam, double* out, int ni, int nj, int nk, const fj_params* p,
+                   void* stream);
+/* Reverse of one step (solver/step.py:18-56): given lam_in[b] = dJ/dq_new[b]
+ * for the state the step produced from blocks[b].q, writes
+ * lam_out[b] = dJ/dq[b].  The step's intermediate states are recomputed from
+ * blocks[b].q.  Supports CUT1TO1, FARFIELD, SYMMETRY and adiabatic WALL faces
+ * (an isothermal wall returns FJ_ERR_NOT_IMPLEMENTED).  lam_out may alias
+ * lam_in. */
+int fj_step_vjp_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
+                    double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
+                    const fj_bc* bcs, int nbcs, const fj_params* p, double dt, void* stream);
+/* As fj_step_vjp_f64, and also adds to *dJ_dmu0 (a device double) the
+ * derivative of J with respect to the viscosity scale mu0 through this step:
+ * the viscous RHS is linear in mu0 for both viscosity laws, so each stage
+ * contributes c_s dt lam_{s+1} . L_vis(q_s) / mu0 (c = 1, 1/4, 2/3). */
+int fj_step_vjp_mu_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
+                       double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
+                       const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dJ_dmu0,
+                       void* stream);
+/* grad[b] = dJ/dq[b] for J = sum over interior cells of vol * 0.5 |rho u|^2 / rho
+ * (the objective of fj_kinetic_energy_f64); ghost cells get 0. */
+int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* const* grad,
+                               int nblocks, int ghost, void* stream);
+
 /* time/rk.py:5-20 one Shu-Osher stage combine, elementwise over n values:
  *   stage 1: out = qs + dt*L
  *   stage 2: out = 0.75*q0 + 0.25*(qs + dt*L)
