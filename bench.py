@@ -213,6 +213,71 @@ def run_reference(args):
     return 0
 
 
+def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32")):
+    """Adjoint/forward time on the 96^3 Taylor-Green configuration (M0 0.3,
+    Re 800, constant viscosity, 1 % noise, kinetic-energy objective after 50
+    steps, a checkpoint every 10 steps), FP64 and FP32-flux, with the FP32-flux
+    gradient's relative L2 distance from the FP64 gradient.  Device time by
+    CUDA events on the stream the kernels run on; "adjoint_over_forward" is the
+    reverse sweep (segment recompute + step adjoints) over the plain forward."""
+    import dataclasses as dc
+
+    import torch
+
+    from famrdp_jax_b200 import cases
+    from famrdp_jax_b200.solver import adjoint, diagnostics
+    from famrdp_jax_b200.solver.step import StepPlan
+
+    out = {"workload": f"tgv{n}: {n}^3 cells, M0 0.3, Re 800, 1% noise, J = kinetic energy after {nsteps} steps, "
+                       f"checkpoint every {every} steps"}
+    c = cases.tgv(n=n, M0=0.3, Re=800.0, noise=0.01, seed=0)
+    grads = {}
+    stream = torch.cuda.current_stream(device)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return r, e0.elapsed_time(e1)
+
+    for prec in precisions:
+        cfg = dc.replace(c.cfg, precision=prec)
+        st = cases.to_state(c, device)
+        plan = StepPlan(st, cfg)
+        dt = diagnostics.cfl_dt(st, cfg, c.cfl)
+        qa = [st.blocks[0].q.clone()]
+        qb = [torch.empty_like(qa[0])]
+        for _ in range(3):
+            plan.run(qa, qb, dt)
+
+        def fwd():
+            a, b = qa, qb
+            for _ in range(nsteps):
+                plan.run(a, b, dt)
+                a, b = b, a
+
+        _, t_fwd = timed(fwd)
+        adjoint.adjoint_kinetic_energy(st, cfg, dt, 2, checkpoint_every=1, plan=plan)  # warm-up
+        run = adjoint._Run(cfg=cfg, metrics=st.metrics, dt=float(dt), nsteps=nsteps, every=every, plan=plan,
+                           tables=adjoint._Tables(cfg), dmu=torch.zeros(1, dtype=torch.float64, device=device))
+        (final, checkpoints), t_ckpt = timed(lambda: adjoint._forward_with_checkpoints(run, [st.blocks[0].q]))
+        lams = adjoint.kinetic_energy_grad(final, st.metrics, cfg.ghost)
+        g, t_rev = timed(lambda: adjoint._reverse_sweep(run, checkpoints, lams))
+        fstate = dc.replace(st, blocks=(dc.replace(st.blocks[0], q=final[0]),))
+        J = diagnostics.kinetic_energy(fstate, cfg.ghost)
+        grads[prec] = g[0]
+        out[prec] = {"forward_ms_per_step": t_fwd / nsteps, "checkpointed_forward_ms_per_step": t_ckpt / nsteps,
+                     "reverse_sweep_ms_per_step": t_rev / nsteps, "adjoint_over_forward": t_rev / t_fwd,
+                     "J": J, "dJ_dmu0": float(run.dmu.item())}
+    if len(grads) == 2:
+        out["f32_vs_f64_grad_rel_l2"] = float(torch.linalg.vector_norm(grads["f32"] - grads["f64"]) /
+                                              torch.linalg.vector_norm(grads["f64"]))
+    return out
+
+
 def _max_over_ranks(x: float, ws: int, device) -> float:
     if ws == 1:
         return x
@@ -348,6 +413,8 @@ def run_ours(args):
            "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps}
 
     cpu = cpu_oracle_sample(case, dt) if (rank == 0 and not args.no_cpu) else None
+    adj = (adjoint_timing(device, args.adjoint_n, args.adjoint_steps, args.adjoint_every)
+           if (rank == 0 and not args.no_adjoint) else None)
     if rank == 0:
         r = results[args.precision]
         line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -359,7 +426,7 @@ def run_ours(args):
                 "variants": {p: results[p] for p in order} | {
                     "f32_vs_f64_rel_l2": err_f32,
                     "f32_vs_f64_note": f"whole state after {warm + args.steps} steps from the same start"},
-                "dt": dt}
+                "adjoint": adj, "dt": dt}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()
@@ -378,7 +445,24 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="print only the adjoint/forward timing (one JSON line)")
+    ap.add_argument("--adjoint-n", type=int, default=96)
+    ap.add_argument("--adjoint-steps", type=int, default=50)
+    ap.add_argument("--adjoint-every", type=int, default=10)
+    ap.add_argument("--adjoint-precision", choices=["both", "f32", "f64"], default="both")
+    ap.add_argument("--adjoint-variant", type=int, default=0, help="face-VJP launch shape (0..2)")
     args = ap.parse_args(argv)
+    if args.adjoint_only:
+        import torch
+
+        from famrdp_jax_b200 import _capi
+        _capi.set_adjoint_variant(args.adjoint_variant, torch.device("cuda:0"))
+        precs = ("f64", "f32") if args.adjoint_precision == "both" else (args.adjoint_precision,)
+        print(json.dumps(adjoint_timing(torch.device("cuda:0"), args.adjoint_n, args.adjoint_steps,
+                                        args.adjoint_every, precs)), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -70,9 +70,12 @@ SIGNATURES = {
     "fj_last_error": (ctypes.c_char_p, [_P]),
     "fj_launch_count": (_I, [_P, ctypes.POINTER(_I64)]),
     "fj_ctx_set_pipeline": (_I, [_P, _I, _I, _I]),
+    "fj_ctx_set_adjoint_variant": (_I, [_P, _I]),
     "fj_plan_create": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjLink), _I, ctypes.POINTER(FjBc), _I,
                             ctypes.POINTER(FjParams), ctypes.POINTER(_P)]),
     "fj_plan_step": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
+    "fj_plan_step_save": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                               ctypes.POINTER(_P), _D, _P]),
     "fj_plan_destroy": (_I, [_P]),
     "fj_plan_stage": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _I, _P]),
     "fj_rhs_vjp_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _P]),
@@ -81,6 +84,9 @@ SIGNATURES = {
     "fj_step_vjp_mu_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), ctypes.POINTER(_P), _I,
                                 ctypes.POINTER(FjLink), _I, ctypes.POINTER(FjBc), _I, ctypes.POINTER(FjParams), _D,
                                 _P, _P]),
+    "fj_step_vjp_saved_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                                   ctypes.POINTER(_P), ctypes.POINTER(_P), _I, ctypes.POINTER(FjLink), _I,
+                                   ctypes.POINTER(FjBc), _I, ctypes.POINTER(FjParams), _D, _P, _P]),
     "fj_kinetic_energy_grad_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), _I, _I, _P]),
     "fj_rk_stage_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _D, _I, _P]),
     "fj_cons_to_prim_f64": (_I, [_P, _P, _I64, _D, _P]),
@@ -165,6 +171,13 @@ def set_pipeline(pipeline: str = DEFAULT_PIPELINE, seg: int = 0, tile: str | int
     c = ctx(device)
     t = TILES[tile] if isinstance(tile, str) else int(tile)
     check(lib().fj_ctx_set_pipeline(c, PIPELINES[pipeline], int(seg), t), "fj_ctx_set_pipeline", c)
+
+
+def set_adjoint_variant(variant: int = 0, device=None) -> None:
+    """Launch shape of the adjoint's face kernel (0 = register-capped default,
+    1 = uncapped, 2 = the other cap)."""
+    c = ctx(device)
+    check(lib().fj_ctx_set_adjoint_variant(c, int(variant)), "fj_ctx_set_adjoint_variant", c)
 
 
 def launch_count(device=None) -> int:

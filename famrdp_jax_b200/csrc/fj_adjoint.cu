@@ -23,6 +23,7 @@
 // forward kernels, then applies the transposed stage combines and RHS VJPs
 // in reverse (solver/step.py:45-53) and finally the transposed boundary
 // conditions and halo fill (mesh/halo.py:56-92, physics/bc/*.py).
+#include <algorithm>
 #include <vector>
 
 #include "fj_adjoint.cuh"
@@ -75,65 +76,115 @@ __global__ void k_adj_prims(const double* __restrict__ q, T* __restrict__ P, int
 __device__ __forceinline__ void atomic_add(float* a, float v) { atomicAdd(a, v); }
 __device__ __forceinline__ void atomic_add(double* a, double v) { atomicAdd(a, v); }
 
+// Face c | c+e_a (stride sa): loads the four MUSCL cells and the two cells'
+// metric rows, then the reverse of MUSCL + Roe; lc[s][v] = adjoint of the
+// primitive v (rho, u, v, w, p) of cell c + (s-1) e_a.
 template <typename T>
-__global__ void k_adj_faces(const T* __restrict__ P, const double* __restrict__ kxyz,
-                            const double* __restrict__ vol, const double* __restrict__ lam,
-                            T* __restrict__ lamP, ADims d, Phys ph) {
-  const int N = d.ni * d.nj * d.nk;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= N) return;
-  int i, j, k;
-  dec(c, d, i, j, k);
-  const int idx[3] = {i, j, k}, n[3] = {d.ni, d.nj, d.nk};
-  const int st[3] = {d.nj * d.nk, d.nk, 1};
+__device__ __forceinline__ void face_vjp_cells(const T* __restrict__ P, const double* __restrict__ K, int N,
+                                               int c, int sa, const T lF[5], const Phys& ph, T lc[4][5]) {
+  Prim<T> cell[4], l4[4];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (idx[a] < 1 || idx[a] > n[a] - 3) continue;
-    const int cr = c + st[a];
-    const bool inL = idx[a] >= 2, inR = idx[a] + 1 <= n[a] - 3;
-    const double ivl = inL ? 1.0 / (vol[c] + 1e-300) : 0.0;
-    const double ivr = inR ? 1.0 / (vol[cr] + 1e-300) : 0.0;
-    T lF[5];
-    bool any = false;
+  for (int s = 0; s < 4; ++s) {
+    const int cc = c + (s - 1) * sa;
+    cell[s] = Prim<T>{P[cc], P[N + cc], P[2 * N + cc], P[3 * N + cc], P[4 * N + cc]};
+    l4[s] = Prim<T>{T(0), T(0), T(0), T(0), T(0)};
+  }
+  const int cr = c + sa;
+  invscd_face_vjp<T>(cell, (T)K[c], (T)K[N + c], (T)K[2 * N + c], (T)K[cr], (T)K[N + cr], (T)K[2 * N + cr],
+                     (T)ph.gm1, (T)ph.inv_gm1, (T)ph.eps_entropy, ph.limiter, lF, l4);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      const double x = (inL ? -lam[v * N + c] * ivl : 0.0) + (inR ? lam[v * N + cr] * ivr : 0.0);
-      lF[v] = (T)x;
-      any |= x != 0.0;
-    }
-    if (!any) continue;
-    Prim<T> cell[4], lc[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int cc = c + (s - 1) * st[a];
-      cell[s] = Prim<T>{P[cc], P[N + cc], P[2 * N + cc], P[3 * N + cc], P[4 * N + cc]};
-      lc[s] = Prim<T>{T(0), T(0), T(0), T(0), T(0)};
-    }
-    const double* K = kxyz + (size_t)(3 * a) * N;
-    invscd_face_vjp<T>(cell, (T)K[c], (T)K[N + c], (T)K[2 * N + c], (T)K[cr], (T)K[N + cr],
-                       (T)K[2 * N + cr], (T)ph.gm1, (T)ph.inv_gm1, (T)ph.eps_entropy, ph.limiter, lF,
-                       lc);
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int cc = c + (s - 1) * st[a];
-      atomic_add(lamP + cc, lc[s].rho);
-      atomic_add(lamP + N + cc, lc[s].u);
-      atomic_add(lamP + 2 * N + cc, lc[s].v);
-      atomic_add(lamP + 3 * N + cc, lc[s].w);
-      atomic_add(lamP + 4 * N + cc, lc[s].p);
-    }
+  for (int s = 0; s < 4; ++s) {
+    lc[s][0] = l4[s].rho;
+    lc[s][1] = l4[s].u;
+    lc[s][2] = l4[s].v;
+    lc[s][3] = l4[s].w;
+    lc[s][4] = l4[s].p;
   }
 }
 
-// lamD: 12 x N (s-major: u, v, w, T; l = 0..2), lamL: 4 x N (local u, v, w, T)
 template <typename T>
-__global__ void k_adj_visc(const T* __restrict__ P, const double* __restrict__ kxyz,
-                           const double* __restrict__ lam, T* __restrict__ lamD,
-                           T* __restrict__ lamL, ADims d, Phys ph) {
+__device__ __forceinline__ void add_cell(T* __restrict__ lamP, int N, int c, const T v[5]) {
+#pragma unroll
+  for (int f = 0; f < 5; ++f)
+    if (v[f] != T(0)) atomic_add(lamP + f * N + c, v[f]);
+}
+
+// The inviscid part of the RHS VJP (reverse of rhs/invscd.py:119-131 and of
+// MUSCL + Roe), accumulated into lamP.  One thread per face c | c+e_a over the
+// linear cell index c, blockIdx.y = the face axis a.  Face adjoint
+// lamF = -lam(c)/vol(c) [2 <= c_a <= n_a-3] + lam(c+e_a)/vol(c+e_a)
+// [c_a+1 <= n_a-3] for faces 1 <= c_a <= n_a-3, in FP64 as the forward's flux
+// difference.  Along k (a = 2) the four contributions to a cell x come from
+// lanes x+1, x, x-1, x-2 of the same warp and are combined by shuffles, so only
+// each cell's total and the contributions that leave the warp use atomics
+// (faces at the ends of a k row are invalid and contribute zero, so a warp that
+// spans two rows combines correctly); along i and j each face adds its four
+// cells' adjoints atomically.
+template <typename T, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, const double* __restrict__ kxyz,
+                                                      const double* __restrict__ vol, const double* __restrict__ lam,
+                                                      T* __restrict__ lamP, ADims d, Phys ph) {
+  const int N = d.ni * d.nj * d.nk;
+  if (blockIdx.x * blockDim.x >= (unsigned)N) return;  // whole block past the end (uniform)
+  const int a = blockIdx.y;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n_a = a == 0 ? d.ni : (a == 1 ? d.nj : d.nk);
+  const int sa = a == 0 ? d.nj * d.nk : (a == 1 ? d.nk : 1);
+  T lc[4][5];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int f = 0; f < 5; ++f) lc[s][f] = T(0);
+  if (c < N) {
+    const int ia = a == 0 ? c / (d.nj * d.nk) : (a == 1 ? (c / d.nk) % d.nj : c % d.nk);
+    if (ia >= 1 && ia <= n_a - 3) {
+      const bool inL = ia >= 2, inR = ia + 1 <= n_a - 3;
+      const int cr = c + sa;
+      const double ivl = inL ? 1.0 / (vol[c] + 1e-300) : 0.0;
+      const double ivr = inR ? 1.0 / (vol[cr] + 1e-300) : 0.0;
+      T lF[5];
+      bool any = false;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const double x = (inL ? -lam[v * N + c] * ivl : 0.0) + (inR ? lam[v * N + cr] * ivr : 0.0);
+        lF[v] = (T)x;
+        any |= x != 0.0;
+      }
+      if (any) face_vjp_cells<T>(P, kxyz + (size_t)(3 * a) * N, N, c, sa, lF, ph, lc);
+    }
+  }
+  if (a != 2) {
+    if (c < N)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) add_cell<T>(lamP, N, c + (s - 1) * sa, lc[s]);
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  T own[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    const T from_right = __shfl_down_sync(0xffffffffu, lc[0][f], 1);  // lane x+1's face, cell x
+    const T from_left = __shfl_up_sync(0xffffffffu, lc[2][f], 1);     // lane x-1's face, cell x
+    const T from_left2 = __shfl_up_sync(0xffffffffu, lc[3][f], 2);    // lane x-2's face, cell x
+    own[f] = lc[1][f] + (lane < 31 ? from_right : T(0)) + (lane >= 1 ? from_left : T(0)) +
+             (lane >= 2 ? from_left2 : T(0));
+  }
+  if (c < N) add_cell<T>(lamP, N, c, own);
+  if (lane == 0) add_cell<T>(lamP, N, c - 1, lc[0]);  // nonzero only for a valid face, so c >= 1
+  if (lane == 31) add_cell<T>(lamP, N, c + 1, lc[2]);
+  if (lane >= 30) add_cell<T>(lamP, N, c + 2, lc[3]);
+}
+
+// lamD: 12 x N (s-major: u, v, w, T; l = 0..2), lamL: 4 x N (local u, v, w, T).
+// If dmu is set, also *dmu += mu_scale * sum_y lamG(y) . G(y): the viscous RHS
+// is L_vis = D G with G linear in mu0, so lam . dL_vis/dmu0 = (D^T lam) . G / mu0.
+template <typename T>
+__device__ __forceinline__ double adj_visc_cell(const T* __restrict__ P, const double* __restrict__ kxyz,
+                                                const double* __restrict__ lam, T* __restrict__ lamD,
+                                                T* __restrict__ lamL, const ADims& d, const Phys& ph, int y,
+                                                bool want_dot) {
   using M = FastMath<T>;
   const int N = d.ni * d.nj * d.nk;
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
-  if (y >= N) return;
   int i, j, k;
   dec(y, d, i, j, k);
   int nb[6];
@@ -192,6 +243,14 @@ __global__ void k_adj_visc(const T* __restrict__ P, const double* __restrict__ k
   const T t00 = T(2) * mu * (g[0][0] - div_u * third), t11 = T(2) * mu * (g[1][1] - div_u * third),
           t22 = T(2) * mu * (g[2][2] - div_u * third);
   const T t01 = mu * (g[0][1] + g[1][0]), t02 = mu * (g[0][2] + g[2][0]), t12 = mu * (g[1][2] + g[2][1]);
+  double dot = 0.0;
+  if (want_dot) {
+    const T ge0 = u * t00 + v * t01 + w * t02 + kappa * g[3][0];
+    const T ge1 = u * t01 + v * t11 + w * t12 + kappa * g[3][1];
+    const T ge2 = u * t02 + v * t12 + w * t22 + kappa * g[3][2];
+    dot = lG[0] * t00 + lG[1] * t01 + lG[2] * t02 + lG[3] * t11 + lG[4] * t12 + lG[5] * t22 + lG[6] * ge0 +
+          lG[7] * ge1 + lG[8] * ge2;
+  }
   // ---- reverse
   const T lGe0 = (T)lG[6], lGe1 = (T)lG[7], lGe2 = (T)lG[8];
   T lt00 = (T)lG[0] + lGe0 * u, lt01 = (T)lG[1] + lGe0 * v + lGe1 * u, lt02 = (T)lG[2] + lGe0 * w + lGe2 * u;
@@ -228,12 +287,29 @@ __global__ void k_adj_visc(const T* __restrict__ P, const double* __restrict__ k
   lamL[N + y] = lv;
   lamL[2 * N + y] = lw;
   lamL[3 * N + y] = lT;
+  return dot;
+}
+
+template <typename T>
+__global__ void k_adj_visc(const T* __restrict__ P, const double* __restrict__ kxyz,
+                           const double* __restrict__ lam, T* __restrict__ lamD,
+                           T* __restrict__ lamL, ADims d, Phys ph, double* __restrict__ dmu,
+                           double mu_scale) {
+  const int N = d.ni * d.nj * d.nk;
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  double dot = 0.0;
+  if (y < N) dot = adj_visc_cell<T>(P, kxyz, lam, lamD, lamL, d, ph, y, dmu != nullptr);
+  if (dmu) {  // warp reduction (all lanes take part), one atomic per warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
+    if ((threadIdx.x & 31) == 0 && dot != 0.0) atomicAdd(dmu, mu_scale * dot);
+  }
 }
 
 template <typename T>
 __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ lamP,
                             const T* __restrict__ lamD, const T* __restrict__ lamL,
-                            double* __restrict__ out, ADims d, Phys ph, int flags) {
+                            double* __restrict__ out, ADims d, Phys ph, int flags, VjpEpilogue e) {
   const int N = d.ni * d.nj * d.nk;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= N) return;
@@ -279,11 +355,28 @@ __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ 
   lu += lke * u;
   lv += lke * v;
   lw += lke * w;
-  out[N + x] = lu * ir;
-  out[2 * N + x] = lv * ir;
-  out[3 * N + x] = lw * ir;
-  out[4 * N + x] = lq4;
-  out[x] = lr - (lu * u + lv * v + lw * w) * ir;
+  const double V[5] = {lr - (lu * u + lv * v + lw * w) * ir, lu * ir, lv * ir, lw * ir, lq4};
+  if (!e.o1) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f) out[f * N + x] = V[f];
+    return;
+  }
+  double o1[5], o2[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    const int t = f * N + x;
+    o1[f] = e.a1 * e.x1[t] + e.e1 * V[f];
+    if (e.y1) o1[f] += e.b1 * e.y1[t];
+    if (e.o2) {
+      o2[f] = e.a2 * e.x2[t];
+      if (e.y2) o2[f] += e.b2 * e.y2[t];
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    e.o1[f * N + x] = o1[f];
+    if (e.o2) e.o2[f * N + x] = o2[f];
+  }
 }
 
 // out = a x + b y + c z (y, z may be null)
@@ -347,7 +440,7 @@ size_t vjp_ws(int64_t N) {
 template <typename T>
 int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
                  const double* lam, double* out, int ni, int nj, int nk, const Phys& ph, int flags,
-                 void* ws, cudaStream_t st) {
+                 void* ws, cudaStream_t st, double* dmu, double mu_scale, const VjpEpilogue* epi) {
   const int N = ni * nj * nk;
   auto al = [](char* p) { return (char*)(((uintptr_t)p + 255) & ~(uintptr_t)255); };
   char* p = al((char*)ws);
@@ -365,14 +458,30 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
   if (flags & kRhsInvscd) {
     cudaError_t e = cudaMemsetAsync(lamP, 0, 5 * (size_t)N * sizeof(T), st);
     if (e != cudaSuccess) return cuda_status(ctx, e, "vjp memset");
-    k_adj_faces<T><<<grid, kAT, 0, st>>>(P, kxyz, vol, lam, lamP, d, ph);
+    // register caps (threads per CTA, minimum CTAs per SM): the FP64 face VJP
+    // needs ~180 registers uncapped; variant 0 trades a few spilled values for
+    // 12 resident warps (FP64) or 24 (FP32)
+    auto launch = [&](auto kern, int nt) {
+      kern<<<dim3((unsigned)((N + nt - 1) / nt), 3), nt, 0, st>>>(P, kxyz, vol, lam, lamP, d, ph);
+    };
+    constexpr bool f64 = sizeof(T) == 8;
+    switch (ctx->adj_variant) {
+      case 1: launch(k_adj_faces<T, 256, 1>, 256); break;
+      case 2:
+        if (f64) launch(k_adj_faces<T, 128, 4>, 128);
+        else launch(k_adj_faces<T, 256, 2>, 256);
+        break;
+      default:
+        if (f64) launch(k_adj_faces<T, 128, 3>, 128);
+        else launch(k_adj_faces<T, 256, 3>, 256);
+    }
     ctx->launches += 1;
   }
   if (flags & kRhsViscous) {
-    k_adj_visc<T><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph);
+    k_adj_visc<T><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale);
     ctx->launches += 1;
   }
-  k_adj_final<T><<<grid, kAT, 0, st>>>(q, lamP, lamD, lamL, out, d, ph, flags);
+  k_adj_final<T><<<grid, kAT, 0, st>>>(q, lamP, lamD, lamL, out, d, ph, flags, epi ? *epi : VjpEpilogue{});
   ctx->launches += 1;
   return launch_status(ctx, "rhs vjp launch");
 }
@@ -386,11 +495,11 @@ size_t rhs_vjp_ws_bytes(int precision, int ni, int nj, int nk) {
 
 int rhs_vjp(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol, const double* lam,
             double* out, int ni, int nj, int nk, const fj_params* p, int flags, void* ws,
-            cudaStream_t st) {
+            cudaStream_t st, double* dmu, double mu_scale, const VjpEpilogue* epi) {
   const Phys ph = make_phys(p);
   if (p->precision == FJ_PREC_F32FLUX)
-    return rhs_vjp_impl<float>(ctx, q, kxyz, vol, lam, out, ni, nj, nk, ph, flags, ws, st);
-  return rhs_vjp_impl<double>(ctx, q, kxyz, vol, lam, out, ni, nj, nk, ph, flags, ws, st);
+    return rhs_vjp_impl<float>(ctx, q, kxyz, vol, lam, out, ni, nj, nk, ph, flags, ws, st, dmu, mu_scale, epi);
+  return rhs_vjp_impl<double>(ctx, q, kxyz, vol, lam, out, ni, nj, nk, ph, flags, ws, st, dmu, mu_scale, epi);
 }
 
 int dot_acc(fj_ctx* ctx, const double* x, const double* y, int64_t n, double scale, double* acc,

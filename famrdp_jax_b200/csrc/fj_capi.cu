@@ -164,20 +164,22 @@ size_t step_layout(const fj_ctx* ctx, const fj_block* blocks, int nblocks, const
   return 2 * *stage_b + *tail_b;
 }
 
-// solver/step.py:18-56 on the device: q_out := q, halo + BC in place on q_out,
+// solver/step.py:18-56 on the device: q0p := q, halo + BC in place on q0p,
 // then the three stages of each block (blocks do not interact between the halo
-// fill and the end of the step, solver/step.py:40-53).
-int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int nblocks,
-              const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs, const fj_params* p,
-              double dt, float* const* kxyz32, double* q1, double* q2, void* tail, size_t tail_b,
-              cudaStream_t st) {
+// fill and the end of the step, solver/step.py:40-53): q1s := stage 1 of q0p,
+// q2s := stage 2, q_out := stage 3.  q0p may equal q_out (the stage-3 kernels
+// read q0 only at the cell they write).
+int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* const* q1s,
+              double* const* q2s, double* const* q_out, int nblocks, const fj_link* links, int nlinks,
+              const fj_bc* bcs, int nbcs, const fj_params* p, double dt, float* const* kxyz32, void* tail,
+              size_t tail_b, cudaStream_t st) {
   std::vector<fj_block> out(blocks, blocks + nblocks);
   int s;
   for (int b = 0; b < nblocks; ++b) {
-    out[b].q = q_out[b];
-    if (q_out[b] != blocks[b].q) {
+    out[b].q = q0p[b];
+    if (q0p[b] != blocks[b].q) {
       const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
-      s = cuda_status(ctx, cudaMemcpyAsync(q_out[b], blocks[b].q, bytes, cudaMemcpyDeviceToDevice, st),
+      s = cuda_status(ctx, cudaMemcpyAsync(q0p[b], blocks[b].q, bytes, cudaMemcpyDeviceToDevice, st),
                       "state copy");
       if (s != FJ_OK) return s;
     }
@@ -188,17 +190,11 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int nbl
   if (s != FJ_OK) return s;
   const int flags = kRhsInvscd | kRhsViscous;
   if (ctx->pipeline == FJ_PIPELINE_SPLIT) {
-    // all blocks per launch: q1/q2 hold every block (step_layout), the tail
-    // holds the intermediates of every block
+    // all blocks per launch; the tail holds the intermediates of every block
     std::vector<SplitBlock> sb(nblocks);
-    std::vector<double*> b1(nblocks), b2(nblocks);
-    size_t off = 0;
     for (int b = 0; b < nblocks; ++b) {
       const fj_block& B = out[b];
-      b1[b] = (double*)((char*)q1 + off);
-      b2[b] = (double*)((char*)q2 + off);
-      off += align256(5 * (size_t)B.ni * B.nj * B.nk * sizeof(double));
-      sb[b] = split_block(B.q, B.q, b1[b], B.kxyz,
+      sb[b] = split_block(B.q, B.q, q1s[b], B.kxyz,
                           (p->precision == FJ_PREC_F32FLUX && kxyz32) ? kxyz32[b] : nullptr, B.vol, B.ni,
                           B.nj, B.nk);
     }
@@ -207,28 +203,44 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int nbl
     s = split_stage(ctx, sb.data(), nblocks, ph, flags, 1, dt, p->precision, st);
     if (s != FJ_OK) return s;
     for (int b = 0; b < nblocks; ++b) {
-      sb[b].q = b1[b];
-      sb[b].out = b2[b];
+      sb[b].q = q1s[b];
+      sb[b].out = q2s[b];
     }
     s = split_stage(ctx, sb.data(), nblocks, ph, flags, 2, dt, p->precision, st);
     if (s != FJ_OK) return s;
     for (int b = 0; b < nblocks; ++b) {
-      sb[b].q = b2[b];
-      sb[b].out = out[b].q;
+      sb[b].q = q2s[b];
+      sb[b].out = q_out[b];
     }
     return split_stage(ctx, sb.data(), nblocks, ph, flags, 3, dt, p->precision, st);
   }
   for (int b = 0; b < nblocks; ++b) {
     const fj_block& B = out[b];
     const float* k32 = kxyz32 ? kxyz32[b] : nullptr;
-    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, q1, B.ni, B.nj, B.nk, p, flags, 1, dt, tail, st, k32);
+    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, q1s[b], B.ni, B.nj, B.nk, p, flags, 1, dt, tail, st, k32);
     if (s != FJ_OK) return s;
-    s = run_rhs(ctx, q1, B.kxyz, B.vol, B.q, q2, B.ni, B.nj, B.nk, p, flags, 2, dt, tail, st, k32);
+    s = run_rhs(ctx, q1s[b], B.kxyz, B.vol, B.q, q2s[b], B.ni, B.nj, B.nk, p, flags, 2, dt, tail, st, k32);
     if (s != FJ_OK) return s;
-    s = run_rhs(ctx, q2, B.kxyz, B.vol, B.q, B.q, B.ni, B.nj, B.nk, p, flags, 3, dt, tail, st, k32);
+    s = run_rhs(ctx, q2s[b], B.kxyz, B.vol, B.q, q_out[b], B.ni, B.nj, B.nk, p, flags, 3, dt, tail, st, k32);
     if (s != FJ_OK) return s;
   }
   return FJ_OK;
+}
+
+// Per-block stage pointers into a [q1 all blocks | q2 all blocks] scratch of
+// step_layout's stage_b bytes each (the non-split pipelines run block by block
+// and share one block-sized q1/q2).
+void stage_ptrs(const fj_ctx* ctx, const fj_block* blocks, int nblocks, void* scratch, size_t stage_b,
+                std::vector<double*>& q1s, std::vector<double*>& q2s) {
+  q1s.resize(nblocks);
+  q2s.resize(nblocks);
+  size_t off = 0;
+  const bool split = ctx->pipeline == FJ_PIPELINE_SPLIT;
+  for (int b = 0; b < nblocks; ++b) {
+    q1s[b] = (double*)((char*)scratch + (split ? off : 0));
+    q2s[b] = (double*)((char*)scratch + stage_b + (split ? off : 0));
+    off += align256(5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double));
+  }
 }
 
 }  // namespace
@@ -283,6 +295,13 @@ int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg, int tile) {
   ctx->pipeline = pipeline;
   ctx->seg = seg;
   ctx->tile = tile;
+  return FJ_OK;
+}
+
+int fj_ctx_set_adjoint_variant(fj_ctx* ctx, int variant) {
+  if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
+  if (variant < 0 || variant >= FJ_NUM_ADJ_VARIANTS) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown variant");
+  ctx->adj_variant = variant;
   return FJ_OK;
 }
 
@@ -401,11 +420,11 @@ int fj_step_f64(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, int n
   size_t stage_b = 0, tail_b = 0;
   s = ensure_ws(ctx, step_layout(ctx, blocks, nblocks, links, nlinks, p, &stage_b, &tail_b));
   if (s != FJ_OK) return s;
-  double* q1 = (double*)ctx->ws;
-  double* q2 = (double*)((char*)ctx->ws + stage_b);
+  std::vector<double*> q1s, q2s;
+  stage_ptrs(ctx, blocks, nblocks, ctx->ws, stage_b, q1s, q2s);
   void* tail = (char*)ctx->ws + 2 * stage_b;
-  return step_body(ctx, blocks, q_out, nblocks, links, nlinks, bcs, nbcs, p, dt, nullptr, q1, q2, tail,
-                   tail_b, S(stream));
+  return step_body(ctx, blocks, q_out, q1s.data(), q2s.data(), q_out, nblocks, links, nlinks, bcs, nbcs, p, dt,
+                   nullptr, tail, tail_b, S(stream));
 }
 
 int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
@@ -458,7 +477,8 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
   return FJ_OK;
 }
 
-int fj_plan_step(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, void* stream) {
+static int plan_step_impl(fj_plan* pl, double* const* q_in, double* const* q_out, double* const* q0_save,
+                          double* const* q1_save, double* const* q2_save, double dt, void* stream) {
   if (!pl) return FJ_ERR_INVALID_ARGUMENT;
   fj_ctx* ctx = pl->ctx;
   const int nb = (int)pl->blocks.size();
@@ -468,16 +488,35 @@ int fj_plan_step(fj_plan* pl, double* const* q_in, double* const* q_out, double 
     if (!q_in[b] || !q_out[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "state pointer is NULL");
     in[b].q = q_in[b];
   }
-  double* q1 = (double*)pl->scratch;
-  double* q2 = (double*)((char*)pl->scratch + pl->stage_bytes);
-  void* tail = (char*)pl->scratch + 2 * pl->stage_bytes;
   const int saved = ctx->pipeline;
   ctx->pipeline = pl->pipeline;  // the scratch was laid out for this pipeline
-  int s = step_body(ctx, in.data(), q_out, nb, pl->links.data(), (int)pl->links.size(), pl->bcs.data(),
-                    (int)pl->bcs.size(), &pl->p, dt, pl->kxyz32.empty() ? nullptr : pl->kxyz32.data(), q1, q2,
-                    tail, pl->halo_bytes, S(stream));
+  std::vector<double*> q1s, q2s;
+  if (q0_save) {
+    q1s.assign(q1_save, q1_save + nb);
+    q2s.assign(q2_save, q2_save + nb);
+  } else {
+    stage_ptrs(ctx, pl->blocks.data(), nb, pl->scratch, pl->stage_bytes, q1s, q2s);
+  }
+  void* tail = (char*)pl->scratch + 2 * pl->stage_bytes;
+  int s = step_body(ctx, in.data(), q0_save ? q0_save : q_out, q1s.data(), q2s.data(), q_out, nb,
+                    pl->links.data(), (int)pl->links.size(), pl->bcs.data(), (int)pl->bcs.size(), &pl->p, dt,
+                    pl->kxyz32.empty() ? nullptr : pl->kxyz32.data(), tail, pl->halo_bytes, S(stream));
   ctx->pipeline = saved;
   return s;
+}
+
+int fj_plan_step(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, void* stream) {
+  return plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);
+}
+
+int fj_plan_step_save(fj_plan* pl, double* const* q_in, double* const* q_out, double* const* q0_save,
+                      double* const* q1_save, double* const* q2_save, double dt, void* stream) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  if (!q0_save || !q1_save || !q2_save) return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "save lists are NULL");
+  for (size_t b = 0; b < pl->blocks.size(); ++b)
+    if (!q0_save[b] || !q1_save[b] || !q2_save[b])
+      return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "save pointer is NULL");
+  return plan_step_impl(pl, q_in, q_out, q0_save, q1_save, q2_save, dt, stream);
 }
 
 int fj_plan_stage(fj_plan* pl, double* const* q, double* const* q0, double* const* out, double dt,
@@ -529,15 +568,16 @@ int fj_rhs_vjp_f64(fj_ctx* ctx, const double* q, const double* kxyz, const doubl
   return rhs_vjp(ctx, q, kxyz, vol, lam, out, ni, nj, nk, p, kRhsInvscd | kRhsViscous, ctx->ws, S(stream));
 }
 
-static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
-                         double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
-                         const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dmu,
-                         void* stream);
+static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* q1_saved,
+                         const double* const* q2_saved, const double* const* lam_in, double* const* lam_out,
+                         int nblocks, const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs,
+                         const fj_params* p, double dt, double* dmu, void* stream);
 
 int fj_step_vjp_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
                     double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
                     const fj_bc* bcs, int nbcs, const fj_params* p, double dt, void* stream) {
-  return step_vjp_impl(ctx, blocks, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt, nullptr, stream);
+  return step_vjp_impl(ctx, blocks, nullptr, nullptr, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt,
+                       nullptr, stream);
 }
 
 int fj_step_vjp_mu_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
@@ -545,7 +585,20 @@ int fj_step_vjp_mu_f64(fj_ctx* ctx, const fj_block* blocks, const double* const*
                        const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dJ_dmu0,
                        void* stream) {
   if (!dJ_dmu0) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "dJ_dmu0 is NULL");
-  return step_vjp_impl(ctx, blocks, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt, dJ_dmu0, stream);
+  return step_vjp_impl(ctx, blocks, nullptr, nullptr, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt,
+                       dJ_dmu0, stream);
+}
+
+int fj_step_vjp_saved_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* q1,
+                          const double* const* q2, const double* const* lam_in, double* const* lam_out,
+                          int nblocks, const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs,
+                          const fj_params* p, double dt, double* dJ_dmu0, void* stream) {
+  if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
+  if (!q1 || !q2) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "saved stage lists are NULL");
+  for (int b = 0; b < nblocks; ++b)
+    if (!q1[b] || !q2[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "saved stage pointer is NULL");
+  return step_vjp_impl(ctx, blocks, q1, q2, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt, dJ_dmu0,
+                       stream);
 }
 
 int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* const* grad, int nblocks,
@@ -560,10 +613,12 @@ int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* cons
   return FJ_OK;
 }
 
-static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
-                         double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
-                         const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dmu,
-                         void* stream) {
+// Reverse of one step.  Without saved states, q0' (copy + halo + BC), q1 and
+// q2 are recomputed first; with them, blocks[b].q is q0' and q1/q2 are read.
+static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* q1_saved,
+                         const double* const* q2_saved, const double* const* lam_in, double* const* lam_out,
+                         int nblocks, const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs,
+                         const fj_params* p, double dt, double* dmu, void* stream) {
   if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
   if (!lam_in || !lam_out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "adjoint lists are NULL");
   std::vector<double*> dummy(nblocks > 0 ? nblocks : 1, nullptr);
@@ -575,75 +630,85 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
   for (int b = 0; b < nbcs; ++b)
     if (bcs[b].type == FJ_BC_WALL && bcs[b].isothermal)
       return set_err(ctx, FJ_ERR_NOT_IMPLEMENTED, "the adjoint of the isothermal wall is not implemented");
+  const bool saved = q1_saved != nullptr;
   cudaStream_t st = S(stream);
-  // layout: [Q0 all blocks][L0 all blocks][Q1][Q2][LA][LB][V][work]
+  // layout: [Q0 all blocks, unless saved][L0 all blocks][Q1][Q2][LA][LB][work]
+  // (Q1/Q2 only without saved states)
   size_t sum5 = 0, max5 = 0, work = 256;
   for (int b = 0; b < nblocks; ++b) {
     const size_t by = align256(5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double));
     sum5 += by;
     max5 = std::max(max5, by);
-    work = std::max(work, rhs_scratch_bytes(ctx, p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
+    if (!saved) work = std::max(work, rhs_scratch_bytes(ctx, p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
     work = std::max(work, rhs_vjp_ws_bytes(p->precision, blocks[b].ni, blocks[b].nj, blocks[b].nk));
   }
   work = std::max(work, halo_ws_bytes(blocks, links, nlinks, p->ghost));
   work = align256(work);
-  s = ensure_ws(ctx, 2 * sum5 + 6 * max5 + work);
+  const size_t q0_bytes = saved ? 0 : sum5;
+  const int nstage = saved ? 0 : 2;
+  s = ensure_ws(ctx, q0_bytes + sum5 + (nstage + 2) * max5 + work);
   if (s != FJ_OK) return s;
   char* base = (char*)ctx->ws;
   std::vector<fj_block> q0(blocks, blocks + nblocks), l0(blocks, blocks + nblocks);
   size_t off = 0;
   for (int b = 0; b < nblocks; ++b) {
-    q0[b].q = (double*)(base + off);
-    l0[b].q = (double*)(base + sum5 + off);
+    if (!saved) q0[b].q = (double*)(base + off);
+    l0[b].q = (double*)(base + q0_bytes + off);
     off += align256(5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double));
   }
-  double* Q1 = (double*)(base + 2 * sum5);
-  double* Q2 = (double*)(base + 2 * sum5 + max5);
-  double* LA = (double*)(base + 2 * sum5 + 2 * max5);
-  double* LB = (double*)(base + 2 * sum5 + 3 * max5);
-  double* V = (double*)(base + 2 * sum5 + 4 * max5);
-  double* W = (double*)(base + 2 * sum5 + 5 * max5);  // viscous RHS for dJ/dmu0
-  void* wk = base + 2 * sum5 + 6 * max5;
+  char* tail = base + q0_bytes + sum5;
+  double* Q1w = saved ? nullptr : (double*)tail;
+  double* Q2w = saved ? nullptr : (double*)(tail + max5);
+  double* LA = (double*)(tail + nstage * max5);
+  double* LB = (double*)(tail + (nstage + 1) * max5);
+  void* wk = tail + (nstage + 2) * max5;
+  // dJ/dmu0 = sum over stages of c_s dt lam_{s+1} . L_vis(q_s) / mu0 (L_vis is
+  // linear in mu0); the viscous VJP kernel accumulates it with this scale.
   const double inv_mu = p->mu0 != 0.0 ? 1.0 / p->mu0 : 0.0;
-  // c_s dt lam_{s+1} . L_vis(q_s) / mu0
-  auto mu_term = [&](const fj_block& B, const double* qs, const double* lam_next, double coef) -> int {
-    if (!dmu) return FJ_OK;
-    int r = run_rhs(ctx, qs, B.kxyz, B.vol, nullptr, W, B.ni, B.nj, B.nk, p, kRhsViscous, 0, 0.0, wk, st);
-    if (r != FJ_OK) return r;
-    return dot_acc(ctx, lam_next, W, 5 * (int64_t)B.ni * B.nj * B.nk, coef * dt * inv_mu, dmu, st);
-  };
-  // ---- forward recompute of q0' (copy + halo + BC)
-  for (int b = 0; b < nblocks; ++b) {
-    const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
-    s = cuda_status(ctx, cudaMemcpyAsync(q0[b].q, blocks[b].q, bytes, cudaMemcpyDeviceToDevice, st), "copy");
+  if (!saved) {
+    // ---- forward recompute of q0' (copy + halo + BC)
+    for (int b = 0; b < nblocks; ++b) {
+      const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
+      s = cuda_status(ctx, cudaMemcpyAsync(q0[b].q, blocks[b].q, bytes, cudaMemcpyDeviceToDevice, st), "copy");
+      if (s != FJ_OK) return s;
+    }
+    s = halo_exchange(ctx, q0.data(), nblocks, links, nlinks, p->ghost, (double*)wk, work, st);
+    if (s != FJ_OK) return s;
+    s = apply_bc(ctx, q0.data(), nblocks, bcs, nbcs, p, st);
     if (s != FJ_OK) return s;
   }
-  s = halo_exchange(ctx, q0.data(), nblocks, links, nlinks, p->ghost, (double*)wk, work, st);
-  if (s != FJ_OK) return s;
-  s = apply_bc(ctx, q0.data(), nblocks, bcs, nbcs, p, st);
-  if (s != FJ_OK) return s;
-  // ---- per block: recompute q1, q2; reverse the three stages
+  // ---- per block: q1, q2 (recomputed or saved); reverse the three stages
   const int flags = kRhsInvscd | kRhsViscous;
   for (int b = 0; b < nblocks; ++b) {
     const fj_block& B = q0[b];
-    const int64_t n5 = 5 * (int64_t)B.ni * B.nj * B.nk;
     double* L0 = l0[b].q;
-    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, Q1, B.ni, B.nj, B.nk, p, flags, 1, dt, wk, st);
-    if (s == FJ_OK) s = run_rhs(ctx, Q1, B.kxyz, B.vol, B.q, Q2, B.ni, B.nj, B.nk, p, flags, 2, dt, wk, st);
-    // stage 3: q3 = 1/3 q0 + 2/3 (q2 + dt L(q2))
-    if (s == FJ_OK) s = mu_term(B, Q2, lam_in[b], 2.0 / 3.0);
-    if (s == FJ_OK) s = rhs_vjp(ctx, Q2, B.kxyz, B.vol, lam_in[b], V, B.ni, B.nj, B.nk, p, flags, wk, st);
-    if (s == FJ_OK) s = axpy3(ctx, LB, lam_in[b], 2.0 / 3.0, V, 2.0 / 3.0 * dt, nullptr, 0.0, n5, st);
-    if (s == FJ_OK) s = axpy3(ctx, L0, lam_in[b], 1.0 / 3.0, nullptr, 0.0, nullptr, 0.0, n5, st);
-    // stage 2: q2 = 3/4 q0 + 1/4 (q1 + dt L(q1))
-    if (s == FJ_OK) s = mu_term(B, Q1, LB, 0.25);
-    if (s == FJ_OK) s = rhs_vjp(ctx, Q1, B.kxyz, B.vol, LB, V, B.ni, B.nj, B.nk, p, flags, wk, st);
-    if (s == FJ_OK) s = axpy3(ctx, LA, LB, 0.25, V, 0.25 * dt, nullptr, 0.0, n5, st);
-    if (s == FJ_OK) s = axpy3(ctx, L0, L0, 1.0, LB, 0.75, nullptr, 0.0, n5, st);
-    // stage 1: q1 = q0 + dt L(q0)
-    if (s == FJ_OK) s = mu_term(B, B.q, LA, 1.0);
-    if (s == FJ_OK) s = rhs_vjp(ctx, B.q, B.kxyz, B.vol, LA, V, B.ni, B.nj, B.nk, p, flags, wk, st);
-    if (s == FJ_OK) s = axpy3(ctx, L0, L0, 1.0, LA, 1.0, V, dt, n5, st);
+    const double* Q1 = saved ? q1_saved[b] : Q1w;
+    const double* Q2 = saved ? q2_saved[b] : Q2w;
+    if (!saved) {
+      s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, Q1w, B.ni, B.nj, B.nk, p, flags, 1, dt, wk, st);
+      if (s == FJ_OK) s = run_rhs(ctx, Q1w, B.kxyz, B.vol, B.q, Q2w, B.ni, B.nj, B.nk, p, flags, 2, dt, wk, st);
+      if (s != FJ_OK) return s;
+    }
+    // stage 3: q3 = 1/3 q0 + 2/3 (q2 + dt L(q2)):
+    //   LB = 2/3 lam + 2/3 dt V3,  L0 = 1/3 lam
+    VjpEpilogue e3;
+    e3.o1 = LB, e3.x1 = lam_in[b], e3.a1 = 2.0 / 3.0, e3.e1 = 2.0 / 3.0 * dt;
+    e3.o2 = L0, e3.x2 = lam_in[b], e3.a2 = 1.0 / 3.0;
+    s = rhs_vjp(ctx, Q2, B.kxyz, B.vol, lam_in[b], nullptr, B.ni, B.nj, B.nk, p, flags, wk, st, dmu,
+                2.0 / 3.0 * dt * inv_mu, &e3);
+    // stage 2: q2 = 3/4 q0 + 1/4 (q1 + dt L(q1)):
+    //   LA = 1/4 LB + dt/4 V2,  L0 += 3/4 LB
+    VjpEpilogue e2;
+    e2.o1 = LA, e2.x1 = LB, e2.a1 = 0.25, e2.e1 = 0.25 * dt;
+    e2.o2 = L0, e2.x2 = L0, e2.a2 = 1.0, e2.y2 = LB, e2.b2 = 0.75;
+    if (s == FJ_OK)
+      s = rhs_vjp(ctx, Q1, B.kxyz, B.vol, LB, nullptr, B.ni, B.nj, B.nk, p, flags, wk, st, dmu,
+                  0.25 * dt * inv_mu, &e2);
+    // stage 1: q1 = q0 + dt L(q0):  L0 += LA + dt V1
+    VjpEpilogue e1;
+    e1.o1 = L0, e1.x1 = L0, e1.a1 = 1.0, e1.y1 = LA, e1.b1 = 1.0, e1.e1 = dt;
+    if (s == FJ_OK)
+      s = rhs_vjp(ctx, B.q, B.kxyz, B.vol, LA, nullptr, B.ni, B.nj, B.nk, p, flags, wk, st, dmu, dt * inv_mu, &e1);
     if (s != FJ_OK) return s;
   }
   // ---- transposed boundary conditions, then transposed halo fill

@@ -22,6 +22,7 @@ struct fj_ctx {
   int pipeline = FJ_PIPELINE_SPLIT;
   int seg = 0;               // fused kernel: planes per CTA along i (0 = automatic)
   int tile = 0;              // fused kernel: tile shape index (FJ_NUM_TILES shapes)
+  int adj_variant = 0;       // face-VJP register cap (FJ_NUM_ADJ_VARIANTS)
 };
 
 // A prepared step of one block set (fj_plan_create): tables, the metric

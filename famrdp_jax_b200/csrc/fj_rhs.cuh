@@ -40,11 +40,32 @@ int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs,
 size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, int ghost);
 
 // ---- adjoint (fj_adjoint.cu, fj_halo.cu) ----
-// out = (dL/dq)^T lam for one block (L = the RHS parts selected by flags).
+// Elementwise epilogue of an RHS VJP V = (dL/dq)^T lam, applied in the kernel
+// that produces V instead of writing V:
+//   o1 = a1 x1 + b1 y1 + e1 V        (y1 may be NULL)
+//   o2 = a2 x2 + b2 y2               (o2 may be NULL; y2 may be NULL)
+// Every input is read at a cell before any output is written there, so an
+// output may alias an input.
+struct VjpEpilogue {
+  double* o1 = nullptr;
+  const double* x1 = nullptr;
+  double a1 = 0.0;
+  const double* y1 = nullptr;
+  double b1 = 0.0;
+  double e1 = 1.0;
+  double* o2 = nullptr;
+  const double* x2 = nullptr;
+  double a2 = 0.0;
+  const double* y2 = nullptr;
+  double b2 = 0.0;
+};
+// out = (dL/dq)^T lam for one block (L = the RHS parts selected by flags), or
+// with epi the epilogue's outputs instead (out unused); with dmu set, also
+// *dmu += mu_scale * lam . L_vis(q) (device accumulator).
 size_t rhs_vjp_ws_bytes(int precision, int ni, int nj, int nk);
 int rhs_vjp(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol, const double* lam,
             double* out, int ni, int nj, int nk, const fj_params* p, int flags, void* ws,
-            cudaStream_t st);
+            cudaStream_t st, double* dmu = nullptr, double mu_scale = 0.0, const VjpEpilogue* epi = nullptr);
 // *acc (device) += scale * dot(x, y)
 int dot_acc(fj_ctx* ctx, const double* x, const double* y, int64_t n, double scale, double* acc,
             cudaStream_t st);

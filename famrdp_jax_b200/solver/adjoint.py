@@ -76,6 +76,27 @@ def step_vjp(qs, metrics, cfg: Config, dt: float, lams, *, tables: _Tables | Non
     return outs
 
 
+def step_vjp_saved(saved, metrics, cfg: Config, dt: float, lams, *, tables: _Tables | None = None,
+                   dmu: torch.Tensor | None = None):
+    """step_vjp on the states a StepPlan.run_save kept: saved = (q0s, q1s, q2s)
+    with q0s the halo-filled start states; the step's forward is not rerun."""
+    t = tables or _Tables(cfg)
+    q0s, q1s, q2s = saved
+    dev = q0s[0].device
+    c = _capi.ctx(dev)
+    outs = [torch.empty_like(q) for q in q0s]
+    lam_c = [l.contiguous() for l in lams]
+    lam_in = (ctypes.c_void_p * len(q0s))(*[_capi.dev_ptr(l, "lam") for l in lam_c])
+    blocks = _topology.block_array(list(q0s), metrics)
+    pa = _topology.ptr_array
+    st = _capi.lib().fj_step_vjp_saved_f64(c, blocks, pa(q1s), pa(q2s), lam_in, pa(outs), len(q0s), t.link_arr,
+                                           len(t.links), t.bc_arr, len(t.bcs), t.params, float(dt),
+                                           _capi.dev_ptr(dmu, "dmu") if dmu is not None else None,
+                                           _capi.stream(dev))
+    _capi.check(st, "fj_step_vjp_saved_f64", c)
+    return outs
+
+
 def kinetic_energy_grad(qs, metrics, ghost: int = 2):
     """dJ/dq of J = sum over interior cells of vol * 0.5 |rho u|^2 / rho."""
     dev = qs[0].device
@@ -88,15 +109,18 @@ def kinetic_energy_grad(qs, metrics, ghost: int = 2):
 
 
 def _forward_segment(plan: StepPlan, qs, dt, nsteps, keep: bool):
-    """nsteps steps from qs; returns the final state and, if keep, every
-    intermediate input state."""
+    """nsteps steps from qs; returns the final state and, if keep, each step's
+    saved intermediate states (halo-filled start state, stage 1 and 2)."""
     states = []
     cur = list(qs)
     for _ in range(nsteps):
-        if keep:
-            states.append(cur)
         nxt = [torch.empty_like(q) for q in cur]
-        plan.run(cur, nxt, dt)
+        if keep:
+            saved = tuple([torch.empty_like(q) for q in cur] for _ in range(3))
+            plan.run_save(cur, nxt, *saved, dt)
+            states.append(saved)
+        else:
+            plan.run(cur, nxt, dt)
         cur = nxt
     return cur, states
 
@@ -114,14 +138,15 @@ class _Run:
 
 
 def _reverse_sweep(run: _Run, checkpoints, lams):
-    """Segments in reverse: recompute the segment's states from its checkpoint,
-    then apply the step adjoints backwards."""
+    """Segments in reverse: recompute the segment's states from its checkpoint
+    (keeping each step's stage states), then apply the step adjoints
+    backwards, releasing each step's states once its adjoint has run."""
     nseg = len(checkpoints)
     for s in reversed(range(nseg)):
         seg_len = min(run.every, run.nsteps - s * run.every)
         _, states = _forward_segment(run.plan, checkpoints[s], run.dt, seg_len, keep=True)
-        for qs in reversed(states):
-            lams = step_vjp(qs, run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu)
+        while states:
+            lams = step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu)
     return lams
 
 

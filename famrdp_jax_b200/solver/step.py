@@ -82,6 +82,17 @@ class StepPlan:
         _capi.check(self._lib.fj_plan_step(self._handle, _topology.ptr_array(qs), _topology.ptr_array(outs),
                                            float(dt), _capi.stream(self.device)), "fj_plan_step", c)
 
+    def run_save(self, qs, outs, q0s, q1s, q2s, dt: float) -> None:
+        """One step that also keeps its intermediate states (the halo-filled
+        start state and the first two stage values) for the step adjoint."""
+        for lst in (qs, outs, q0s, q1s, q2s):
+            if [tuple(q.shape) for q in lst] != self.shapes:
+                raise ValueError("state shapes differ from the plan's")
+        c = _capi.ctx(self.device)
+        pa = _topology.ptr_array
+        _capi.check(self._lib.fj_plan_step_save(self._handle, pa(qs), pa(outs), pa(q0s), pa(q1s), pa(q2s), float(dt),
+                                                _capi.stream(self.device)), "fj_plan_step_save", c)
+
     def stage(self, qs, q0s, outs, dt: float, stage: int) -> None:
         """One TVD-RK3 stage of every block (no halo fill)."""
         c = _capi.ctx(self.device)

@@ -118,6 +118,12 @@ const char* fj_last_error(const fj_ctx* ctx);
  * 8x64, 16x16 (the last three FP32-flux only; FP64 maps them to 8x32/8x16). */
 #define FJ_NUM_TILES 7
 int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg, int tile);
+/* Launch shape of the face kernel of the RHS adjoint (a tuning knob; results
+ * agree to the rounding of atomic accumulation order): 0 = register-capped
+ * for occupancy (default), 1 = uncapped, 2 = the other cap.  The reference
+ * has no counterpart. */
+#define FJ_NUM_ADJ_VARIANTS 3
+int fj_ctx_set_adjoint_variant(fj_ctx* ctx, int variant);
 /* Number of kernels launched through this context so far (instrumentation;
  * the reference has no counterpart). */
 int fj_launch_count(const fj_ctx* ctx, int64_t* out);
@@ -213,6 +219,13 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
  * q_in[b] (in-place step), but must not partially overlap any state. */
 int fj_plan_step(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,
                  void* stream);
+/* As fj_plan_step, and also keeps the step's intermediate states for a later
+ * fj_step_vjp_saved_f64: q0_save[b] = q_in[b] after the halo fill and the
+ * boundary conditions, q1_save[b] and q2_save[b] = the first two stage values.
+ * The three saves are distinct (5, ni, nj, nk) arrays that overlap no state. */
+int fj_plan_step_save(fj_plan* plan, double* const* q_in, double* const* q_out,
+                      double* const* q0_save, double* const* q1_save, double* const* q2_save,
+                      double dt, void* stream);
 int fj_plan_destroy(fj_plan* plan);
 /* One TVD-RK3 stage (1..3) of every block of the plan, without the halo fill
  * (solver/step.py:45-53): out[b] from q[b] (stage input) and q0[b] (step start
@@ -245,6 +258,14 @@ int fj_step_vjp_mu_f64(fj_ctx* ctx, const fj_block* blocks, const double* const*
                        double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
                        const fj_bc* bcs, int nbcs, const fj_params* p, double dt, double* dJ_dmu0,
                        void* stream);
+/* fj_step_vjp_f64 / fj_step_vjp_mu_f64 on states kept by fj_plan_step_save:
+ * blocks[b].q = q0_save[b], and q1[b], q2[b] = q1_save[b], q2_save[b], so the
+ * step's forward is not recomputed.  dJ_dmu0 may be NULL. */
+int fj_step_vjp_saved_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* q1,
+                          const double* const* q2, const double* const* lam_in,
+                          double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
+                          const fj_bc* bcs, int nbcs, const fj_params* p, double dt,
+                          double* dJ_dmu0, void* stream);
 /* grad[b] = dJ/dq[b] for J = sum over interior cells of vol * 0.5 |rho u|^2 / rho
  * (the objective of fj_kinetic_energy_f64); ghost cells get 0. */
 int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* const* grad,

@@ -172,3 +172,59 @@ def test_reference_gradient_is_finite_and_nonzero(cuda_device):
     g = adjoint.step_vjp([dev(q)], metrics, cfg, 1e-6, [torch.ones((5, ni, nj, nk), dtype=torch.float64,
                                                                     device="cuda")])[0]
     assert torch.all(torch.isfinite(g)) and torch.any(g != 0)
+
+
+@pytest.mark.parametrize("which", ["periodic", "mirror"])
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_saved_step_vjp_matches_recomputing_vjp(cuda_device, which, precision):
+    """fj_plan_step_save + fj_step_vjp_saved_f64 against fj_plan_step and the
+    recomputing fj_step_vjp_mu_f64: same new state, same adjoint, same dJ/dmu0."""
+    import dataclasses
+    qs, mets, cfg = _periodic_case() if which == "periodic" else _mirror_case()
+    cfg = dataclasses.replace(cfg, precision=precision)
+    dt = 0.5 * NP.cfl_dt(qs, mets, cfg.gas.gamma, 0.5, 2)
+    metrics = tuple(Metrics(jac=dev(v), kxyz=dev(k), vol=dev(v)) for k, v in mets)
+    st = State(blocks=tuple(Block(q=dev(q), xyz=None) for q in qs), metrics=metrics)
+    plan = StepPlan(st, cfg)
+    qd = [b.q for b in st.blocks]
+    ref_out = [torch.empty_like(q) for q in qd]
+    plan.run(qd, ref_out, dt)
+    out = [torch.empty_like(q) for q in qd]
+    saved = tuple([torch.empty_like(q) for q in qd] for _ in range(3))
+    plan.run_save(qd, out, *saved, dt)
+    for a, b in zip(out, ref_out):
+        assert torch.equal(a, b)
+    lam = [dev(np.random.default_rng(3).standard_normal(q.shape)) for q in qs]
+    dmu_a = torch.zeros(1, dtype=torch.float64, device="cuda")
+    dmu_b = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ga = adjoint.step_vjp(qd, metrics, cfg, dt, lam, dmu=dmu_a)
+    gb = adjoint.step_vjp_saved(saved, metrics, cfg, dt, lam, dmu=dmu_b)
+    # the face adjoints are accumulated with atomics, whose order varies from
+    # run to run: FP64 rounding in the FP64 path, FP32 rounding in the FP32 one
+    tol = 1e-13 if precision == "f64" else 1e-6
+    for a, b in zip(ga, gb):
+        assert rel_l2(host(b), host(a)) <= tol
+    assert abs(float(dmu_a) - float(dmu_b)) <= tol * abs(float(dmu_a))
+
+
+def test_mu_gradient_matches_autograd(cuda_device):
+    """dJ/dmu0 of one step (J = lam . q_new) against torch.autograd of the
+    oracle's twin with mu0 as a leaf."""
+    import dataclasses
+    qs, mets, cfg = _periodic_case()
+    dt = 0.5 * NP.cfl_dt(qs, mets, cfg.gas.gamma, 0.5, 2)
+    lam = [np.random.default_rng(5).standard_normal(q.shape) for q in qs]
+    h = 1e-2 * cfg.gas.mu0
+
+    def J(mu):
+        c2 = dataclasses.replace(cfg, gas=dataclasses.replace(cfg.gas, mu0=mu))
+        out = TORCH.step([torch.tensor(q) for q in qs], [(torch.tensor(k), torch.tensor(v)) for k, v in mets], c2, dt)
+        return sum(float(torch.sum(o * torch.tensor(l))) for o, l in zip(out, lam))
+    # J is nearly linear in mu0 (exactly linear within one stage): central
+    # differences of the FP64 oracle agree to ~1e-8 between h = 1e-2 mu0 and
+    # 1e-3 mu0; the larger h keeps the cancellation error smallest
+    ref = (J(cfg.gas.mu0 + h) - J(cfg.gas.mu0 - h)) / (2 * h)
+    metrics = tuple(Metrics(jac=dev(v), kxyz=dev(k), vol=dev(v)) for k, v in mets)
+    dmu = torch.zeros(1, dtype=torch.float64, device="cuda")
+    adjoint.step_vjp([dev(q) for q in qs], metrics, cfg, dt, [dev(l) for l in lam], dmu=dmu)
+    assert abs(float(dmu) - ref) <= 1e-7 * abs(ref), (float(dmu), ref)
