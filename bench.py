@@ -40,6 +40,7 @@ import json
 import os
 import statistics
 import subprocess
+import threading
 import sys
 import time
 
@@ -74,7 +75,10 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms around the
+    timed region: entering waits for the first sample (so sampling is live
+    when timing starts), leaving waits for one more sample taken after the
+    region, then stops the sampler."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -82,25 +86,47 @@ class ClockSampler:
 
     def __init__(self, gpu_index: int):
         self.gpu, self.proc, self.lines = gpu_index, None, []
+        self._cv = threading.Condition()
+        self._reader = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                with self._cv:
+                    self.lines.append(line.strip())
+                    self._cv.notify_all()
+
+    def _wait_for(self, n, timeout):
+        with self._cv:
+            self._cv.wait_for(lambda: len(self.lines) >= n, timeout=timeout)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return self
+        self._reader = threading.Thread(target=self._read, daemon=True)
+        self._reader.start()
+        self._wait_for(1, 10.0)
         return self
 
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except Exception:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+        if self.proc is None:
+            return
+        with self._cv:
+            n = len(self.lines)
+        self._wait_for(n + 1, 2.0)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+            self.proc.wait()
+        if self._reader is not None:
+            self._reader.join(timeout=5)
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -139,17 +165,22 @@ def build_case(args, metrics_fn=None):
         return cases.tgv(n=32)
     if args.workload == "tree24":
         return cases.tree24(seed=args.seed)
+    if args.workload == "ensemble64":
+        return cases.ensemble(ninst=64, n=64, seed=args.seed)
     raise SystemExit(f"unknown workload {args.workload}")
 
 
 def workload_desc(case, args):
     desc = {"wavy4": f"{args.n}^3 cells each, 2x2 in i-j, periodic, curvilinear, M 0.5, Re 1e4, 1% noise",
             "tgv32": "32^3 Taylor-Green vortex, M0 0.1, Re 1600, constant viscosity, self-periodic",
-            "tree24": "uneven blocks U[16,160]^3 on a random spanning tree, farfield/periodic faces, M 0.8, Re 5e4"}
+            "tree24": "uneven blocks U[16,160]^3 on a random spanning tree, farfield/periodic faces, M 0.8, Re 5e4",
+            "ensemble64": "64 independent self-periodic 64^3 Taylor-Green instances, M U[0.1,0.9], Re log-U[1e2,1e4], "
+                          "0.5% noise, per-instance mu0 and dt, all instances per launch"}
     return {"workload": f"{case.name}: {len(case.qs)} blocks, {desc[args.workload]}",
             "blocks": len(case.qs), "cells_interior": case.interior_cells, "cells_padded": case.padded_cells,
             "precision": args.precision, "ghost": case.cfg.ghost, "seed": args.seed,
-            "l2": "inputs larger than L2 (state + metrics per step >> 126 MB)"}
+            "l2": "inputs larger than L2 (state + metrics per step >> 126 MB)",
+            "cuda_graph": "each timed step is one replay of a captured step graph (halo, BCs, 3 stages)"}
 
 
 def cpu_oracle_sample(case, dt):
@@ -231,6 +262,7 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"))
     out = {"workload": f"tgv{n}: {n}^3 cells, M0 0.3, Re 800, 1% noise, J = kinetic energy after {nsteps} steps, "
                        f"checkpoint every {every} steps"}
     c = cases.tgv(n=n, M0=0.3, Re=800.0, noise=0.01, seed=0)
+    dq_dM0 = cases.tgv_dq0_dM0(c)
     grads = {}
     stream = torch.cuda.current_stream(device)
 
@@ -263,15 +295,19 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"))
         adjoint.adjoint_kinetic_energy(st, cfg, dt, 2, checkpoint_every=1, plan=plan)  # warm-up
         run = adjoint._Run(cfg=cfg, metrics=st.metrics, dt=float(dt), nsteps=nsteps, every=every, plan=plan,
                            tables=adjoint._Tables(cfg), dmu=torch.zeros(1, dtype=torch.float64, device=device))
+        run.buffers([st.blocks[0].q])  # the driver's reusable buffers, outside the timed region
         (final, checkpoints), t_ckpt = timed(lambda: adjoint._forward_with_checkpoints(run, [st.blocks[0].q]))
         lams = adjoint.kinetic_energy_grad(final, st.metrics, cfg.ghost)
         g, t_rev = timed(lambda: adjoint._reverse_sweep(run, checkpoints, lams))
         fstate = dc.replace(st, blocks=(dc.replace(st.blocks[0], q=final[0]),))
         J = diagnostics.kinetic_energy(fstate, cfg.ghost)
         grads[prec] = g[0]
+        dmu = float(run.dmu.item())
+        # M0 enters the initial state and mu0 = rho0 M0 / Re (dt held fixed)
+        dJ_dM0 = float(torch.sum(g[0] * torch.as_tensor(dq_dM0, device=device))) + dmu * 1.0 / c.meta["Re"]
         out[prec] = {"forward_ms_per_step": t_fwd / nsteps, "checkpointed_forward_ms_per_step": t_ckpt / nsteps,
                      "reverse_sweep_ms_per_step": t_rev / nsteps, "adjoint_over_forward": t_rev / t_fwd,
-                     "J": J, "dJ_dmu0": float(run.dmu.item())}
+                     "J": J, "dJ_dmu0": dmu, "dJ_dM0": dJ_dM0}
     if len(grads) == 2:
         out["f32_vs_f64_grad_rel_l2"] = float(torch.linalg.vector_norm(grads["f32"] - grads["f64"]) /
                                               torch.linalg.vector_norm(grads["f64"]))
@@ -314,6 +350,10 @@ def run_ours(args):
     cells = case.interior_cells
     st0 = cases.to_state(case, device)
     dt = diagnostics.cfl_dt(st0, case.cfg, case.cfl)
+    ens = None
+    if "mu0" in case.meta and isinstance(case.meta["mu0"], list):  # independent instances
+        ens = (case.meta["mu0"], [diagnostics.cfl_dt(State(blocks=(b,), metrics=(m,)), case.cfg, case.cfl)
+                                  for b, m in zip(st0.blocks, st0.metrics)])
 
     def barrier():
         if ws > 1:
@@ -326,11 +366,13 @@ def run_ours(args):
         cfg = dataclasses.replace(case.cfg, precision=prec)
         state = cases.to_state(case, device)
         plan = StepPlan(state, cfg)
+        if ens:
+            plan.set_ensemble(*ens)
         plans[prec] = (plan, cfg, state)
         qa = [b.q for b in state.blocks]
         qb = [torch.empty_like(q) for q in qa]
-        for _ in range(warm):
-            plan.run(qa, qb, dt)
+        for _ in range(warm):  # also captures the two ping-pong step graphs
+            plan.run(qa, qb, dt, graph=True)
             qa, qb = qb, qa
         torch.cuda.synchronize()
         barrier()
@@ -341,7 +383,7 @@ def run_ours(args):
         with ClockSampler(_gpu_index(local)) as clk:
             e0.record(s)
             for _ in range(args.steps):
-                plan.run(qa, qb, dt)
+                plan.run(qa, qb, dt, graph=True)
                 qa, qb = qb, qa
             e1.record(s)
             torch.cuda.synchronize()
@@ -426,7 +468,8 @@ def run_ours(args):
                 "variants": {p: results[p] for p in order} | {
                     "f32_vs_f64_rel_l2": err_f32,
                     "f32_vs_f64_note": f"whole state after {warm + args.steps} steps from the same start"},
-                "adjoint": adj, "dt": dt}
+                "adjoint": adj,
+                "dt": dt if not ens else {"per_instance": True, "min": min(ens[1]), "max": max(ens[1])}}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()
@@ -440,7 +483,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["wavy4", "tgv32", "tree24"], default="wavy4")
+    ap.add_argument("--workload", choices=["wavy4", "tgv32", "tree24", "ensemble64"], default="wavy4")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--seed", type=int, default=0)

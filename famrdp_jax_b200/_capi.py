@@ -74,6 +74,8 @@ SIGNATURES = {
     "fj_plan_create": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjLink), _I, ctypes.POINTER(FjBc), _I,
                             ctypes.POINTER(FjParams), ctypes.POINTER(_P)]),
     "fj_plan_step": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
+    "fj_plan_set_ensemble": (_I, [_P, _P, _P]),
+    "fj_plan_step_graph": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_step_save": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
                                ctypes.POINTER(_P), _D, _P]),
     "fj_plan_destroy": (_I, [_P]),
@@ -87,6 +89,9 @@ SIGNATURES = {
     "fj_step_vjp_saved_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), ctypes.POINTER(_P),
                                    ctypes.POINTER(_P), ctypes.POINTER(_P), _I, ctypes.POINTER(FjLink), _I,
                                    ctypes.POINTER(FjBc), _I, ctypes.POINTER(FjParams), _D, _P, _P]),
+    "fj_step_vjp_ensemble_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                                      ctypes.POINTER(_P), ctypes.POINTER(_P), _I, ctypes.POINTER(FjLink), _I,
+                                      ctypes.POINTER(FjBc), _I, ctypes.POINTER(FjParams), _D, _P, _P, _P, _P]),
     "fj_kinetic_energy_grad_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), _I, _I, _P]),
     "fj_rk_stage_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _D, _I, _P]),
     "fj_cons_to_prim_f64": (_I, [_P, _P, _I64, _D, _P]),

@@ -130,6 +130,64 @@ def tgv(n=32, M0=0.1, Re=1600.0, gamma=1.4, Pr=0.72, visc_law="constant", noise=
                 steps=steps, meta={"n": n, "M0": M0, "Re": Re, "h": h})
 
 
+def tgv_dq0_dM0(case: Case) -> np.ndarray:
+    """d q0 / d M0 of a ``tgv`` case at its Mach number (same seed, so the
+    noise draws are held fixed): u, v, w scale with M0, and rho and p carry
+    M0^2 b with b = (rho0/16)(cos 2x + cos 2y)(cos 2z + 2), each times its own
+    noise factor.  The case's viscosity mu0 = rho0 M0 / Re also depends on M0;
+    that part is d mu0 / d M0 = rho0 / Re (see ``case.meta``)."""
+    n, M0, h = case.meta["n"], case.meta["M0"], case.meta["h"]
+    gamma = case.cfg.gas.gamma
+    g = case.cfg.ghost
+    x = (np.arange(n + 2 * g) - g + 0.5) * h
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    rho0, p0 = 1.0, 1.0 / gamma
+    b = (rho0 / 16.0) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+    q = case.qs[0]
+    rho = q[0]
+    u, v, w = q[1] / rho, q[2] / rho, q[3] / rho
+    p = (gamma - 1.0) * (q[4] - 0.5 * rho * (u * u + v * v + w * w))
+    clean = p0 + M0 ** 2 * b  # p (and rho T0) before the noise factors
+    drho = 2.0 * M0 * b * rho / clean
+    dp = 2.0 * M0 * b * p / clean
+    du, dv, dw = u / M0, v / M0, w / M0
+    out = np.empty_like(q)
+    out[0] = drho
+    out[1] = drho * u + rho * du
+    out[2] = drho * v + rho * dv
+    out[3] = drho * w + rho * dw
+    out[4] = dp / (gamma - 1.0) + 0.5 * drho * (u * u + v * v + w * w) + rho * (u * du + v * dv + w * dw)
+    return out
+
+
+def ensemble(ninst=64, n=64, M_range=(0.1, 0.9), Re_range=(1e2, 1e4), noise=0.005, seed=0, gamma=1.4, Pr=0.72,
+             visc_law="constant", limiter="minmod", cfl=0.5, steps=100, precision="f32") -> Case:
+    """Independent self-periodic Taylor-Green instances of n^3 cells: Mach
+    uniform in M_range and Re log-uniform in Re_range from ``seed``, each
+    with its own noise seed.  Per-instance mu0 = rho0 M / Re is in
+    ``meta["mu0"]``; the case's gas model carries instance 0's.  Time steps
+    are per instance (``meta`` has no dt: compute it from each instance's
+    initial state)."""
+    rng = np.random.default_rng(seed)
+    Ms = rng.uniform(M_range[0], M_range[1], ninst)
+    Res = np.exp(rng.uniform(np.log(Re_range[0]), np.log(Re_range[1]), ninst))
+    qs, metrics, topos, mu0 = [], [], [], []
+    for b in range(ninst):
+        c = tgv(n=n, M0=float(Ms[b]), Re=float(Res[b]), gamma=gamma, Pr=Pr, visc_law=visc_law, noise=noise,
+                seed=seed * 1000 + b + 1, limiter=limiter, cfl=cfl, precision=precision)
+        qs.append(c.qs[0])
+        metrics.append(c.metrics[0])
+        topos.append(_self_periodic_topology(b))
+        mu0.append(c.cfg.gas.mu0)
+    gas = GasModel(gamma=gamma, R=1.0, mu0=mu0[0], T0=1.0 / gamma, Ts=(1.0 / gamma) * 110.4 / 288.15, Pr_lam=Pr,
+                   visc_law=visc_law)
+    cfg = Config(gas=gas, scheme=_scheme(limiter), bc_params={}, topology=tuple(topos), ghost=GHOST,
+                 nan_check=False, cfl=cfl, precision=precision)
+    return Case(name=f"ensemble{ninst}x{n}", qs=qs, metrics=metrics, cfg=cfg, cfl=cfl, steps=steps,
+                meta={"n": n, "M0": [float(m) for m in Ms], "Re": [float(r) for r in Res], "mu0": mu0,
+                      "h": 2.0 * math.pi / n})
+
+
 def _noisy_freestream(shape, M, gamma, rng, noise):
     rho = np.ones(shape) * (1 + noise * rng.standard_normal(shape))
     p = np.full(shape, 1.0 / gamma) * (1 + noise * rng.standard_normal(shape))

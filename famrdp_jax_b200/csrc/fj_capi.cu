@@ -51,13 +51,15 @@ size_t rhs_scratch_bytes(const fj_ctx* ctx, int precision, int ni, int nj, int n
 }
 
 SplitBlock split_block(const double* q, const double* q0, double* out, const double* kxyz,
-                       const float* kxyz32, const double* vol, int ni, int nj, int nk) {
+                       const void* kaos, const double* vol, int ni, int nj, int nk, double mu0, double dt) {
   SplitBlock b{};
+  b.mu0 = mu0;
+  b.dt = dt;
   b.q = q;
   b.q0 = q0;
   b.out = out;
   b.kxyz = kxyz;
-  b.kxyz32 = kxyz32;
+  b.kaos = kaos;
   b.vol = vol;
   b.ni = ni;
   b.nj = nj;
@@ -67,20 +69,22 @@ SplitBlock split_block(const double* q, const double* q0, double* out, const dou
 
 int run_rhs(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
             const double* q0, double* out, int ni, int nj, int nk, const fj_params* p, int flags,
-            int stage, double dt, void* ws, cudaStream_t st, const float* kxyz32 = nullptr) {
+            int stage, double dt, void* ws, cudaStream_t st, const void* kmet = nullptr) {
+  // kmet: a plan's metric copy for this block and pipeline (split: records
+  // in the flux type; fused, FP32-flux: field-major FP32), or nullptr
   Phys ph = make_phys(p);
   if (ctx->pipeline == FJ_PIPELINE_SPLIT) {
-    SplitBlock b = split_block(q, q0, out, kxyz, p->precision == FJ_PREC_F32FLUX ? kxyz32 : nullptr,
-                               vol, ni, nj, nk);
+    SplitBlock b = split_block(q, q0, out, kxyz, kmet,
+                               vol, ni, nj, nk, p->mu0, dt);
     split_assign_scratch(p->precision, &b, 1, ws);
-    return split_stage(ctx, &b, 1, ph, flags, stage, dt, p->precision, st);
+    return split_stage(ctx, &b, 1, ph, flags, stage, p->precision, st);
   }
   if (ctx->pipeline == FJ_PIPELINE_FUSED) {
     StageArgs a{};
     a.q = q;
     a.q0 = q0;
     a.kxyz = kxyz;
-    a.kxyz32 = p->precision == FJ_PREC_F32FLUX ? kxyz32 : nullptr;
+    a.kxyz32 = p->precision == FJ_PREC_F32FLUX ? (const float*)kmet : nullptr;
     a.vol = vol;
     a.out = out;
     a.ni = ni;
@@ -169,10 +173,12 @@ size_t step_layout(const fj_ctx* ctx, const fj_block* blocks, int nblocks, const
 // fill and the end of the step, solver/step.py:40-53): q1s := stage 1 of q0p,
 // q2s := stage 2, q_out := stage 3.  q0p may equal q_out (the stage-3 kernels
 // read q0 only at the cell they write).
+// mu0_b / dt_b (nullable): per-block viscosity scale and time step that
+// replace p->mu0 and dt (independent instances of an ensemble).
 int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* const* q1s,
               double* const* q2s, double* const* q_out, int nblocks, const fj_link* links, int nlinks,
-              const fj_bc* bcs, int nbcs, const fj_params* p, double dt, float* const* kxyz32, void* tail,
-              size_t tail_b, cudaStream_t st) {
+              const fj_bc* bcs, int nbcs, const fj_params* p, double dt, void* const* kmet, void* tail,
+              size_t tail_b, cudaStream_t st, const double* mu0_b = nullptr, const double* dt_b = nullptr) {
   std::vector<fj_block> out(blocks, blocks + nblocks);
   int s;
   for (int b = 0; b < nblocks; ++b) {
@@ -195,33 +201,37 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
     for (int b = 0; b < nblocks; ++b) {
       const fj_block& B = out[b];
       sb[b] = split_block(B.q, B.q, q1s[b], B.kxyz,
-                          (p->precision == FJ_PREC_F32FLUX && kxyz32) ? kxyz32[b] : nullptr, B.vol, B.ni,
-                          B.nj, B.nk);
+                          kmet ? kmet[b] : nullptr, B.vol, B.ni,
+                          B.nj, B.nk, mu0_b ? mu0_b[b] : p->mu0, dt_b ? dt_b[b] : dt);
     }
     split_assign_scratch(p->precision, sb.data(), nblocks, tail);
     const Phys ph = make_phys(p);
-    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 1, dt, p->precision, st);
+    // the assembly of stages 1 and 2 also writes the next stage's primitives
+    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 1, p->precision, st, false, true);
     if (s != FJ_OK) return s;
     for (int b = 0; b < nblocks; ++b) {
       sb[b].q = q1s[b];
       sb[b].out = q2s[b];
     }
-    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 2, dt, p->precision, st);
+    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 2, p->precision, st, true, true);
     if (s != FJ_OK) return s;
     for (int b = 0; b < nblocks; ++b) {
       sb[b].q = q2s[b];
       sb[b].out = q_out[b];
     }
-    return split_stage(ctx, sb.data(), nblocks, ph, flags, 3, dt, p->precision, st);
+    return split_stage(ctx, sb.data(), nblocks, ph, flags, 3, p->precision, st, true, false);
   }
   for (int b = 0; b < nblocks; ++b) {
     const fj_block& B = out[b];
-    const float* k32 = kxyz32 ? kxyz32[b] : nullptr;
-    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, q1s[b], B.ni, B.nj, B.nk, p, flags, 1, dt, tail, st, k32);
+    const void* k32 = kmet ? kmet[b] : nullptr;
+    fj_params pb = *p;
+    if (mu0_b) pb.mu0 = mu0_b[b];
+    const double dtb = dt_b ? dt_b[b] : dt;
+    s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, q1s[b], B.ni, B.nj, B.nk, &pb, flags, 1, dtb, tail, st, k32);
     if (s != FJ_OK) return s;
-    s = run_rhs(ctx, q1s[b], B.kxyz, B.vol, B.q, q2s[b], B.ni, B.nj, B.nk, p, flags, 2, dt, tail, st, k32);
+    s = run_rhs(ctx, q1s[b], B.kxyz, B.vol, B.q, q2s[b], B.ni, B.nj, B.nk, &pb, flags, 2, dtb, tail, st, k32);
     if (s != FJ_OK) return s;
-    s = run_rhs(ctx, q2s[b], B.kxyz, B.vol, B.q, q_out[b], B.ni, B.nj, B.nk, p, flags, 3, dt, tail, st, k32);
+    s = run_rhs(ctx, q2s[b], B.kxyz, B.vol, B.q, q_out[b], B.ni, B.nj, B.nk, &pb, flags, 3, dtb, tail, st, k32);
     if (s != FJ_OK) return s;
   }
   return FJ_OK;
@@ -451,20 +461,27 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
     delete pl;
     return set_err(ctx, FJ_ERR_NO_MEMORY, "plan scratch allocation failed");
   }
-  if (p->precision == FJ_PREC_F32FLUX) {
-    pl->kxyz32.assign(nblocks, nullptr);
+  // metric copies for the FP32-flux path: per-cell FP32 records for the split
+  // pipeline, field-major FP32 for the fused kernel (the FP64 kernels read
+  // the caller's kxyz)
+  const bool split = pl->pipeline == FJ_PIPELINE_SPLIT;
+  if (p->precision == FJ_PREC_F32FLUX &&
+      (pl->pipeline == FJ_PIPELINE_SPLIT || pl->pipeline == FJ_PIPELINE_FUSED)) {
+    pl->kmet.assign(nblocks, nullptr);
     for (int b = 0; b < nblocks; ++b) {
-      const size_t n9 = 9 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
-      e = cudaMalloc(&pl->kxyz32[b], n9 * sizeof(float));
+      const int64_t N = (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
+      const size_t bytes = split ? split_metric_record_bytes(p->precision, N) : 9 * (size_t)N * sizeof(float);
+      e = cudaMalloc(&pl->kmet[b], bytes);
       if (e != cudaSuccess) {
         cudaGetLastError();
         fj_plan_destroy(pl);
-        return set_err(ctx, FJ_ERR_NO_MEMORY, "plan FP32 metric allocation failed");
+        return set_err(ctx, FJ_ERR_NO_MEMORY, "plan metric copy allocation failed");
       }
-      s = convert_f64_f32(blocks[b].kxyz, pl->kxyz32[b], (int64_t)n9, nullptr);
+      s = split ? split_metric_records(blocks[b].kxyz, pl->kmet[b], N, p->precision, nullptr)
+                : convert_f64_f32(blocks[b].kxyz, (float*)pl->kmet[b], 9 * N, nullptr);
       if (s != FJ_OK) {
         fj_plan_destroy(pl);
-        return set_err(ctx, s, "plan FP32 metric conversion failed");
+        return set_err(ctx, s, "plan metric conversion failed");
       }
     }
     e = cudaStreamSynchronize(nullptr);
@@ -500,13 +517,86 @@ static int plan_step_impl(fj_plan* pl, double* const* q_in, double* const* q_out
   void* tail = (char*)pl->scratch + 2 * pl->stage_bytes;
   int s = step_body(ctx, in.data(), q0_save ? q0_save : q_out, q1s.data(), q2s.data(), q_out, nb,
                     pl->links.data(), (int)pl->links.size(), pl->bcs.data(), (int)pl->bcs.size(), &pl->p, dt,
-                    pl->kxyz32.empty() ? nullptr : pl->kxyz32.data(), tail, pl->halo_bytes, S(stream));
+                    pl->kmet.empty() ? nullptr : pl->kmet.data(), tail, pl->halo_bytes, S(stream),
+                    pl->mu0_b.empty() ? nullptr : pl->mu0_b.data(), pl->dt_b.empty() ? nullptr : pl->dt_b.data());
   ctx->pipeline = saved;
   return s;
 }
 
 int fj_plan_step(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, void* stream) {
   return plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);
+}
+
+int fj_plan_set_ensemble(fj_plan* pl, const double* mu0, const double* dt) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  const size_t nb = pl->blocks.size();
+  if (mu0)
+    for (size_t b = 0; b < nb; ++b)
+      if (!(mu0[b] >= 0.0)) return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "mu0 must be >= 0");
+  if (dt)
+    for (size_t b = 0; b < nb; ++b)
+      if (!(dt[b] >= 0.0) || dt[b] == INFINITY) return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "bad dt");
+  pl->mu0_b.clear();
+  pl->dt_b.clear();
+  if (mu0) pl->mu0_b.assign(mu0, mu0 + nb);
+  if (dt) pl->dt_b.assign(dt, dt + nb);
+  for (fj_graph_entry& g : pl->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  pl->graphs.clear();
+  return FJ_OK;
+}
+
+int fj_plan_step_graph(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, void* stream) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  fj_ctx* ctx = pl->ctx;
+  const int nb = (int)pl->blocks.size();
+  if (!q_in || !q_out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "q_in/q_out is NULL");
+  std::vector<double*> in(q_in, q_in + nb), out(q_out, q_out + nb);
+  for (int b = 0; b < nb; ++b)
+    if (!in[b] || !out[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "state pointer is NULL");
+  size_t hit = pl->graphs.size();
+  for (size_t g = 0; g < pl->graphs.size(); ++g)
+    if (pl->graphs[g].q_in == in && pl->graphs[g].q_out == out && pl->graphs[g].dt == dt) hit = g;
+  if (hit == pl->graphs.size()) {
+    if (!pl->capture_stream) {
+      int s = cuda_status(ctx, cudaStreamCreateWithFlags(&pl->capture_stream, cudaStreamNonBlocking),
+                          "capture stream");
+      if (s != FJ_OK) return s;
+    }
+    int s = cuda_status(ctx, cudaStreamBeginCapture(pl->capture_stream, cudaStreamCaptureModeThreadLocal),
+                        "begin capture");
+    if (s != FJ_OK) return s;
+    const int64_t before = ctx->launches;
+    s = plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, pl->capture_stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(pl->capture_stream, &graph);
+    const int64_t nlaunch = ctx->launches - before;
+    ctx->launches = before;  // nothing has run yet
+    if (s == FJ_OK) s = cuda_status(ctx, e, "end capture");
+    fj_graph_entry ent;
+    if (s == FJ_OK) s = cuda_status(ctx, cudaGraphInstantiate(&ent.exec, graph, 0), "graph instantiate");
+    if (graph) cudaGraphDestroy(graph);
+    if (s != FJ_OK) {
+      cudaGetLastError();
+      return s;
+    }
+    ent.q_in = in;
+    ent.q_out = out;
+    ent.dt = dt;
+    ent.launches = nlaunch;
+    if ((int)pl->graphs.size() >= FJ_PLAN_MAX_GRAPHS) {
+      cudaGraphExecDestroy(pl->graphs.front().exec);
+      pl->graphs.erase(pl->graphs.begin());
+    }
+    pl->graphs.push_back(ent);
+    hit = pl->graphs.size() - 1;
+  } else if (hit + 1 != pl->graphs.size()) {
+    std::rotate(pl->graphs.begin() + hit, pl->graphs.begin() + hit + 1, pl->graphs.end());
+    hit = pl->graphs.size() - 1;
+  }
+  int s = cuda_status(ctx, cudaGraphLaunch(pl->graphs[hit].exec, S(stream)), "graph launch");
+  if (s == FJ_OK) ctx->launches += pl->graphs[hit].launches;
+  return s;
 }
 
 int fj_plan_step_save(fj_plan* pl, double* const* q_in, double* const* q_out, double* const* q0_save,
@@ -539,15 +629,19 @@ int fj_plan_stage(fj_plan* pl, double* const* q, double* const* q0, double* cons
     for (int b = 0; b < nb; ++b) {
       const fj_block& B = pl->blocks[b];
       sb[b] = split_block(q[b], stage > 1 ? q0[b] : q[b], out[b], B.kxyz,
-                          pl->kxyz32.empty() ? nullptr : pl->kxyz32[b], B.vol, B.ni, B.nj, B.nk);
+                          pl->kmet.empty() ? nullptr : pl->kmet[b], B.vol, B.ni, B.nj, B.nk,
+                          pl->mu0_b.empty() ? pl->p.mu0 : pl->mu0_b[b], pl->dt_b.empty() ? dt : pl->dt_b[b]);
     }
     split_assign_scratch(pl->p.precision, sb.data(), nb, tail);
-    s = split_stage(ctx, sb.data(), nb, make_phys(&pl->p), flags, stage, dt, pl->p.precision, S(stream));
+    s = split_stage(ctx, sb.data(), nb, make_phys(&pl->p), flags, stage, pl->p.precision, S(stream));
   } else {
     for (int b = 0; b < nb && s == FJ_OK; ++b) {
       const fj_block& B = pl->blocks[b];
-      s = run_rhs(ctx, q[b], B.kxyz, B.vol, stage > 1 ? q0[b] : q[b], out[b], B.ni, B.nj, B.nk, &pl->p, flags,
-                  stage, dt, tail, S(stream), pl->kxyz32.empty() ? nullptr : pl->kxyz32[b]);
+      fj_params pb = pl->p;
+      if (!pl->mu0_b.empty()) pb.mu0 = pl->mu0_b[b];
+      s = run_rhs(ctx, q[b], B.kxyz, B.vol, stage > 1 ? q0[b] : q[b], out[b], B.ni, B.nj, B.nk, &pb, flags,
+                  stage, pl->dt_b.empty() ? dt : pl->dt_b[b], tail, S(stream),
+                  pl->kmet.empty() ? nullptr : pl->kmet[b]);
     }
   }
   ctx->pipeline = saved;
@@ -571,7 +665,8 @@ int fj_rhs_vjp_f64(fj_ctx* ctx, const double* q, const double* kxyz, const doubl
 static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* q1_saved,
                          const double* const* q2_saved, const double* const* lam_in, double* const* lam_out,
                          int nblocks, const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs,
-                         const fj_params* p, double dt, double* dmu, void* stream);
+                         const fj_params* p, double dt, double* dmu, void* stream, const double* mu0_b = nullptr,
+                         const double* dt_b = nullptr, bool dmu_per_block = false);
 
 int fj_step_vjp_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* lam_in,
                     double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
@@ -601,6 +696,19 @@ int fj_step_vjp_saved_f64(fj_ctx* ctx, const fj_block* blocks, const double* con
                        stream);
 }
 
+int fj_step_vjp_ensemble_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* q1,
+                             const double* const* q2, const double* const* lam_in, double* const* lam_out,
+                             int nblocks, const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs,
+                             const fj_params* p, double dt, const double* mu0, const double* dts, double* dJ_dmu0,
+                             void* stream) {
+  if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
+  if (!q1 || !q2) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "saved stage lists are NULL");
+  for (int b = 0; b < nblocks; ++b)
+    if (!q1[b] || !q2[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "saved stage pointer is NULL");
+  return step_vjp_impl(ctx, blocks, q1, q2, lam_in, lam_out, nblocks, links, nlinks, bcs, nbcs, p, dt, dJ_dmu0,
+                       stream, mu0, dts, true);
+}
+
 int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* const* grad, int nblocks,
                                int ghost, void* stream) {
   if (!ctx || !blocks || !grad || nblocks <= 0 || ghost < 0) return FJ_ERR_INVALID_ARGUMENT;
@@ -615,10 +723,14 @@ int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* cons
 
 // Reverse of one step.  Without saved states, q0' (copy + halo + BC), q1 and
 // q2 are recomputed first; with them, blocks[b].q is q0' and q1/q2 are read.
+// mu0_b / dt_b: per-block overrides (ensembles); dmu_per_block: dmu holds one
+// accumulator per block instead of one in total.
 static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* const* q1_saved,
                          const double* const* q2_saved, const double* const* lam_in, double* const* lam_out,
                          int nblocks, const fj_link* links, int nlinks, const fj_bc* bcs, int nbcs,
-                         const fj_params* p, double dt, double* dmu, void* stream) {
+                         const fj_params* p, double dt, double* dmu, void* stream, const double* mu0_b,
+                         const double* dt_b, bool dmu_per_block) {
+  const double dt_all = dt;
   if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
   if (!lam_in || !lam_out) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "adjoint lists are NULL");
   std::vector<double*> dummy(nblocks > 0 ? nblocks : 1, nullptr);
@@ -662,9 +774,6 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
   double* LA = (double*)(tail + nstage * max5);
   double* LB = (double*)(tail + (nstage + 1) * max5);
   void* wk = tail + (nstage + 2) * max5;
-  // dJ/dmu0 = sum over stages of c_s dt lam_{s+1} . L_vis(q_s) / mu0 (L_vis is
-  // linear in mu0); the viscous VJP kernel accumulates it with this scale.
-  const double inv_mu = p->mu0 != 0.0 ? 1.0 / p->mu0 : 0.0;
   if (!saved) {
     // ---- forward recompute of q0' (copy + halo + BC)
     for (int b = 0; b < nblocks; ++b) {
@@ -684,9 +793,17 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
     double* L0 = l0[b].q;
     const double* Q1 = saved ? q1_saved[b] : Q1w;
     const double* Q2 = saved ? q2_saved[b] : Q2w;
+    fj_params pb = *p;
+    if (mu0_b) pb.mu0 = mu0_b[b];
+    const double dt = dt_b ? dt_b[b] : dt_all;
+    double* dmu_b = dmu ? (dmu_per_block ? dmu + b : dmu) : nullptr;
+    // dJ/dmu0 = sum over stages of c_s dt lam_{s+1} . L_vis(q_s) / mu0 (L_vis is
+    // linear in mu0); the viscous VJP kernel accumulates it with this scale.
+    const double inv_mu = pb.mu0 != 0.0 ? 1.0 / pb.mu0 : 0.0;
+    const fj_params* const pp = &pb;
     if (!saved) {
-      s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, Q1w, B.ni, B.nj, B.nk, p, flags, 1, dt, wk, st);
-      if (s == FJ_OK) s = run_rhs(ctx, Q1w, B.kxyz, B.vol, B.q, Q2w, B.ni, B.nj, B.nk, p, flags, 2, dt, wk, st);
+      s = run_rhs(ctx, B.q, B.kxyz, B.vol, B.q, Q1w, B.ni, B.nj, B.nk, pp, flags, 1, dt, wk, st);
+      if (s == FJ_OK) s = run_rhs(ctx, Q1w, B.kxyz, B.vol, B.q, Q2w, B.ni, B.nj, B.nk, pp, flags, 2, dt, wk, st);
       if (s != FJ_OK) return s;
     }
     // stage 3: q3 = 1/3 q0 + 2/3 (q2 + dt L(q2)):
@@ -694,7 +811,7 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
     VjpEpilogue e3;
     e3.o1 = LB, e3.x1 = lam_in[b], e3.a1 = 2.0 / 3.0, e3.e1 = 2.0 / 3.0 * dt;
     e3.o2 = L0, e3.x2 = lam_in[b], e3.a2 = 1.0 / 3.0;
-    s = rhs_vjp(ctx, Q2, B.kxyz, B.vol, lam_in[b], nullptr, B.ni, B.nj, B.nk, p, flags, wk, st, dmu,
+    s = rhs_vjp(ctx, Q2, B.kxyz, B.vol, lam_in[b], nullptr, B.ni, B.nj, B.nk, pp, flags, wk, st, dmu_b,
                 2.0 / 3.0 * dt * inv_mu, &e3);
     // stage 2: q2 = 3/4 q0 + 1/4 (q1 + dt L(q1)):
     //   LA = 1/4 LB + dt/4 V2,  L0 += 3/4 LB
@@ -702,13 +819,14 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
     e2.o1 = LA, e2.x1 = LB, e2.a1 = 0.25, e2.e1 = 0.25 * dt;
     e2.o2 = L0, e2.x2 = L0, e2.a2 = 1.0, e2.y2 = LB, e2.b2 = 0.75;
     if (s == FJ_OK)
-      s = rhs_vjp(ctx, Q1, B.kxyz, B.vol, LB, nullptr, B.ni, B.nj, B.nk, p, flags, wk, st, dmu,
+      s = rhs_vjp(ctx, Q1, B.kxyz, B.vol, LB, nullptr, B.ni, B.nj, B.nk, pp, flags, wk, st, dmu_b,
                   0.25 * dt * inv_mu, &e2);
     // stage 1: q1 = q0 + dt L(q0):  L0 += LA + dt V1
     VjpEpilogue e1;
     e1.o1 = L0, e1.x1 = L0, e1.a1 = 1.0, e1.y1 = LA, e1.b1 = 1.0, e1.e1 = dt;
     if (s == FJ_OK)
-      s = rhs_vjp(ctx, B.q, B.kxyz, B.vol, LA, nullptr, B.ni, B.nj, B.nk, p, flags, wk, st, dmu, dt * inv_mu, &e1);
+      s = rhs_vjp(ctx, B.q, B.kxyz, B.vol, LA, nullptr, B.ni, B.nj, B.nk, pp, flags, wk, st, dmu_b, dt * inv_mu,
+                  &e1);
     if (s != FJ_OK) return s;
   }
   // ---- transposed boundary conditions, then transposed halo fill
@@ -726,7 +844,10 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
 
 int fj_plan_destroy(fj_plan* pl) {
   if (!pl) return FJ_OK;
-  for (float* k : pl->kxyz32)
+  for (fj_graph_entry& g : pl->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (pl->capture_stream) cudaStreamDestroy(pl->capture_stream);
+  for (void* k : pl->kmet)
     if (k) cudaFree(k);
   if (pl->scratch) cudaFree(pl->scratch);
   delete pl;

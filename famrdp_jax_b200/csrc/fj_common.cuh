@@ -25,18 +25,31 @@ struct fj_ctx {
   int adj_variant = 0;       // face-VJP register cap (FJ_NUM_ADJ_VARIANTS)
 };
 
+// One captured step (fj_plan_step_graph) for a fixed set of state pointers
+// and dt.
+struct fj_graph_entry {
+  std::vector<double*> q_in, q_out;
+  double dt = 0.0;
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;  // kernels in the graph
+};
+
 // A prepared step of one block set (fj_plan_create): tables, the metric
-// pointers, FP32 metric copies for the FP32-flux path, and owned scratch.
+// pointers, metric copies in the layout of the plan's pipeline, and owned
+// scratch.
 struct fj_plan {
   fj_ctx* ctx = nullptr;
   std::vector<fj_block> blocks;
   std::vector<fj_link> links;
   std::vector<fj_bc> bcs;
   fj_params p{};
-  std::vector<float*> kxyz32;
+  std::vector<void*> kmet;  // per-block metric copy for the plan's pipeline (or empty)
   void* scratch = nullptr;   // q1 | q2 | tail (intermediates, halo slabs)
   size_t stage_bytes = 0, halo_bytes = 0;  // halo_bytes: size of the tail
   int pipeline = 0;
+  std::vector<double> mu0_b, dt_b;        // per-block overrides (ensembles), empty = none
+  cudaStream_t capture_stream = nullptr;  // private stream for graph capture
+  std::vector<fj_graph_entry> graphs;     // most recently used last
 };
 
 namespace fj {

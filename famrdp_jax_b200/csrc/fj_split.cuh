@@ -9,29 +9,48 @@
 
 namespace fj {
 
-constexpr int kMaxSplitBlocks = 32;  // blocks per launch (more are chunked)
+constexpr int kMaxSplitBlocks = 64;  // blocks per launch (more are chunked)
+
+// Values per cell of the metric record copy in flux type T: kxyz[l][m]
+// l-major (9 values), padded to a multiple of 16 bytes.
+template <typename T>
+constexpr int kRecK = sizeof(T) == 4 ? 12 : 10;
 
 struct SplitBlock {
   const double* q;       // stage input (5, ni, nj, nk)
   const double* q0;      // step start state (stages 2, 3)
   double* out;           // RHS (stage 0) or stage result; may alias q0, never q
   const double* kxyz;    // (3, 3, ni, nj, nk)
-  const float* kxyz32;   // optional FP32 copy (FP32-flux path) or nullptr
+  const void* kaos;      // FP32-flux only: optional FP32 metric records (kRecK per cell), or nullptr
   const double* vol;     // (ni, nj, nk)
   void* prim;            // scratch: 6 x N flux-type values
   void* F;               // scratch: 15 x N (face c | c+e_a, axis-major)
-  void* G;               // scratch: 9 x N viscous flux components
+  void* G;               // scratch: viscous flux components (records: 8 per cell)
+  void* Gz;              // records only: the ninth component, one per cell
+  double mu0;            // viscosity scale of this block (per-instance ensembles)
+  double dt;             // time step of this block (stages 1..3)
   int ni, nj, nk;
   int cta_begin;         // filled by the launcher
 };
 
+// Metric records (kRecK values of the flux type per cell) from the caller's
+// field-major FP64 kxyz (3, 3, N).
+int split_metric_records(const double* kxyz, void* out, int64_t N, int precision, cudaStream_t st);
+// Bytes of one block's metric records.
+size_t split_metric_record_bytes(int precision, int64_t N);
 // Scratch bytes of the intermediates of `cells` padded cells in total.
 size_t split_scratch_bytes(int precision, int64_t cells);
 // Points prim/F/G of every block into one scratch region of
 // split_scratch_bytes(precision, sum of the blocks' cells) bytes.
 void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* scratch);
-// One RHS (stage 0) or TVD-RK3 stage (1..3) of all blocks: three launches.
+// One RHS (stage 0) or TVD-RK3 stage (1..3) of all blocks: three launches
+// (per chunk of kMaxSplitBlocks blocks).  ph supplies everything but mu0,
+// which comes per block like dt.
+// prims_ready: the blocks' primitives were already written (by the previous
+// stage's assembly with next_prims), so the primitive launch is skipped;
+// next_prims (stages 1, 2): the assembly also writes the primitives of its
+// result for the next stage.
 int split_stage(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                int stage, double dt, int precision, cudaStream_t st);
+                int stage, int precision, cudaStream_t st, bool prims_ready = false, bool next_prims = false);
 
 }  // namespace fj

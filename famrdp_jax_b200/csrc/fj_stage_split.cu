@@ -15,10 +15,18 @@
 //                    (solver/step.py:45-53)
 //
 // Intermediates live in scratch in the flux type T (float on the FP32-flux
-// path, double on the FP64 path): 6 primitives + 15 face-flux + 9 viscous
-// components per cell.  Each launch covers every block of a table; a CTA
-// handles 256 consecutive cells of one block, and neighbours are read through
-// L1/L2 (consecutive threads touch consecutive cells).
+// path, double on the FP64 path) as per-cell RECORDS, so that a cell's fields
+// sit at compile-time offsets from one address and move with 16-byte vector
+// loads and stores:
+//   P  8 T per cell: rho u v w p T (2 pad)
+//   F 16 T per cell: the faces c | c+e_i, c | c+e_j, c | c+e_k, 5 T each (1 pad)
+//   G 12 T per cell: tau_00 tau_01 tau_02 tau_11 tau_12 tau_22, the energy
+//     flux components 0..2 (3 pad)
+// A plan also keeps the metrics as records (kRecK<T> T per cell: the nine
+// kxyz[l][m], l-major, then pad), converted once from the caller's FP64
+// field-major kxyz; without one the kernels read kxyz field by field.
+// Each launch covers every block of a table; a CTA handles 256 consecutive
+// cells of one block, and neighbours are read through L1/L2.
 #include "fj_common.cuh"
 #include "fj_physics.cuh"
 #include "fj_rhs.cuh"
@@ -51,12 +59,18 @@ struct Table {
   int n;
   Dev b[kMaxSplitBlocks];
 };
+static_assert(sizeof(Table) <= 32764, "kernel parameter space (sm_70+, CUDA 12.1+)");
 
-// Locates the block of CTA `cta` (blocks own contiguous CTA ranges).
+// Locates the block of CTA `cta` (blocks own contiguous, increasing CTA
+// ranges): the last b with cta_begin <= cta, by bisection.
 __device__ __forceinline__ int find_block(const Table& t, int cta) {
-  int b = 0;
-  while (b + 1 < t.n && t.b[b + 1].blk.cta_begin <= cta) ++b;
-  return b;
+  int lo = 0, hi = t.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (t.b[mid].blk.cta_begin <= cta) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
 struct Cell {
@@ -82,8 +96,337 @@ __device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x) {
   return true;
 }
 
+// ---- record access -------------------------------------------------------
+constexpr int kRecP = 8, kRecF = 16, kRecG = 8;  // G: 8 components per record + 1 in Gz
+
+// Minimum resident CTAs per SM (register caps): FP64 face arithmetic needs
+// more registers than FP32 at the same occupancy.
+template <typename T>
+struct SplitOcc {
+  static constexpr int fluxes = sizeof(T) == 8 ? 2 : 3;
+  static constexpr int assemble = sizeof(T) == 8 ? 3 : 4;
+};
+
+// n values of a 16-byte aligned record (n a multiple of 16 / sizeof(T)).
+template <typename T, int n>
+__device__ __forceinline__ void ld_rec(const T* __restrict__ p, T* v) {
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int i = 0; i < n / 4; ++i) {
+      const float4 x = __ldg(reinterpret_cast<const float4*>(p) + i);
+      v[4 * i] = x.x;
+      v[4 * i + 1] = x.y;
+      v[4 * i + 2] = x.z;
+      v[4 * i + 3] = x.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < n / 2; ++i) {
+      const double2 x = __ldg(reinterpret_cast<const double2*>(p) + i);
+      v[2 * i] = x.x;
+      v[2 * i + 1] = x.y;
+    }
+  }
+}
+
+template <typename T, int n>
+__device__ __forceinline__ void st_rec(T* __restrict__ p, const T* v) {
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int i = 0; i < n / 4; ++i)
+      reinterpret_cast<float4*>(p)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < n / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(v[2 * i], v[2 * i + 1]);
+  }
+}
+
+template <typename T>
+struct Cell6 {
+  T r, u, v, w, p, t;
+};
+
+template <typename T>
+__device__ __forceinline__ Cell6<T> load_cell(const T* __restrict__ P, int32_t c) {
+  T x[kRecP];
+  ld_rec<T, kRecP>(P + (size_t)c * kRecP, x);
+  return Cell6<T>{x[0], x[1], x[2], x[3], x[4], x[5]};
+}
+
+// The nine kxyz[l][m] of cell c, from the record copy (K_AOS) or from the
+// caller's field-major FP64 array.
+template <typename T, bool K_AOS>
+__device__ __forceinline__ void metric9(const SplitBlock& B, int32_t N, int32_t c, T kk[9]) {
+  if constexpr (K_AOS) {
+    T x[kRecK<T>];
+    ld_rec<T, kRecK<T>>((const T*)B.kaos + (size_t)c * kRecK<T>, x);
+#pragma unroll
+    for (int lm = 0; lm < 9; ++lm) kk[lm] = x[lm];
+  } else {
+#pragma unroll
+    for (int lm = 0; lm < 9; ++lm) kk[lm] = (T)__ldg(B.kxyz + (size_t)lm * N + c);
+  }
+}
+
+// Row l (kxyz[l][0..2]) of cell c.
+template <typename T, bool K_AOS>
+__device__ __forceinline__ void metric_row(const SplitBlock& B, int32_t N, int l, int32_t c, T k[3]) {
+  if constexpr (K_AOS) {
+    const T* K = (const T*)B.kaos + (size_t)c * kRecK<T> + 3 * l;
+    k[0] = __ldg(K);
+    k[1] = __ldg(K + 1);
+    k[2] = __ldg(K + 2);
+  } else {
+    const double* K = B.kxyz + (size_t)(3 * l) * N + c;
+    k[0] = (T)__ldg(K);
+    k[1] = (T)__ldg(K + N);
+    k[2] = (T)__ldg(K + 2 * (size_t)N);
+  }
+}
+
+// Primitives rho u v w p T of one cell from its conserved values, in FP64
+// (physics/eos.py:12-17; T = p / max(rho R, 1e-300), rhs/viscous.py:36).
+__device__ __forceinline__ void prims_of(const double q[5], double gm1, double R, double out[6]) {
+  const double r = q[0];
+  const double ir = 1.0 / r;
+  const double u = q[1] * ir, v = q[2] * ir, w = q[3] * ir;
+  const double p = gm1 * (q[4] - r * (0.5 * (u * u + v * v + w * w)));
+  out[0] = r;
+  out[1] = u;
+  out[2] = v;
+  out[3] = w;
+  out[4] = p;
+  out[5] = r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, const double gm1,
+                                                              const double R) {
+  const int b = find_block(tab, blockIdx.x);
+  const SplitBlock& B = tab.b[b].blk;
+  const int32_t N = B.ni * B.nj * B.nk;
+  const int32_t c = (blockIdx.x - B.cta_begin) * kSplitThreads + threadIdx.x;
+  if (c >= N) return;
+  const double* q = B.q + c;
+  const double qc[5] = {q[0], q[N], q[2 * (size_t)N], q[3 * (size_t)N], q[4 * (size_t)N]};
+  double pv[6];
+  prims_of(qc, gm1, R, pv);
+  const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)pv[4], (T)pv[5], T(0), T(0)};
+  st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
+}
+
+// Roe face c | c+e_a from the primitives of c-e_a, c, c+e_a, c+2e_a and the
+// kxyz rows of c and c+e_a (rhs/invscd.py:62-100).
+template <typename T>
+__device__ __forceinline__ void face_from_cells(const Cell6<T>& a0, const Cell6<T>& a1, const Cell6<T>& a2,
+                                                const Cell6<T>& a3, const T kl[3], const T kr[3],
+                                                const Phys& ph, T* F) {
+  Prim<T> cell[4] = {{a0.r, a0.u, a0.v, a0.w, a0.p}, {a1.r, a1.u, a1.v, a1.w, a1.p},
+                     {a2.r, a2.u, a2.v, a2.w, a2.p}, {a3.r, a3.u, a3.v, a3.w, a3.p}};
+  invscd_face_fast<T>(cell, kl[0], kl[1], kl[2], kr[0], kr[1], kr[2], (T)ph.gm1, (T)ph.inv_gm1,
+                      (T)ph.eps_entropy, ph.limiter, F);
+}
+
+template <typename T, bool K_AOS>
+__global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::fluxes) k_split_fluxes(const Table tab, const Phys ph,
+                                                                                   const int flags) {
+  using M = FastMath<T>;
+  const int b = find_block(tab, blockIdx.x);
+  Cell x;
+  if (!decode(tab.b[b], blockIdx.x, x)) return;
+  const SplitBlock& B = tab.b[b].blk;
+  // 32-bit cell indices: kRecF N < 2^31 is checked on the host
+  const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
+  const int32_t si = x.nj * x.nk, sj = x.nk;
+  const T* __restrict__ P = (const T*)B.prim;
+  const bool vis = (flags & kRhsViscous) != 0, inv = (flags & kRhsInvscd) != 0;
+
+  // neighbour offsets with the padded-array wrap (jnp.roll) for the viscous
+  // stencil; faces exist only where no wrap is involved
+  const int32_t ip = x.i + 1 == x.ni ? c - (x.ni - 1) * si : c + si;
+  const int32_t im = x.i == 0 ? c + (x.ni - 1) * si : c - si;
+  const int32_t jp = x.j + 1 == x.nj ? c - (x.nj - 1) * sj : c + sj;
+  const int32_t jm = x.j == 0 ? c + (x.nj - 1) * sj : c - sj;
+  const int32_t kp = x.k + 1 == x.nk ? c - (x.nk - 1) : c + 1;
+  const int32_t km = x.k == 0 ? c + (x.nk - 1) : c - 1;
+
+  const Cell6<T> C0 = load_cell<T>(P, c);
+  const Cell6<T> Im = load_cell<T>(P, im), Ip = load_cell<T>(P, ip);
+  const Cell6<T> Jm = load_cell<T>(P, jm), Jp = load_cell<T>(P, jp);
+  const Cell6<T> Km = load_cell<T>(P, km), Kp = load_cell<T>(P, kp);
+  T kk[9];
+  metric9<T, K_AOS>(B, N, c, kk);
+
+  if (vis) {
+    // viscous flux components at c (rhs/viscous.py:36-105)
+    const T h = T(0.5);
+    const T d[4][3] = {{h * (Ip.u - Im.u), h * (Jp.u - Jm.u), h * (Kp.u - Km.u)},
+                       {h * (Ip.v - Im.v), h * (Jp.v - Jm.v), h * (Kp.v - Km.v)},
+                       {h * (Ip.w - Im.w), h * (Jp.w - Jm.w), h * (Kp.w - Km.w)},
+                       {h * (Ip.t - Im.t), h * (Jp.t - Jm.t), h * (Kp.t - Km.t)}};
+    T g[4][3];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int m = 0; m < 3; ++m) g[s][m] = d[s][0] * kk[m] + d[s][1] * kk[3 + m] + d[s][2] * kk[6 + m];
+    T mu = (T)B.mu0;
+    if (ph.visc_law == 0) {  // Sutherland (physics/eos.py:24-25)
+      const T r = C0.t * (T)ph.inv_T0;
+      mu = (T)B.mu0 * (r * M::sqrt_pos(r)) * (T)ph.sfac * M::rcp(C0.t + (T)ph.Ts);
+    }
+    const T kappa = (T)ph.kap_fac * mu;
+    const T third = (T)(1.0 / 3.0);
+    const T div_u = g[0][0] + g[1][1] + g[2][2];
+    const T t00 = T(2) * mu * (g[0][0] - div_u * third);
+    const T t01 = mu * (g[0][1] + g[1][0]);
+    const T t02 = mu * (g[0][2] + g[2][0]);
+    const T t11 = T(2) * mu * (g[1][1] - div_u * third);
+    const T t12 = mu * (g[1][2] + g[2][1]);
+    const T t22 = T(2) * mu * (g[2][2] - div_u * third);
+    const T rec[kRecG] = {t00, t01, t02, t11, t12, t22,
+                          C0.u * t00 + C0.v * t01 + C0.w * t02 + kappa * g[3][0],
+                          C0.u * t01 + C0.v * t11 + C0.w * t12 + kappa * g[3][1]};
+    st_rec<T, kRecG>((T*)B.G + (size_t)c * kRecG, rec);
+    ((T*)B.Gz)[c] = C0.u * t02 + C0.v * t12 + C0.w * t22 + kappa * g[3][2];
+  }
+  if (inv) {
+    // the three faces c | c+e_a for c_a in [1, n_a - 3]; invalid faces are
+    // stored as zeros (never read)
+    T Fr[kRecF];
+#pragma unroll
+    for (int v = 0; v < kRecF; ++v) Fr[v] = T(0);
+    T kn[3];
+    if (x.i >= 1 && x.i <= x.ni - 3) {
+      const Cell6<T> I2 = load_cell<T>(P, c + 2 * si);
+      metric_row<T, K_AOS>(B, N, 0, c + si, kn);
+      face_from_cells<T>(Im, C0, Ip, I2, kk, kn, ph, Fr);
+    }
+    if (x.j >= 1 && x.j <= x.nj - 3) {
+      const Cell6<T> J2 = load_cell<T>(P, c + 2 * sj);
+      metric_row<T, K_AOS>(B, N, 1, c + sj, kn);
+      face_from_cells<T>(Jm, C0, Jp, J2, kk + 3, kn, ph, Fr + 5);
+    }
+    if (x.k >= 1 && x.k <= x.nk - 3) {
+      const Cell6<T> K2 = load_cell<T>(P, c + 2);
+      metric_row<T, K_AOS>(B, N, 2, c + 1, kn);
+      face_from_cells<T>(Km, C0, Kp, K2, kk + 6, kn, ph, Fr + 10);
+    }
+    st_rec<T, kRecF>((T*)B.F + (size_t)c * kRecF, Fr);
+  }
+}
+
+// With next_prims, also writes the primitives of the stage result (the next
+// stage's input) in place of a separate k_split_prims launch.
+template <typename T, bool K_AOS>
+__global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::assemble) k_split_assemble(const Table tab,
+                                                                                       const int flags,
+                                                                                       const int stage,
+                                                                                       const int next_prims,
+                                                                                       const double gm1,
+                                                                                       const double R) {
+  const int b = find_block(tab, blockIdx.x);
+  Cell x;
+  if (!decode(tab.b[b], blockIdx.x, x)) return;
+  const SplitBlock& B = tab.b[b].blk;
+  const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
+  const int32_t si = x.nj * x.nk, sj = x.nk;
+  const int n[3] = {x.ni, x.nj, x.nk};
+  const int idx[3] = {x.i, x.j, x.k};
+  const int32_t st[3] = {si, sj, 1};
+  double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (flags & kRhsInvscd) {
+    const T* F = (const T*)B.F;
+    const bool on[3] = {idx[0] >= 2 && idx[0] <= n[0] - 3, idx[1] >= 2 && idx[1] <= n[1] - 3,
+                        idx[2] >= 2 && idx[2] <= n[2] - 3};
+    if (on[0] || on[1] || on[2]) {
+      const double ivd = 1.0 / (B.vol[c] + 1e-300);
+      T Fc[kRecF];
+      ld_rec<T, kRecF>(F + (size_t)c * kRecF, Fc);
+      T Fm[3][5];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) Fm[a][v] = on[a] ? F[(size_t)(c - st[a]) * kRecF + 5 * a + v] : T(0);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        double dsum;
+        if (sizeof(T) == sizeof(double)) {
+          dsum = 0.0;  // axis by axis like the reference
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            if (on[a]) dsum += (double)(Fc[5 * a + v] - Fm[a][v]);
+        } else {
+          T s = T(0);
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            if (on[a]) s += Fc[5 * a + v] - Fm[a][v];
+          dsum = (double)s;
+        }
+        r[v] = -dsum * ivd;
+      }
+    }
+  }
+  if (flags & kRhsViscous) {
+    // sum_l 0.5 kxyz[l][jj] (G(c+e_l) - G(c-e_l)) per equation, one
+    // neighbour record at a time (rhs/viscous.py:86-117)
+    const T* G = (const T*)B.G;
+    const T* Gz = (const T*)B.Gz;
+    T kk[9];
+    metric9<T, K_AOS>(B, N, c, kk);
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        const int32_t nb = side == 0 ? (idx[l] + 1 == n[l] ? c - (n[l] - 1) * st[l] : c + st[l])
+                                     : (idx[l] == 0 ? c + (n[l] - 1) * st[l] : c - st[l]);
+        const T s = side == 0 ? T(0.5) : T(-0.5);
+        T g[kRecG];
+        ld_rec<T, kRecG>(G + (size_t)nb * kRecG, g);
+        const T gz = Gz[nb];
+        const T k0 = s * kk[3 * l], k1 = s * kk[3 * l + 1], k2 = s * kk[3 * l + 2];
+        acc[0] += g[0] * k0 + g[1] * k1 + g[2] * k2;
+        acc[1] += g[1] * k0 + g[3] * k1 + g[4] * k2;
+        acc[2] += g[2] * k0 + g[4] * k1 + g[5] * k2;
+        acc[3] += g[6] * k0 + g[7] * k1 + gz * k2;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) r[e + 1] += (double)acc[e];
+  }
+  double* out = B.out + c;
+  if (stage == 0) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) out[(size_t)v * N] = r[v];
+  } else {
+    const double ca = stage == 2 ? 0.75 : 1.0 / 3.0;
+    const double cb = stage == 2 ? 0.25 : 2.0 / 3.0;
+    const double* q = B.q + c;
+    const double* q0 = B.q0 + c;
+    double qn[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double t = q[(size_t)v * N] + B.dt * r[v];
+      qn[v] = stage == 1 ? t : ca * q0[(size_t)v * N] + cb * t;
+      out[(size_t)v * N] = qn[v];
+    }
+    if (next_prims) {
+      double pv[6];
+      prims_of(qn, gm1, R, pv);
+      const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)pv[4], (T)pv[5], T(0), T(0)};
+      st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
+    }
+  }
+}
+
+// ---- field-major variant (the FP64 path) ----------------------------------
+// The FP64 path keeps its intermediates field-major (6 + 15 + 9 arrays of N):
+// 16-byte records would cost it more registers (two doubles per vector lane)
+// and padding bytes than the index arithmetic they save.
+namespace fm {
+
+template <typename T>
+__global__ void __launch_bounds__(kSplitThreads) k_fm_prims(const Table tab, const double gm1,
                                                               const double R) {
   const int b = find_block(tab, blockIdx.x);
   const SplitBlock& B = tab.b[b].blk;
@@ -107,7 +450,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, 
 
 template <typename T>
 __device__ __forceinline__ T metric(const SplitBlock& B, int64_t N, int lm, int64_t c) {
-  return B.kxyz32 ? (T)__ldg(B.kxyz32 + lm * N + c) : (T)__ldg(B.kxyz + lm * N + c);
+  return (T)__ldg(B.kxyz + lm * N + c);
 }
 
 // Primitives (rho, u, v, w, p[, T]) of one cell from the field-major scratch.
@@ -142,21 +485,14 @@ __device__ __forceinline__ void face_from_cells(const Cell6<T>& a0, const Cell6<
 
 template <typename T>
 __device__ __forceinline__ void metric_row(const SplitBlock& B, int32_t N, int row, int32_t c, T k[3]) {
-  if (B.kxyz32) {
-    const float* K = B.kxyz32 + 3 * row * N;
-    k[0] = (T)__ldg(K + c);
-    k[1] = (T)__ldg(K + N + c);
-    k[2] = (T)__ldg(K + 2 * N + c);
-  } else {
-    const double* K = B.kxyz + 3 * row * N;
-    k[0] = (T)__ldg(K + c);
-    k[1] = (T)__ldg(K + N + c);
-    k[2] = (T)__ldg(K + 2 * N + c);
-  }
+  const double* K = B.kxyz + 3 * row * N;
+  k[0] = (T)__ldg(K + c);
+  k[1] = (T)__ldg(K + N + c);
+  k[2] = (T)__ldg(K + 2 * N + c);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSplitThreads) k_split_fluxes(const Table tab, const Phys ph,
+__global__ void __launch_bounds__(kSplitThreads, 2) k_fm_fluxes(const Table tab, const Phys ph,
                                                                const int flags) {
   using M = FastMath<T>;
   const int b = find_block(tab, blockIdx.x);
@@ -199,10 +535,10 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_fluxes(const Table tab,
     for (int s = 0; s < 4; ++s)
 #pragma unroll
       for (int m = 0; m < 3; ++m) g[s][m] = d[s][0] * kk[m] + d[s][1] * kk[3 + m] + d[s][2] * kk[6 + m];
-    T mu = (T)ph.mu0;
+    T mu = (T)B.mu0;
     if (ph.visc_law == 0) {  // Sutherland (physics/eos.py:24-25)
       const T r = C0.t * (T)ph.inv_T0;
-      mu = (T)ph.mu0 * (r * M::sqrt_pos(r)) * (T)ph.sfac * M::rcp(C0.t + (T)ph.Ts);
+      mu = (T)B.mu0 * (r * M::sqrt_pos(r)) * (T)ph.sfac * M::rcp(C0.t + (T)ph.Ts);
     }
     const T kappa = (T)ph.kap_fac * mu;
     const T third = (T)(1.0 / 3.0);
@@ -256,8 +592,9 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_fluxes(const Table tab,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSplitThreads) k_split_assemble(const Table tab, const int flags,
-                                                                 const int stage, const double dt) {
+__global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table tab, const int flags,
+                                                                 const int stage, const int next_prims,
+                                                                 const double gm1, const double R) {
   const int b = find_block(tab, blockIdx.x);
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
@@ -334,37 +671,81 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_assemble(const Table ta
   } else {
     const double ca = stage == 2 ? 0.75 : 1.0 / 3.0;
     const double cb = stage == 2 ? 0.25 : 2.0 / 3.0;
+    double qn[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const int64_t o = v * N + c;
-      const double t = B.q[o] + dt * r[v];
-      B.out[o] = stage == 1 ? t : ca * B.q0[o] + cb * t;
+      const double t = B.q[o] + B.dt * r[v];
+      qn[v] = stage == 1 ? t : ca * B.q0[o] + cb * t;
+      B.out[o] = qn[v];
+    }
+    if (next_prims) {
+      double pv[6];
+      prims_of(qn, gm1, R, pv);
+      T* P = (T*)B.prim;
+#pragma unroll
+      for (int v = 0; v < 6; ++v) P[v * N + c] = (T)pv[v];
     }
   }
 }
 
+
+}  // namespace fm
+
+template <typename T>
+__global__ void k_metric_records(const double* __restrict__ kxyz, T* __restrict__ out, int64_t N) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  T rec[kRecK<T>];
+#pragma unroll
+  for (int lm = 0; lm < 9; ++lm) rec[lm] = (T)kxyz[lm * N + c];
+#pragma unroll
+  for (int lm = 9; lm < kRecK<T>; ++lm) rec[lm] = T(0);
+  st_rec<T, kRecK<T>>(out + c * kRecK<T>, rec);
+}
+
+template <typename T, bool K_AOS>
+int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage, bool prims_ready,
+               bool next_prims, cudaStream_t st) {
+  const int np = next_prims ? 1 : 0;
+  if constexpr (sizeof(T) == 8) {
+    if (!prims_ready) fm::k_fm_prims<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R);
+    fm::k_fm_fluxes<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
+    fm::k_fm_assemble<double><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R);
+  } else {
+    if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R);
+    k_split_fluxes<T, K_AOS><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
+    k_split_assemble<T, K_AOS><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R);
+  }
+  return prims_ready ? 2 : 3;
+}
+
 template <typename T>
 int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                 int stage, double dt, cudaStream_t st) {
+                 int stage, bool prims_ready, bool next_prims, cudaStream_t st) {
   for (int base = 0; base < nblocks; base += kMaxSplitBlocks) {
     Table tab;
     tab.n = std::min(kMaxSplitBlocks, nblocks - base);
     int ctas = 0;
+    const bool k_aos = blocks[base].kaos != nullptr;
     for (int t = 0; t < tab.n; ++t) {
-      // the kernels index the 15 face-flux fields with 32-bit offsets
-      if (15 * (int64_t)blocks[base + t].ni * blocks[base + t].nj * blocks[base + t].nk > INT32_MAX)
+      const SplitBlock& sb = blocks[base + t];
+      // the kernels index cells and records with 32-bit offsets
+      if ((int64_t)kRecF * sb.ni * sb.nj * sb.nk > INT32_MAX)
         return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "block too large for the split pipeline");
-      tab.b[t].blk = blocks[base + t];
+      if ((sb.kaos != nullptr) != k_aos)
+        return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "metric records on some blocks only");
+      tab.b[t].blk = sb;
       tab.b[t].blk.cta_begin = ctas;
-      tab.b[t].dk.init((uint32_t)blocks[base + t].nk);
-      tab.b[t].dj.init((uint32_t)blocks[base + t].nj);
-      const int64_t N = (int64_t)blocks[base + t].ni * blocks[base + t].nj * blocks[base + t].nk;
+      tab.b[t].dk.init((uint32_t)sb.nk);
+      tab.b[t].dj.init((uint32_t)sb.nj);
+      const int64_t N = (int64_t)sb.ni * sb.nj * sb.nk;
       ctas += (int)((N + kSplitThreads - 1) / kSplitThreads);
     }
-    k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R);
-    k_split_fluxes<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
-    k_split_assemble<T><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, dt);
-    ctx->launches += 3;
+    if (k_aos && sizeof(T) == 8)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "the FP64 split path reads kxyz directly");
+    ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, ph, flags, stage, prims_ready, next_prims, st)
+                           : launch_tab<T, false>(tab, ctas, ph, flags, stage, prims_ready, next_prims, st);
     int s = launch_status(ctx, "split stage launch");
     if (s != FJ_OK) return s;
   }
@@ -373,35 +754,70 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
 
 }  // namespace
 
+int split_metric_records(const double* kxyz, void* out, int64_t N, int precision, cudaStream_t st) {
+  if (N <= 0) return FJ_OK;
+  const int grid = (int)((N + 255) / 256);
+  if (precision == FJ_PREC_F32FLUX)
+    k_metric_records<float><<<grid, 256, 0, st>>>(kxyz, (float*)out, N);
+  else
+    k_metric_records<double><<<grid, 256, 0, st>>>(kxyz, (double*)out, N);
+  return cudaGetLastError() == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
+}
+
+size_t split_metric_record_bytes(int precision, int64_t N) {
+  return precision == FJ_PREC_F32FLUX ? (size_t)N * kRecK<float> * sizeof(float)
+                                      : (size_t)N * kRecK<double> * sizeof(double);
+}
+
+// Values per cell of each intermediate: records (FP32-flux) or field-major
+// arrays (FP64).
+static void split_counts(int precision, int& nP, int& nF, int& nG) {
+  const bool rec = precision == FJ_PREC_F32FLUX;
+  nP = rec ? kRecP : 6;
+  nF = rec ? kRecF : 15;
+  nG = 9;  // records: kRecG per cell in G, then one per cell in Gz
+}
+
 size_t split_scratch_bytes(int precision, int64_t cells) {
   const size_t t = precision == FJ_PREC_F32FLUX ? sizeof(float) : sizeof(double);
-  return (size_t)(6 + 15 + 9) * (size_t)cells * t + 3 * 256;
+  int nP, nF, nG;
+  split_counts(precision, nP, nF, nG);
+  return (size_t)(nP + nF + nG) * (size_t)cells * t + 3 * 256;
 }
 
 void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* scratch) {
   const size_t t = precision == FJ_PREC_F32FLUX ? sizeof(float) : sizeof(double);
+  int nP, nF, nG;
+  split_counts(precision, nP, nF, nG);
   char* p = (char*)scratch;
   auto al = [](char* x) { return (char*)(((uintptr_t)x + 255) & ~(uintptr_t)255); };
   int64_t total = 0;
   for (int b = 0; b < nblocks; ++b) total += (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
   char* prim = al(p);
-  char* F = al(prim + 6 * total * t);
-  char* G = al(F + 15 * total * t);
+  char* F = al(prim + nP * total * t);
+  char* G = al(F + nF * total * t);
   int64_t off = 0;
   for (int b = 0; b < nblocks; ++b) {
     const int64_t N = (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
-    blocks[b].prim = prim + 6 * off * t;
-    blocks[b].F = F + 15 * off * t;
-    blocks[b].G = G + 9 * off * t;
+    blocks[b].prim = prim + nP * off * t;  // records are multiples of 16 bytes
+    blocks[b].F = F + nF * off * t;
+    if (precision == FJ_PREC_F32FLUX) {
+      blocks[b].G = G + kRecG * off * t;
+      blocks[b].Gz = G + (kRecG * total + off) * t;
+    } else {
+      blocks[b].G = G + nG * off * t;
+      blocks[b].Gz = nullptr;
+    }
     off += N;
   }
 }
 
 int split_stage(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                int stage, double dt, int precision, cudaStream_t st) {
+                int stage, int precision, cudaStream_t st, bool prims_ready, bool next_prims) {
+  if (next_prims && (stage < 1 || stage > 2)) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "next_prims needs stage 1 or 2");
   if (precision == FJ_PREC_F32FLUX)
-    return launch_split<float>(ctx, blocks, nblocks, ph, flags, stage, dt, st);
-  return launch_split<double>(ctx, blocks, nblocks, ph, flags, stage, dt, st);
+    return launch_split<float>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, st);
+  return launch_split<double>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, st);
 }
 
 }  // namespace fj

@@ -77,23 +77,36 @@ def step_vjp(qs, metrics, cfg: Config, dt: float, lams, *, tables: _Tables | Non
 
 
 def step_vjp_saved(saved, metrics, cfg: Config, dt: float, lams, *, tables: _Tables | None = None,
-                   dmu: torch.Tensor | None = None):
+                   dmu: torch.Tensor | None = None, mu0s=None, dts=None, out=None):
     """step_vjp on the states a StepPlan.run_save kept: saved = (q0s, q1s, q2s)
-    with q0s the halo-filled start states; the step's forward is not rerun."""
+    with q0s the halo-filled start states; the step's forward is not rerun.
+    For an ensemble (mu0s / dts per block, as given to StepPlan.set_ensemble)
+    ``dmu`` has one entry per block and receives each block's dJ/dmu0.
+    ``out`` (optional) receives the result and may be ``lams`` itself."""
     t = tables or _Tables(cfg)
     q0s, q1s, q2s = saved
+    n = len(q0s)
     dev = q0s[0].device
     c = _capi.ctx(dev)
-    outs = [torch.empty_like(q) for q in q0s]
+    outs = out if out is not None else [torch.empty_like(q) for q in q0s]
     lam_c = [l.contiguous() for l in lams]
-    lam_in = (ctypes.c_void_p * len(q0s))(*[_capi.dev_ptr(l, "lam") for l in lam_c])
+    lam_in = (ctypes.c_void_p * n)(*[_capi.dev_ptr(l, "lam") for l in lam_c])
     blocks = _topology.block_array(list(q0s), metrics)
     pa = _topology.ptr_array
-    st = _capi.lib().fj_step_vjp_saved_f64(c, blocks, pa(q1s), pa(q2s), lam_in, pa(outs), len(q0s), t.link_arr,
-                                           len(t.links), t.bc_arr, len(t.bcs), t.params, float(dt),
-                                           _capi.dev_ptr(dmu, "dmu") if dmu is not None else None,
-                                           _capi.stream(dev))
-    _capi.check(st, "fj_step_vjp_saved_f64", c)
+    dmu_p = _capi.dev_ptr(dmu, "dmu") if dmu is not None else None
+    if mu0s is None and dts is None:
+        st = _capi.lib().fj_step_vjp_saved_f64(c, blocks, pa(q1s), pa(q2s), lam_in, pa(outs), n, t.link_arr,
+                                               len(t.links), t.bc_arr, len(t.bcs), t.params, float(dt), dmu_p,
+                                               _capi.stream(dev))
+        _capi.check(st, "fj_step_vjp_saved_f64", c)
+        return outs
+    if dmu is not None and dmu.numel() != n:
+        raise ValueError("an ensemble's dmu needs one entry per block")
+    arr = (lambda x: None if x is None else (ctypes.c_double * n)(*[float(v) for v in x]))
+    st = _capi.lib().fj_step_vjp_ensemble_f64(c, blocks, pa(q1s), pa(q2s), lam_in, pa(outs), n, t.link_arr,
+                                              len(t.links), t.bc_arr, len(t.bcs), t.params, float(dt), arr(mu0s),
+                                              arr(dts), dmu_p, _capi.stream(dev))
+    _capi.check(st, "fj_step_vjp_ensemble_f64", c)
     return outs
 
 
@@ -108,23 +121,6 @@ def kinetic_energy_grad(qs, metrics, ghost: int = 2):
     return grads
 
 
-def _forward_segment(plan: StepPlan, qs, dt, nsteps, keep: bool):
-    """nsteps steps from qs; returns the final state and, if keep, each step's
-    saved intermediate states (halo-filled start state, stage 1 and 2)."""
-    states = []
-    cur = list(qs)
-    for _ in range(nsteps):
-        nxt = [torch.empty_like(q) for q in cur]
-        if keep:
-            saved = tuple([torch.empty_like(q) for q in cur] for _ in range(3))
-            plan.run_save(cur, nxt, *saved, dt)
-            states.append(saved)
-        else:
-            plan.run(cur, nxt, dt)
-        cur = nxt
-    return cur, states
-
-
 @dataclass
 class _Run:
     cfg: Config
@@ -135,18 +131,49 @@ class _Run:
     plan: StepPlan
     tables: _Tables
     dmu: torch.Tensor | None = None
+    # device buffers reused by every segment (allocated on first use): two
+    # state sets to ping-pong through a segment and one (q0', q1, q2) triple
+    # per step of a segment
+    _ping: list | None = None
+    _saved: list | None = None
+
+    def buffers(self, like):
+        if self._ping is None:
+            self._ping = [[torch.empty_like(q) for q in like] for _ in range(2)]
+            self._saved = [tuple([torch.empty_like(q) for q in like] for _ in range(3)) for _ in range(self.every)]
+        return self._ping, self._saved
+
+
+def _forward_segment(run: _Run, qs, nsteps, keep: bool):
+    """nsteps steps from qs through the run's ping-pong buffers; returns the
+    final state (a ping-pong buffer) and, if keep, each step's saved
+    intermediate states (halo-filled start state, stage 1 and 2)."""
+    ping, pool = run.buffers(qs)
+    states = []
+    cur = list(qs)
+    for n in range(nsteps):
+        nxt = ping[n % 2]
+        if keep:
+            run.plan.run_save(cur, nxt, *pool[n], run.dt)
+            states.append(pool[n])
+        else:
+            run.plan.run(cur, nxt, run.dt)
+        cur = nxt
+    return cur, states
 
 
 def _reverse_sweep(run: _Run, checkpoints, lams):
     """Segments in reverse: recompute the segment's states from its checkpoint
     (keeping each step's stage states), then apply the step adjoints
-    backwards, releasing each step's states once its adjoint has run."""
+    backwards.  The adjoint is updated in place in one working copy."""
+    lams = [l.clone() for l in lams]
     nseg = len(checkpoints)
     for s in reversed(range(nseg)):
         seg_len = min(run.every, run.nsteps - s * run.every)
-        _, states = _forward_segment(run.plan, checkpoints[s], run.dt, seg_len, keep=True)
+        _, states = _forward_segment(run, checkpoints[s], seg_len, keep=True)
         while states:
-            lams = step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu)
+            step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu,
+                           mu0s=run.plan.mu0s, dts=run.plan.dts, out=lams)
     return lams
 
 
@@ -157,9 +184,9 @@ def _forward_with_checkpoints(run: _Run, q0s):
     while done < run.nsteps:
         checkpoints.append([q.clone() for q in cur])
         n = min(run.every, run.nsteps - done)
-        cur, _ = _forward_segment(run.plan, cur, run.dt, n, keep=False)
+        cur, _ = _forward_segment(run, cur, n, keep=False)
         done += n
-    return cur, checkpoints
+    return [q.clone() for q in cur], checkpoints
 
 
 class _Trajectory(torch.autograd.Function):
@@ -209,3 +236,25 @@ def adjoint_kinetic_energy(state: State, cfg: Config, dt: float, nsteps: int, ch
     lams = kinetic_energy_grad(final, state.metrics, cfg.ghost)
     grads = _reverse_sweep(run, checkpoints, lams)
     return J, grads, float(dmu.item())
+
+
+def adjoint_kinetic_energy_ensemble(state: State, cfg: Config, nsteps: int, *, mu0s, dts,
+                                    checkpoint_every: int = 10, plan: StepPlan | None = None):
+    """Per-instance adjoint of an ensemble of independent blocks (block b with
+    its own mu0s[b] and dts[b]): J_b = kinetic energy of block b after nsteps
+    steps, and dJ_b/dq0_b and dJ_b/dmu0_b for every b, from one checkpointed
+    reverse sweep of all blocks (the objective sum_b J_b decouples)."""
+    plan = plan or StepPlan(state, cfg)
+    plan.set_ensemble(mu0s, dts)
+    dev = state.blocks[0].q.device
+    nb = len(state.blocks)
+    dmu = torch.zeros(nb, dtype=torch.float64, device=dev)
+    run = _Run(cfg=cfg, metrics=state.metrics, dt=0.0, nsteps=int(nsteps), every=max(1, int(checkpoint_every)),
+               plan=plan, tables=_Tables(cfg), dmu=dmu)
+    final, checkpoints = _forward_with_checkpoints(run, [b.q for b in state.blocks])
+    from famrdp_jax_b200.solver import diagnostics
+    Js = [diagnostics.kinetic_energy(State(blocks=(Block(q=q, xyz=b.xyz),), metrics=(m,)), cfg.ghost)
+          for q, b, m in zip(final, state.blocks, state.metrics)]
+    lams = kinetic_energy_grad(final, state.metrics, cfg.ghost)
+    grads = _reverse_sweep(run, checkpoints, lams)
+    return Js, grads, dmu.cpu().tolist()

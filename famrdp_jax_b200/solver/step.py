@@ -74,13 +74,37 @@ class StepPlan:
                                                self.params, ctypes.byref(h)), "fj_plan_create", c)
         self._handle = h.value
         self._lib = _capi.lib()
+        self.mu0s = None
+        self.dts = None
 
-    def run(self, qs, outs, dt: float) -> None:
+    def run(self, qs, outs, dt: float, graph: bool = False) -> None:
+        """One step qs -> outs.  With graph=True the step is captured once per
+        (qs, outs, dt) pointer set as a CUDA graph and replayed afterwards
+        (use fixed ping-pong buffers)."""
         if [tuple(q.shape) for q in qs] != self.shapes or [tuple(o.shape) for o in outs] != self.shapes:
             raise ValueError("state shapes differ from the plan's")
         c = _capi.ctx(self.device)
-        _capi.check(self._lib.fj_plan_step(self._handle, _topology.ptr_array(qs), _topology.ptr_array(outs),
-                                           float(dt), _capi.stream(self.device)), "fj_plan_step", c)
+        fn = self._lib.fj_plan_step_graph if graph else self._lib.fj_plan_step
+        _capi.check(fn(self._handle, _topology.ptr_array(qs), _topology.ptr_array(outs), float(dt),
+                       _capi.stream(self.device)), "fj_plan_step_graph" if graph else "fj_plan_step", c)
+
+    def set_ensemble(self, mu0=None, dt=None) -> None:
+        """Per-block viscosity scale and time step (independent instances):
+        block b then uses mu0[b] and dt[b], and the dt argument of run/stage is
+        ignored while dt is set.  None restores the plan-wide value."""
+        n = len(self.shapes)
+
+        def arr(x):
+            if x is None:
+                return None
+            if len(x) != n:
+                raise ValueError("one value per block expected")
+            return (ctypes.c_double * n)(*[float(v) for v in x])
+
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_set_ensemble(self._handle, arr(mu0), arr(dt)), "fj_plan_set_ensemble", c)
+        self.mu0s = None if mu0 is None else [float(v) for v in mu0]
+        self.dts = None if dt is None else [float(v) for v in dt]
 
     def run_save(self, qs, outs, q0s, q1s, q2s, dt: float) -> None:
         """One step that also keeps its intermediate states (the halo-filled

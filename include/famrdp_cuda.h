@@ -209,9 +209,10 @@ int fj_rk_stage_f64(fj_ctx* ctx, const double* q, const double* q0, const double
 /* A prepared step (solver/step.py:18-56 for a fixed block set): the link and
  * boundary tables are copied and checked once, the metrics are bound (they
  * must stay valid and unchanged while the plan lives) and, for the FP32-flux
- * precision, an FP32 copy of every block's kxyz is built.  The plan owns its
- * scratch, so fj_plan_step allocates nothing.  Creation synchronises the
- * device. */
+ * precision, an FP32 copy of every block's kxyz is built in the layout of the
+ * context's pipeline (split: per-cell records, 48 B per cell; fused:
+ * field-major).  The plan owns its scratch,
+ * so fj_plan_step allocates nothing.  Creation synchronises the device. */
 typedef struct fj_plan fj_plan;
 int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
                    int nlinks, const fj_bc* bcs, int nbcs, const fj_params* p, fj_plan** out);
@@ -226,6 +227,21 @@ int fj_plan_step(fj_plan* plan, double* const* q_in, double* const* q_out, doubl
 int fj_plan_step_save(fj_plan* plan, double* const* q_in, double* const* q_out,
                       double* const* q0_save, double* const* q1_save, double* const* q2_save,
                       double dt, void* stream);
+/* Per-block viscosity scale and time step for ensembles of independent
+ * instances: with mu0 non-NULL, block b uses mu0[b] in place of p->mu0; with
+ * dt non-NULL, block b advances by dt[b] and the dt argument of the step and
+ * stage calls is ignored.  NULL restores the plan-wide value.  The arrays are
+ * host arrays of nblocks values, copied; captured graphs are dropped. */
+int fj_plan_set_ensemble(fj_plan* plan, const double* mu0, const double* dt);
+/* fj_plan_step through a CUDA graph: the first call for a given (q_in, q_out,
+ * dt) captures the step's launches (copy, halo fill, boundary conditions and
+ * the three stages) on a private stream and instantiates them; later calls
+ * with the same pointers and dt replay the graph on `stream`.  The plan keeps
+ * the FJ_PLAN_MAX_GRAPHS most recently used graphs (a ping-pong loop uses
+ * two). */
+#define FJ_PLAN_MAX_GRAPHS 4
+int fj_plan_step_graph(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,
+                       void* stream);
 int fj_plan_destroy(fj_plan* plan);
 /* One TVD-RK3 stage (1..3) of every block of the plan, without the halo fill
  * (solver/step.py:45-53): out[b] from q[b] (stage input) and q0[b] (step start
@@ -266,6 +282,16 @@ int fj_step_vjp_saved_f64(fj_ctx* ctx, const fj_block* blocks, const double* con
                           double* const* lam_out, int nblocks, const fj_link* links, int nlinks,
                           const fj_bc* bcs, int nbcs, const fj_params* p, double dt,
                           double* dJ_dmu0, void* stream);
+/* fj_step_vjp_saved_f64 for an ensemble (fj_plan_set_ensemble): block b uses
+ * mu0[b] and dt[b] (host arrays of nblocks values; NULL = p->mu0 / dt), and
+ * dJ_dmu0 (device, nblocks doubles, or NULL) receives each block's own
+ * dJ/dmu0[b]. */
+int fj_step_vjp_ensemble_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* q1,
+                             const double* const* q2, const double* const* lam_in,
+                             double* const* lam_out, int nblocks, const fj_link* links,
+                             int nlinks, const fj_bc* bcs, int nbcs, const fj_params* p,
+                             double dt, const double* mu0, const double* dts, double* dJ_dmu0,
+                             void* stream);
 /* grad[b] = dJ/dq[b] for J = sum over interior cells of vol * 0.5 |rho u|^2 / rho
  * (the objective of fj_kinetic_energy_f64); ghost cells get 0. */
 int fj_kinetic_energy_grad_f64(fj_ctx* ctx, const fj_block* blocks, double* const* grad,

@@ -118,7 +118,7 @@ def test_trajectory_gradient_matches_finite_differences(cuda_device):
     rng = np.random.default_rng(11)
     eps = 1e-7
     gnorm = float(torch.linalg.vector_norm(g))
-    for _ in range(6):
+    for _ in range(16):
         d = torch.tensor(rng.standard_normal(tuple(q0.shape)), dtype=torch.float64, device="cuda")
         d = d / torch.linalg.vector_norm(d)
         fd = (_J(c, q0 + eps * d, nsteps, dt) - _J(c, q0 - eps * d, nsteps, dt)) / (2 * eps)
@@ -228,3 +228,80 @@ def test_mu_gradient_matches_autograd(cuda_device):
     dmu = torch.zeros(1, dtype=torch.float64, device="cuda")
     adjoint.step_vjp([dev(q) for q in qs], metrics, cfg, dt, [dev(l) for l in lam], dmu=dmu)
     assert abs(float(dmu) - ref) <= 1e-7 * abs(ref), (float(dmu), ref)
+
+
+def test_mach_gradient_matches_finite_differences(cuda_device):
+    """dJ/dM0 of the kinetic-energy objective: M0 enters the Taylor-Green
+    initial state and the viscosity mu0 = rho0 M0 / Re, so
+    dJ/dM0 = dJ/dq0 . dq0/dM0 + dJ/dmu0 * rho0 / Re, with dt held fixed (it is
+    computed once from the initial state).  Central differences regenerate
+    the case at M0 +- h with the same seed (the same noise draws); h keeps the
+    state perturbation near 1e-7 in L2, as in the trajectory test."""
+    n, M0, Re, nsteps = 12, 0.3, 800.0, 4
+
+    def case(m):
+        return cases.tgv(n=n, M0=m, Re=Re, noise=0.01, seed=2)
+
+    c = case(M0)
+    st = cases.to_state(c, "cuda:0")
+    dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], 1.4, 0.5, 2)
+    J, grads, dmu = adjoint.adjoint_kinetic_energy(st, c.cfg, dt, nsteps, checkpoint_every=2)
+    dq = torch.tensor(cases.tgv_dq0_dM0(c), device="cuda")
+    dJ = float(torch.sum(grads[0] * dq)) + dmu * 1.0 / Re
+    h = 1e-8 * M0
+
+    def J_of(m):
+        cm = case(m)
+        s = cases.to_state(cm, "cuda:0")
+        plan = StepPlan(s, cm.cfg)
+        for _ in range(nsteps):
+            s = step(s, cm.cfg, dt, plan=plan)
+        return diagnostics.kinetic_energy(s, 2)
+
+    fd = (J_of(M0 + h) - J_of(M0 - h)) / (2 * h)
+    assert abs(fd - dJ) <= 1e-6 * abs(dJ), (fd, dJ)
+
+
+def test_ensemble_matches_separate_instances(cuda_device):
+    """An ensemble plan (per-block mu0 and dt, all blocks per launch) steps each
+    instance exactly like a plan of that instance alone, and matches the
+    oracle; the per-instance adjoint (J_b, dJ_b/dq0_b, dJ_b/dmu0_b) matches the
+    single-instance adjoint."""
+    import dataclasses
+    ens = cases.ensemble(ninst=3, n=8, seed=5, precision="f64")
+    st = cases.to_state(ens, "cuda:0")
+    mets = [(m[1], m[2]) for m in ens.metrics]
+    dts = [NP.cfl_dt([q], [mt], 1.4, 0.5, 2) for q, mt in zip(ens.qs, mets)]
+    mu0s = ens.meta["mu0"]
+    plan = StepPlan(st, ens.cfg)
+    plan.set_ensemble(mu0s, dts)
+    qa = [b.q.clone() for b in st.blocks]
+    qb = [torch.empty_like(q) for q in qa]
+    nsteps = 3
+    for _ in range(nsteps):
+        plan.run(qa, qb, 123.0)  # the dt argument is ignored while per-block dt is set
+        qa, qb = qb, qa
+    for b in range(3):
+        cfg_b = dataclasses.replace(ens.cfg, gas=dataclasses.replace(ens.cfg.gas, mu0=mu0s[b]),
+                                    topology=(cases._self_periodic_topology(0),))
+        s_b = State(blocks=(st.blocks[b],), metrics=(st.metrics[b],))
+        p_b = StepPlan(s_b, cfg_b)
+        x = [st.blocks[b].q.clone()]
+        y = [torch.empty_like(x[0])]
+        ref = [ens.qs[b]]
+        for _ in range(nsteps):
+            p_b.run(x, y, dts[b])
+            x, y = y, x
+            ref = NP.step(ref, [mets[b]], cfg_b, dts[b])
+        assert torch.equal(x[0], qa[b]), b
+        assert rel_l2(host(qa[b]), ref[0]) <= 1e-12
+    Js, grads, dmus = adjoint.adjoint_kinetic_energy_ensemble(st, ens.cfg, nsteps, mu0s=mu0s, dts=dts,
+                                                              checkpoint_every=2)
+    for b in range(3):
+        cfg_b = dataclasses.replace(ens.cfg, gas=dataclasses.replace(ens.cfg.gas, mu0=mu0s[b]),
+                                    topology=(cases._self_periodic_topology(0),))
+        s_b = State(blocks=(st.blocks[b],), metrics=(st.metrics[b],))
+        J, g, dmu = adjoint.adjoint_kinetic_energy(s_b, cfg_b, dts[b], nsteps, checkpoint_every=2)
+        assert abs(J - Js[b]) <= 1e-14 * abs(J)
+        assert rel_l2(host(grads[b]), host(g[0])) <= 1e-13
+        assert abs(dmu - dmus[b]) <= 1e-12 * abs(dmu)

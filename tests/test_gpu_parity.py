@@ -354,3 +354,36 @@ def test_check_state_reports_injected_nan(cuda_device):
         diagnostics.check_state(st, 1.4)
     n, rmin, _ = diagnostics.check_state(st, 1.4, raise_on_error=False)
     assert n == 1 and rmin == -1.0
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_graph_step_matches_plain_step(cuda_device, precision):
+    """fj_plan_step_graph: ping-pong steps replayed from two captured graphs
+    give bit-identical states to fj_plan_step, and each replay counts the
+    graph's kernels."""
+    import dataclasses
+    from famrdp_jax_b200 import _capi
+    from famrdp_jax_b200.solver.step import StepPlan
+    c = cases.tree24(nblocks=5, lo=6, hi=12, seed=3)
+    cfg = dataclasses.replace(c.cfg, precision=precision)
+    st = state_from_case(c)
+    dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], cfg.gas.gamma, c.cfl, 2)
+    plan = StepPlan(st, cfg)
+    a = [b.q.clone() for b in st.blocks]
+    b_ = [torch.empty_like(q) for q in a]
+    ga = [q.clone() for q in a]
+    gb = [torch.empty_like(q) for q in a]
+    for n in range(5):
+        plan.run(a, b_, dt)
+        a, b_ = b_, a
+        before = _capi.launch_count()
+        plan.run(ga, gb, dt, graph=True)
+        per_step = _capi.launch_count() - before
+        ga, gb = gb, ga
+        for x, y in zip(a, ga):
+            assert torch.equal(x, y), n
+    assert per_step > 0
+    # a later replay of an already captured pointer set reuses its graph
+    before = _capi.launch_count()
+    plan.run(ga, gb, dt, graph=True)
+    assert _capi.launch_count() - before == per_step
