@@ -314,6 +314,12 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"))
     return out
 
 
+def _throughput(cells: int, steps: int, ms: float, ws: int) -> float:
+    """Whole-job Mcell-stages/s of ws replicas that each advanced `cells`
+    interior cells by `steps` steps (3 stages each) in `ms` (slowest rank)."""
+    return ws * cells * 3 * steps / (ms / 1e3) / 1e6
+
+
 def _max_over_ranks(x: float, ws: int, device) -> float:
     if ws == 1:
         return x
@@ -390,7 +396,7 @@ def run_ours(args):
         launches = _capi.launch_count(device) - n0
         barrier()
         ms = _max_over_ranks(e0.elapsed_time(e1), ws, device)
-        results[prec] = {"ms_per_step": ms / args.steps, "value": ws * cells * 3 * args.steps / (ms / 1e3) / 1e6,
+        results[prec] = {"ms_per_step": ms / args.steps, "value": _throughput(cells, args.steps, ms, ws),
                          "launches": launches,
                          "step_hbm_gbs": STEP_BYTES[prec] * case.padded_cells * ws / (ms / args.steps / 1e3) / 1e9}
         if prec == args.precision:
@@ -451,7 +457,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = _max_over_ranks(x0.elapsed_time(x1), ws, device)
     bytes_io = sum(h.numel() * 8 for h in host_in)
-    e2e = {"value": ws * cells * 3 * e2e_steps / (e2e_ms / 1e3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+    e2e = {"value": _throughput(cells, e2e_steps, e2e_ms, ws), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
            "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps}
 
     cpu = cpu_oracle_sample(case, dt) if (rank == 0 and not args.no_cpu) else None

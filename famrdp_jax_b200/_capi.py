@@ -92,6 +92,7 @@ SIGNATURES = {
     "fj_step_vjp_ensemble_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), ctypes.POINTER(_P),
                                       ctypes.POINTER(_P), ctypes.POINTER(_P), _I, ctypes.POINTER(FjLink), _I,
                                       ctypes.POINTER(FjBc), _I, ctypes.POINTER(FjParams), _D, _P, _P, _P, _P]),
+    "fj_residual_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), _I, _I, _D, _P, _P]),
     "fj_kinetic_energy_grad_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), _I, _I, _P]),
     "fj_rk_stage_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _D, _I, _P]),
     "fj_cons_to_prim_f64": (_I, [_P, _P, _I64, _D, _P]),

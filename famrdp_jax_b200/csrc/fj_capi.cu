@@ -31,6 +31,8 @@ int reduce_kinetic_energy(fj_ctx* ctx, const fj_block* blocks, int nblocks, int 
                           cudaStream_t st);
 int reduce_check_state(fj_ctx* ctx, const fj_block* blocks, int nblocks, double gamma,
                        int64_t* nonfinite, double* min_rho, double* min_p, cudaStream_t st);
+int reduce_residual(fj_ctx* ctx, const fj_block* blocks, const double* const* prev, int nblocks, int g,
+                    double dt, double* res5, cudaStream_t st);
 }  // namespace fj
 
 using namespace fj;
@@ -889,6 +891,12 @@ int fj_check_state_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, double 
   if (!ctx || !nonfinite_out || !min_rho_out || !min_p_out) return FJ_ERR_INVALID_ARGUMENT;
   return reduce_check_state(ctx, blocks, nblocks, gamma, nonfinite_out, min_rho_out, min_p_out,
                             S(stream));
+}
+
+int fj_residual_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* q_prev, int nblocks, int ghost,
+                    double dt, double* res_out, void* stream) {
+  if (!ctx || !res_out || ghost < 0) return FJ_ERR_INVALID_ARGUMENT;
+  return reduce_residual(ctx, blocks, q_prev, nblocks, ghost, dt, res_out, S(stream));
 }
 
 }  // extern "C"

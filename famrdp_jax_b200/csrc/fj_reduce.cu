@@ -1,6 +1,6 @@
 // fj_reduce.cu -- FP64 global reductions over all blocks: the CFL time step,
-// the kinetic-energy integral and the state check (finite values, minimum
-// density and pressure).  None of these exists in the reference, which takes
+// the kinetic-energy integral, the state check (finite values, minimum
+// density and pressure) and the per-component residual RMS of dq/dt.  None of these exists in the reference, which takes
 // dt as an argument (solver/step.py:18) and declares but never reads
 // Config.cfl / Config.nan_check (core/types.py:187-189).
 //
@@ -110,6 +110,31 @@ __global__ void k_ke_partial(const double* __restrict__ q, const double* __restr
   }
   s = block_reduce<0>(s, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// part layout per CTA: sum over interior cells of ((q - q_prev) / dt)^2 per
+// component (5 values)
+__global__ void k_res_partial(const double* __restrict__ q, const double* __restrict__ qp, Dims d,
+                              double inv_dt, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const int64_t N = (int64_t)d.ni * d.nj * d.nk;
+  const int64_t NI = (int64_t)(d.ni - 2 * d.g) * (d.nj - 2 * d.g) * (d.nk - 2 * d.g);
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < NI;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t c;
+    interior_cell(t, d, c);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double r = (q[v * N + c] - qp[v * N + c]) * inv_dt;
+      s[v] += r * r;
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    const double x = block_reduce<0>(s[v], sh);
+    if (threadIdx.x == 0) part[5 * blockIdx.x + v] = x;
+  }
 }
 
 // part layout per CTA: [nonfinite count, min rho, min p]
@@ -243,6 +268,35 @@ int reduce_check_state(fj_ctx* ctx, const fj_block* blocks, int nblocks, double 
   *min_p = h[2];
   if (h[0] > 0.0 || !(h[1] > 0.0) || !(h[2] > 0.0))
     return set_err(ctx, FJ_ERR_NONFINITE, "state has non-finite values or non-positive rho/p");
+  return FJ_OK;
+}
+
+int reduce_residual(fj_ctx* ctx, const fj_block* blocks, const double* const* prev, int nblocks, int g,
+                    double dt, double* res5, cudaStream_t st) {
+  int s = check_blocks(ctx, blocks, nblocks, g);
+  if (s != FJ_OK) return s;
+  if (!prev || !(dt > 0.0)) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bad previous states or dt");
+  for (int b = 0; b < nblocks; ++b)
+    if (!prev[b]) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "previous state is NULL");
+  s = ensure_red(ctx, sizeof(double) * (5 * (size_t)kRedBlocks * nblocks + 8));
+  if (s != FJ_OK) return s;
+  double* part = (double*)ctx->red;
+  double* out = part + 5 * (size_t)kRedBlocks * nblocks;
+  int64_t cells = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    Dims d{blocks[b].ni, blocks[b].nj, blocks[b].nk, g};
+    cells += (int64_t)(d.ni - 2 * g) * (d.nj - 2 * g) * (d.nk - 2 * g);
+    k_res_partial<<<kRedBlocks, kThreads, 0, st>>>(blocks[b].q, prev[b], d, 1.0 / dt,
+                                                   part + 5 * (size_t)b * kRedBlocks);
+  }
+  for (int v = 0; v < 5; ++v) k_fold<0><<<1, 1024, 0, st>>>(part, kRedBlocks * nblocks, 5, v, out + v);
+  ctx->launches += nblocks + 5;
+  double h[5];
+  s = cuda_status(ctx, cudaMemcpyAsync(h, out, 5 * sizeof(double), cudaMemcpyDeviceToHost, st), "residual copy");
+  if (s != FJ_OK) return s;
+  s = cuda_status(ctx, cudaStreamSynchronize(st), "residual sync");
+  if (s != FJ_OK) return s;
+  for (int v = 0; v < 5; ++v) res5[v] = sqrt(h[v] / (double)cells);
   return FJ_OK;
 }
 

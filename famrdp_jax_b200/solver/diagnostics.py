@@ -49,3 +49,16 @@ def check_state(state: State, gamma: float, *, raise_on_error: bool = True):
     if s != _capi.FJ_ERR_NONFINITE or raise_on_error:
         _capi.check(s, "fj_check_state_f64", c)
     return n.value, r.value, pm.value
+
+
+def residual(state: State, prev, dt: float, ghost: int = 2) -> list[float]:
+    """Per-component RMS over interior cells of (q - q_prev) / dt for the five
+    conserved variables, over all blocks (``prev``: the previous step's q per
+    block)."""
+    qs = [b.q for b in state.blocks]
+    dev = qs[0].device
+    c = _capi.ctx(dev)
+    out = (ctypes.c_double * 5)()
+    _capi.check(_capi.lib().fj_residual_f64(c, _topology.block_array(qs), _topology.ptr_array(list(prev)), len(qs),
+                                            int(ghost), float(dt), out, _capi.stream(dev)), "fj_residual_f64", c)
+    return list(out)

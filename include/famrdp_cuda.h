@@ -316,6 +316,12 @@ int fj_cfl_dt_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_par
 /* J = sum_interior vol * 0.5 * (q1^2 + q2^2 + q3^2) / q0 over all blocks. */
 int fj_kinetic_energy_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, int ghost,
                           double* out, void* stream);
+/* Residual of one step for logging: res_out[v] = sqrt(mean over interior
+ * cells of ((blocks[b].q - q_prev[b]) / dt)^2) for each conserved component v
+ * (rho, rho u, rho v, rho w, rho E), over all blocks.  Synchronises the
+ * stream.  The reference plans such a log (one line per step) but has none. */
+int fj_residual_f64(fj_ctx* ctx, const fj_block* blocks, const double* const* q_prev, int nblocks,
+                    int ghost, double dt, double* res_out, void* stream);
 /* Counts non-finite values of q over all padded cells of all blocks and the
  * minimum density and pressure; returns FJ_ERR_NONFINITE when count > 0 or
  * min rho <= 0 or min p <= 0. */

@@ -90,8 +90,8 @@ def test_eos_roundtrip_and_parity(cuda_device):
 
 def test_limiters_and_muscl(cuda_device):
     np.testing.assert_allclose(host(minmod(dev([1.0, -1.0]), dev([-1.0, 1.0]))), 0.0, atol=1e-15)
-    assert float(host(minmod(dev(2.0), dev(5.0)))) == 2.0
-    assert float(host(minmod(dev(-3.0), dev(-7.0)))) == -3.0
+    assert host(minmod(dev(2.0), dev(5.0))).item() == 2.0
+    assert host(minmod(dev(-3.0), dev(-7.0))).item() == -3.0
     rng = np.random.default_rng(5)
     a, b = rng.standard_normal(1000), rng.standard_normal(1000)
     np.testing.assert_allclose(host(vanleer(dev(a), dev(b))), NP.vanleer(a, b), rtol=1e-14)
@@ -387,3 +387,58 @@ def test_graph_step_matches_plain_step(cuda_device, precision):
     before = _capi.launch_count()
     plan.run(ga, gb, dt, graph=True)
     assert _capi.launch_count() - before == per_step
+
+
+def test_step_on_parsed_gridgen_topology(cuda_device, pipeline):
+    """Two blocks joined through a parsed GridGen topology (a j-interface pair
+    with orientation 0 plus wall, symmetry and farfield faces), sized as the
+    file declares (5 x 5 x 3 nodes + 2 ghosts per side): FP64 steps against
+    the oracle."""
+    from pathlib import Path
+    from famrdp_jax_b200.mesh.io_top import parse_topology
+    tops = tuple(parse_topology(Path(__file__).parent / "golden" / "mini.inp"))
+    blocks = [random_block((9, 9, 7), 20 + b, noise=0.02) for b in range(2)]
+    qs = [b[0] for b in blocks]
+    mets = [(b[1], b[2]) for b in blocks]
+    q_inf = list(qs[0][:, 4, 4, 3])
+    cfg = _cfg(topology=tops, bc_params={f: {"q_inf": q_inf} for f in Face})
+    case = cases.Case(name="gridgen2", qs=qs, metrics=[(b[2], b[1], b[2]) for b in blocks], cfg=cfg, cfl=0.5,
+                      steps=3)
+    dt = 0.5 * NP.cfl_dt(qs, mets, cfg.gas.gamma, 0.5, 2)
+    errs, _ = _run_steps(case, 3, dt)
+    assert max(errs) <= 1e-12, errs
+
+
+def test_residual_and_monitored_run(cuda_device, tmp_path):
+    """fj_residual_f64 against the NumPy residual of the oracle's step, and the
+    monitored loop: same states as plain steps, one log row per step, and a
+    planted NaN stops it with FloatingPointError and dumps both states."""
+    from famrdp_jax_b200.solver.run import run, write_residual_log
+    c = cases.tgv(n=12, M0=0.3, Re=400.0, noise=0.01, seed=1)
+    st = state_from_case(c)
+    mets = [(m[1], m[2]) for m in c.metrics]
+    dt = NP.cfl_dt(c.qs, mets, c.cfg.gas.gamma, c.cfl, 2)
+    q1 = NP.step(c.qs, mets, c.cfg, dt)
+    g = 2
+    inner = (slice(None),) + (slice(g, -g),) * 3
+    ref = np.sqrt(np.mean(((q1[0] - c.qs[0]) / dt)[inner] ** 2, axis=(1, 2, 3)))
+    st1 = step(st, c.cfg, dt)
+    got = diagnostics.residual(st1, [b.q for b in st.blocks], dt, g)
+    np.testing.assert_allclose(got, ref, rtol=1e-9)
+    final, log = run(st, c.cfg, dt, 4)
+    ref_st = st
+    for _ in range(4):
+        ref_st = step(ref_st, c.cfg, dt)
+    assert torch.equal(final.blocks[0].q, ref_st.blocks[0].q) and final.step == 4
+    assert [r[0] for r in log.rows] == [1, 2, 3, 4]
+    np.testing.assert_allclose(log.rows[0][2], got, rtol=1e-14)
+    write_residual_log(tmp_path / "res.txt", log)
+    assert len((tmp_path / "res.txt").read_text().splitlines()) == 5
+    bad = st.blocks[0].q.clone()
+    bad[0, 5, 5, 5] = float("nan")
+    import dataclasses
+    st_bad = dataclasses.replace(st, blocks=(dataclasses.replace(st.blocks[0], q=bad),))
+    cfg = dataclasses.replace(c.cfg, nan_check=True)
+    with pytest.raises(FloatingPointError, match="step 1"):
+        run(st_bad, cfg, dt, 3, dump_dir=tmp_path / "dumps")
+    assert sorted(p.name for p in (tmp_path / "dumps").iterdir()) == ["step0000000_good.pt", "step0000001_bad.pt"]
