@@ -314,6 +314,48 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"))
     return out
 
 
+def error_table(case, dt, device, marks=(1, 10, 100), ens=None):
+    """FP32-flux against FP64, both on this GPU from the same start, in
+    lockstep: relative L2 per conserved variable over the full padded state
+    and over the interior at the marked steps.  The FP64 GPU path matches the
+    CPU oracle to <= 1e-12 per step (the parity tests), so it stands in for the
+    oracle over runs the oracle cannot finish here."""
+    import torch
+
+    from famrdp_jax_b200 import cases
+    from famrdp_jax_b200.solver.step import StepPlan
+
+    runs = {}
+    for prec in ("f64", "f32"):
+        cfg = dataclasses.replace(case.cfg, precision=prec)
+        st = cases.to_state(case, device)
+        plan = StepPlan(st, cfg)
+        if ens:
+            plan.set_ensemble(*ens)
+        runs[prec] = [plan, [b.q.clone() for b in st.blocks], [torch.empty_like(b.q) for b in st.blocks]]
+    g = case.cfg.ghost
+    names = ["rho", "rhou", "rhov", "rhow", "rhoE"]
+    table = {}
+    for n in range(1, max(marks) + 1):
+        for prec, r in runs.items():
+            r[0].run(r[1], r[2], dt, graph=True)
+            r[1], r[2] = r[2], r[1]
+        if n in marks:
+            row = {}
+            for part in ("full", "interior"):
+                for v, nm in enumerate(names):
+                    num = den = 0.0
+                    for a, b in zip(runs["f32"][1], runs["f64"][1]):
+                        x, y = a[v], b[v]
+                        if part == "interior":
+                            x, y = x[g:-g, g:-g, g:-g], y[g:-g, g:-g, g:-g]
+                        num += float(torch.sum((x - y) ** 2))
+                        den += float(torch.sum(y ** 2))
+                    row[f"{part}_{nm}"] = (num / den) ** 0.5
+            table[str(n)] = row
+    return {"reference": "FP64 path on the GPU (<= 1e-12 per step against the oracle)", "rel_l2": table}
+
+
 def _throughput(cells: int, steps: int, ms: float, ws: int) -> float:
     """Whole-job Mcell-stages/s of ws replicas that each advanced `cells`
     interior cells by `steps` steps (3 stages each) in `ms` (slowest rank)."""
@@ -461,6 +503,8 @@ def run_ours(args):
            "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps}
 
     cpu = cpu_oracle_sample(case, dt) if (rank == 0 and not args.no_cpu) else None
+    marks = (1, 10, 100, 200) if args.workload == "tree24" else (1, 10, 100)
+    errs = error_table(case, dt, device, marks, ens) if (rank == 0 and not args.no_error_table) else None
     adj = (adjoint_timing(device, args.adjoint_n, args.adjoint_steps, args.adjoint_every)
            if (rank == 0 and not args.no_adjoint) else None)
     if rank == 0:
@@ -474,7 +518,7 @@ def run_ours(args):
                 "variants": {p: results[p] for p in order} | {
                     "f32_vs_f64_rel_l2": err_f32,
                     "f32_vs_f64_note": f"whole state after {warm + args.steps} steps from the same start"},
-                "adjoint": adj,
+                "adjoint": adj, "fp32_error_table": errs,
                 "dt": dt if not ens else {"per_instance": True, "min": min(ens[1]), "max": max(ens[1])}}
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -495,6 +539,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
+    ap.add_argument("--no-error-table", action="store_true", help="skip the FP32-vs-FP64 error table")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint/forward timing (one JSON line)")
     ap.add_argument("--adjoint-n", type=int, default=96)

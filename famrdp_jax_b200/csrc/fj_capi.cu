@@ -2,6 +2,7 @@
 // (declared in include/famrdp_cuda.h).  Validation, scratch sizing and
 // dispatch only; the kernels live in the other translation units.
 #include <algorithm>
+#include <cmath>
 #include <new>
 #include <vector>
 
@@ -180,7 +181,8 @@ size_t step_layout(const fj_ctx* ctx, const fj_block* blocks, int nblocks, const
 int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* const* q1s,
               double* const* q2s, double* const* q_out, int nblocks, const fj_link* links, int nlinks,
               const fj_bc* bcs, int nbcs, const fj_params* p, double dt, void* const* kmet, void* tail,
-              size_t tail_b, cudaStream_t st, const double* mu0_b = nullptr, const double* dt_b = nullptr) {
+              size_t tail_b, cudaStream_t st, const double* mu0_b = nullptr, const double* dt_b = nullptr,
+              double p_ref = 0.0) {
   std::vector<fj_block> out(blocks, blocks + nblocks);
   int s;
   for (int b = 0; b < nblocks; ++b) {
@@ -207,7 +209,8 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
                           B.nj, B.nk, mu0_b ? mu0_b[b] : p->mu0, dt_b ? dt_b[b] : dt);
     }
     split_assign_scratch(p->precision, sb.data(), nblocks, tail);
-    const Phys ph = make_phys(p);
+    Phys ph = make_phys(p);
+    ph.p_ref = p_ref;
     // the assembly of stages 1 and 2 also writes the next stage's primitives
     s = split_stage(ctx, sb.data(), nblocks, ph, flags, 1, p->precision, st, false, true);
     if (s != FJ_OK) return s;
@@ -479,7 +482,8 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
         fj_plan_destroy(pl);
         return set_err(ctx, FJ_ERR_NO_MEMORY, "plan metric copy allocation failed");
       }
-      s = split ? split_metric_records(blocks[b].kxyz, pl->kmet[b], N, p->precision, nullptr)
+      s = split ? split_metric_records(blocks[b].kxyz, pl->kmet[b], blocks[b].ni, blocks[b].nj, blocks[b].nk,
+                                       p->precision, nullptr)
                 : convert_f64_f32(blocks[b].kxyz, (float*)pl->kmet[b], 9 * N, nullptr);
       if (s != FJ_OK) {
         fj_plan_destroy(pl);
@@ -490,6 +494,12 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
     if (e != cudaSuccess) {
       fj_plan_destroy(pl);
       return cuda_status(ctx, e, "plan metric conversion");
+    }
+    // the FP32-flux split path offsets the momentum fluxes' pressure by the
+    // mean pressure of the state the plan is created with
+    if (split) {
+      s = mean_pressure(blocks, nblocks, p->gamma - 1.0, &pl->p_ref);
+      if (s != FJ_OK || !std::isfinite(pl->p_ref)) pl->p_ref = 0.0;
     }
   }
   *out = pl;
@@ -520,7 +530,8 @@ static int plan_step_impl(fj_plan* pl, double* const* q_in, double* const* q_out
   int s = step_body(ctx, in.data(), q0_save ? q0_save : q_out, q1s.data(), q2s.data(), q_out, nb,
                     pl->links.data(), (int)pl->links.size(), pl->bcs.data(), (int)pl->bcs.size(), &pl->p, dt,
                     pl->kmet.empty() ? nullptr : pl->kmet.data(), tail, pl->halo_bytes, S(stream),
-                    pl->mu0_b.empty() ? nullptr : pl->mu0_b.data(), pl->dt_b.empty() ? nullptr : pl->dt_b.data());
+                    pl->mu0_b.empty() ? nullptr : pl->mu0_b.data(), pl->dt_b.empty() ? nullptr : pl->dt_b.data(),
+                    pl->p_ref);
   ctx->pipeline = saved;
   return s;
 }
@@ -635,7 +646,9 @@ int fj_plan_stage(fj_plan* pl, double* const* q, double* const* q0, double* cons
                           pl->mu0_b.empty() ? pl->p.mu0 : pl->mu0_b[b], pl->dt_b.empty() ? dt : pl->dt_b[b]);
     }
     split_assign_scratch(pl->p.precision, sb.data(), nb, tail);
-    s = split_stage(ctx, sb.data(), nb, make_phys(&pl->p), flags, stage, pl->p.precision, S(stream));
+    Phys ph = make_phys(&pl->p);
+    ph.p_ref = pl->p_ref;
+    s = split_stage(ctx, sb.data(), nb, ph, flags, stage, pl->p.precision, S(stream));
   } else {
     for (int b = 0; b < nb && s == FJ_OK; ++b) {
       const fj_block& B = pl->blocks[b];

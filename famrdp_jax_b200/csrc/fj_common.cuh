@@ -48,6 +48,7 @@ struct fj_plan {
   size_t stage_bytes = 0, halo_bytes = 0;  // halo_bytes: size of the tail
   int pipeline = 0;
   std::vector<double> mu0_b, dt_b;        // per-block overrides (ensembles), empty = none
+  double p_ref = 0.0;                     // FP32-flux split path: momentum-flux pressure offset
   cudaStream_t capture_stream = nullptr;  // private stream for graph capture
   std::vector<fj_graph_entry> graphs;     // most recently used last
 };
@@ -142,6 +143,9 @@ struct Phys {
   // derived once on the host: 1/(gamma-1), 1/T0, T0+Ts, cp/Pr
   double inv_gm1, inv_T0, sfac, kap_fac;
   int limiter, visc_law;
+  // FP32-flux split path with metric records only: the pressure offset of the
+  // momentum fluxes (roe_prim), added back in FP64 in the assembly; 0 elsewhere
+  double p_ref = 0.0;
 };
 
 inline Phys make_phys(const fj_params* p) {

@@ -257,17 +257,29 @@ __device__ __forceinline__ void muscl2_fast(T c0, T c1, T c2, T c3, int limiter,
 
 // Roe flux (flux/roe.py:21-85) of the primitive face states L, R along the unit
 // normal n; inv_gm1 = 1/(gamma-1).
-template <typename T>
+//
+// POFF (the FP32-flux split path): the states carry the pressure OFFSET
+// p' = p - p_ref instead of p.  The energies and enthalpies add p_ref back as
+// constants, energy differences use p' differences, and the momentum
+// components leave out the constant part p_ref n of their pressure term
+// (p n = p' n + p_ref n), which the caller adds in FP64.  In FP32 that keeps
+// the rounding of the large, nearly uniform pressure out of the small
+// momentum fluxes and pressure jumps.  The two forms are equal in exact
+// arithmetic; POFF = false is the reference arrangement.
+template <typename T, bool POFF = false>
 __device__ __forceinline__ void roe_prim(const Prim<T>& L, const Prim<T>& R, T n0, T n1, T n2,
-                                         T gm1, T inv_gm1, T eps_entropy, T F[5]) {
+                                         T gm1, T inv_gm1, T eps_entropy, T F[5], T p_ref = T(0)) {
   using M = FastMath<T>;
   const T rhoL = fj_max(L.rho, Tiny<T>::rho()), rhoR = fj_max(R.rho, Tiny<T>::rho());
   const T keL = T(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
   const T keR = T(0.5) * (R.u * R.u + R.v * R.v + R.w * R.w);
-  const T EL = L.p * inv_gm1 + L.rho * keL;  // conserved energies (eos.py:8)
-  const T ER = R.p * inv_gm1 + R.rho * keR;
-  const T HL = (EL + L.p) * M::rcp(rhoL);
-  const T HR = (ER + R.p) * M::rcp(rhoR);
+  // conserved energies (eos.py:8) and enthalpies
+  const T eL = L.p * inv_gm1 + L.rho * keL, eR = R.p * inv_gm1 + R.rho * keR;
+  const T Ec = POFF ? p_ref * inv_gm1 : T(0), Hc = POFF ? p_ref * (inv_gm1 + T(1)) : T(0);
+  const T EL = POFF ? eL + Ec : eL;
+  const T ER = POFF ? eR + Ec : eR;
+  const T HL = (POFF ? (eL + L.p) + Hc : EL + L.p) * M::rcp(rhoL);
+  const T HR = (POFF ? (eR + R.p) + Hc : ER + R.p) * M::rcp(rhoR);
   const T sqL = M::sqrt_pos(rhoL), sqR = M::sqrt_pos(rhoR);
   const T inv_ss = M::rcp(fj_max(sqL + sqR, Tiny<T>::ss()));
   const T wl = sqL * inv_ss, wr = sqR * inv_ss;
@@ -293,7 +305,7 @@ __device__ __forceinline__ void roe_prim(const Prim<T>& L, const Prim<T>& R, T n
   const T d1 = R.rho * R.u - L.rho * L.u;
   const T d2 = R.rho * R.v - L.rho * L.v;
   const T d3 = R.rho * R.w - L.rho * L.w;
-  const T d4 = ER - EL;
+  const T d4 = POFF ? eR - eL : ER - EL;
   const T dp = gm1 * (d4 - u_h * d1 - v_h * d2 - w_h * d3 + T(0.5) * q2 * d0);
   const T dun = (d1 * n0 + d2 * n1 + d3 * n2) - un_h * d0;
   const T rcd = rho_h * c_h * dun;
@@ -312,11 +324,12 @@ __device__ __forceinline__ void roe_prim(const Prim<T>& L, const Prim<T>& R, T n
   const T unR = R.u * n0 + R.v * n1 + R.w * n2;
   const T mL = rhoL * unL, mR = rhoR * unR;
   F[0] = T(0.5) * (mL + mR) - T(0.5) * (s1 + s5 + al2 * a23);
-  F[1] = T(0.5) * ((mL * L.u + L.p * n0) + (mR * R.u + R.p * n0)) -
+  const T pL = L.p, pR = R.p;  // p' with POFF: the p_ref n part is the caller's
+  F[1] = T(0.5) * ((mL * L.u + pL * n0) + (mR * R.u + pR * n0)) -
          T(0.5) * (s1 * (u_h - cn0) + s5 * (u_h + cn0) + al2 * (a23 * u_h + t1));
-  F[2] = T(0.5) * ((mL * L.v + L.p * n1) + (mR * R.v + R.p * n1)) -
+  F[2] = T(0.5) * ((mL * L.v + pL * n1) + (mR * R.v + pR * n1)) -
          T(0.5) * (s1 * (v_h - cn1) + s5 * (v_h + cn1) + al2 * (a23 * v_h + t2));
-  F[3] = T(0.5) * ((mL * L.w + L.p * n2) + (mR * R.w + R.p * n2)) -
+  F[3] = T(0.5) * ((mL * L.w + pL * n2) + (mR * R.w + pR * n2)) -
          T(0.5) * (s1 * (w_h - cn2) + s5 * (w_h + cn2) + al2 * (a23 * w_h + t3));
   F[4] = T(0.5) * (mL * HL + mR * HR) -
          T(0.5) * (s1 * (H_h - cun) + s5 * (H_h + cun) + al2 * (a23 * (T(0.5) * q2) + t4));
@@ -325,10 +338,10 @@ __device__ __forceinline__ void roe_prim(const Prim<T>& L, const Prim<T>& R, T n
 // One inviscid face (rhs/invscd.py:62-100) in the reformulated arithmetic:
 // MUSCL on the four cells' primitives, face normal from the two adjacent
 // cells' kxyz rows, Roe, times |n|.
-template <typename T>
+template <typename T, bool POFF = false>
 __device__ __forceinline__ void invscd_face_fast(const Prim<T> c[4], T kl0, T kl1, T kl2, T kr0,
                                                  T kr1, T kr2, T gm1, T inv_gm1, T eps_entropy,
-                                                 int limiter, T F[5]) {
+                                                 int limiter, T F[5], T p_ref = T(0)) {
   Prim<T> L, R;
   muscl2_fast(c[0].rho, c[1].rho, c[2].rho, c[3].rho, limiter, L.rho, R.rho);
   muscl2_fast(c[0].u, c[1].u, c[2].u, c[3].u, limiter, L.u, R.u);
@@ -338,7 +351,7 @@ __device__ __forceinline__ void invscd_face_fast(const Prim<T> c[4], T kl0, T kl
   const T nf0 = T(0.5) * (kl0 + kr0), nf1 = T(0.5) * (kl1 + kr1), nf2 = T(0.5) * (kl2 + kr2);
   const T nmag = FastMath<T>::sqrt_nn(nf0 * nf0 + nf1 * nf1 + nf2 * nf2) + Tiny<T>::nmag();
   const T inv = FastMath<T>::rcp(nmag);
-  roe_prim(L, R, nf0 * inv, nf1 * inv, nf2 * inv, gm1, inv_gm1, eps_entropy, F);
+  roe_prim<T, POFF>(L, R, nf0 * inv, nf1 * inv, nf2 * inv, gm1, inv_gm1, eps_entropy, F, p_ref);
 #pragma unroll
   for (int v = 0; v < 5; ++v) F[v] = F[v] * nmag;
 }

@@ -34,8 +34,11 @@ struct SplitBlock {
 };
 
 // Metric records (kRecK values of the flux type per cell) from the caller's
-// field-major FP64 kxyz (3, 3, N).
-int split_metric_records(const double* kxyz, void* out, int64_t N, int precision, cudaStream_t st);
+// field-major FP64 kxyz (3, 3, ni, nj, nk): the nine kxyz[l][m] and, in FP32
+// records, the three face-normal difference sums the pressure offset uses.
+int split_metric_records(const double* kxyz, void* out, int ni, int nj, int nk, int precision, cudaStream_t st);
+// Mean pressure over all padded cells of the blocks (synchronous).
+int mean_pressure(const fj_block* blocks, int nblocks, double gm1, double* out);
 // Bytes of one block's metric records.
 size_t split_metric_record_bytes(int precision, int64_t N);
 // Scratch bytes of the intermediates of `cells` padded cells in total.

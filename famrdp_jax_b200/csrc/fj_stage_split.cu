@@ -156,12 +156,17 @@ __device__ __forceinline__ Cell6<T> load_cell(const T* __restrict__ P, int32_t c
 // The nine kxyz[l][m] of cell c, from the record copy (K_AOS) or from the
 // caller's field-major FP64 array.
 template <typename T, bool K_AOS>
-__device__ __forceinline__ void metric9(const SplitBlock& B, int32_t N, int32_t c, T kk[9]) {
+__device__ __forceinline__ void metric9(const SplitBlock& B, int32_t N, int32_t c, T kk[9], T* gcl = nullptr) {
   if constexpr (K_AOS) {
     T x[kRecK<T>];
     ld_rec<T, kRecK<T>>((const T*)B.kaos + (size_t)c * kRecK<T>, x);
 #pragma unroll
     for (int lm = 0; lm < 9; ++lm) kk[lm] = x[lm];
+    if (gcl) {
+      gcl[0] = x[9];
+      gcl[1] = x[10];
+      gcl[2] = x[11];
+    }
   } else {
 #pragma unroll
     for (int lm = 0; lm < 9; ++lm) kk[lm] = (T)__ldg(B.kxyz + (size_t)lm * N + c);
@@ -199,9 +204,10 @@ __device__ __forceinline__ void prims_of(const double q[5], double gm1, double R
   out[5] = r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300;
 }
 
+// p_ref != 0 (the record path): the pressure slot holds p - p_ref.
 template <typename T>
 __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, const double gm1,
-                                                              const double R) {
+                                                              const double R, const double p_ref) {
   const int b = find_block(tab, blockIdx.x);
   const SplitBlock& B = tab.b[b].blk;
   const int32_t N = B.ni * B.nj * B.nk;
@@ -211,20 +217,21 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, 
   const double qc[5] = {q[0], q[N], q[2 * (size_t)N], q[3 * (size_t)N], q[4 * (size_t)N]};
   double pv[6];
   prims_of(qc, gm1, R, pv);
-  const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)pv[4], (T)pv[5], T(0), T(0)};
+  const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)(pv[4] - p_ref), (T)pv[5], T(0), T(0)};
   st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
 }
 
 // Roe face c | c+e_a from the primitives of c-e_a, c, c+e_a, c+2e_a and the
 // kxyz rows of c and c+e_a (rhs/invscd.py:62-100).
-template <typename T>
+// POFF: the cells carry p' = p - p_ref (see roe_prim).
+template <typename T, bool POFF>
 __device__ __forceinline__ void face_from_cells(const Cell6<T>& a0, const Cell6<T>& a1, const Cell6<T>& a2,
                                                 const Cell6<T>& a3, const T kl[3], const T kr[3],
-                                                const Phys& ph, T* F) {
+                                                const Phys& ph, T* F, T p_ref) {
   Prim<T> cell[4] = {{a0.r, a0.u, a0.v, a0.w, a0.p}, {a1.r, a1.u, a1.v, a1.w, a1.p},
                      {a2.r, a2.u, a2.v, a2.w, a2.p}, {a3.r, a3.u, a3.v, a3.w, a3.p}};
-  invscd_face_fast<T>(cell, kl[0], kl[1], kl[2], kr[0], kr[1], kr[2], (T)ph.gm1, (T)ph.inv_gm1,
-                      (T)ph.eps_entropy, ph.limiter, F);
+  invscd_face_fast<T, POFF>(cell, kl[0], kl[1], kl[2], kr[0], kr[1], kr[2], (T)ph.gm1, (T)ph.inv_gm1,
+                            (T)ph.eps_entropy, ph.limiter, F, p_ref);
 }
 
 template <typename T, bool K_AOS>
@@ -296,20 +303,23 @@ __global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::fluxes) k_split_fl
 #pragma unroll
     for (int v = 0; v < kRecF; ++v) Fr[v] = T(0);
     T kn[3];
+    // with metric records the primitives carry p' = p - p_ref and the FP64
+    // correction of the momentum fluxes is in the records
+    const T p_ref = K_AOS ? (T)ph.p_ref : T(0);
     if (x.i >= 1 && x.i <= x.ni - 3) {
       const Cell6<T> I2 = load_cell<T>(P, c + 2 * si);
       metric_row<T, K_AOS>(B, N, 0, c + si, kn);
-      face_from_cells<T>(Im, C0, Ip, I2, kk, kn, ph, Fr);
+      face_from_cells<T, K_AOS>(Im, C0, Ip, I2, kk, kn, ph, Fr, p_ref);
     }
     if (x.j >= 1 && x.j <= x.nj - 3) {
       const Cell6<T> J2 = load_cell<T>(P, c + 2 * sj);
       metric_row<T, K_AOS>(B, N, 1, c + sj, kn);
-      face_from_cells<T>(Jm, C0, Jp, J2, kk + 3, kn, ph, Fr + 5);
+      face_from_cells<T, K_AOS>(Jm, C0, Jp, J2, kk + 3, kn, ph, Fr + 5, p_ref);
     }
     if (x.k >= 1 && x.k <= x.nk - 3) {
       const Cell6<T> K2 = load_cell<T>(P, c + 2);
       metric_row<T, K_AOS>(B, N, 2, c + 1, kn);
-      face_from_cells<T>(Km, C0, Kp, K2, kk + 6, kn, ph, Fr + 10);
+      face_from_cells<T, K_AOS>(Km, C0, Kp, K2, kk + 6, kn, ph, Fr + 10, p_ref);
     }
     st_rec<T, kRecF>((T*)B.F + (size_t)c * kRecF, Fr);
   }
@@ -323,7 +333,8 @@ __global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::assemble) k_split_
                                                                                        const int stage,
                                                                                        const int next_prims,
                                                                                        const double gm1,
-                                                                                       const double R) {
+                                                                                       const double R,
+                                                                                       const double ph_p_ref) {
   const int b = find_block(tab, blockIdx.x);
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
@@ -342,6 +353,15 @@ __global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::assemble) k_split_
       const double ivd = 1.0 / (B.vol[c] + 1e-300);
       T Fc[kRecF];
       ld_rec<T, kRecF>(F + (size_t)c * kRecF, Fc);
+      // sum over the active axes of the face-normal differences, from the
+      // FP64 metrics (the p_ref n part the face fluxes left out)
+      double pg[3] = {0.0, 0.0, 0.0};
+      if constexpr (K_AOS) {
+        const T* rec = (const T*)B.kaos + (size_t)c * kRecK<T>;
+        pg[0] = ph_p_ref * (double)rec[9];
+        pg[1] = ph_p_ref * (double)rec[10];
+        pg[2] = ph_p_ref * (double)rec[11];
+      }
       T Fm[3][5];
 #pragma unroll
       for (int a = 0; a < 3; ++a)
@@ -361,6 +381,7 @@ __global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::assemble) k_split_
           for (int a = 0; a < 3; ++a)
             if (on[a]) s += Fc[5 * a + v] - Fm[a][v];
           dsum = (double)s;
+          if (v >= 1 && v <= 3) dsum += pg[v - 1];
         }
         r[v] = -dsum * ivd;
       }
@@ -413,7 +434,7 @@ __global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::assemble) k_split_
     if (next_prims) {
       double pv[6];
       prims_of(qn, gm1, R, pv);
-      const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)pv[4], (T)pv[5], T(0), T(0)};
+      const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)(pv[4] - ph_p_ref), (T)pv[5], T(0), T(0)};
       st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
     }
   }
@@ -692,8 +713,14 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table ta
 
 }  // namespace fm
 
+// Record of cell c: the nine kxyz[l][m], then (FP32 records) the three
+// gcl[m] = sum over the axes a with c_a in [2, n_a-3] of
+// 0.5 (kxyz[a][m](c+e_a) - kxyz[a][m](c-e_a)), evaluated in FP64: the sum of
+// the face-normal differences n_a(c) - n_a(c-e_a) the assembly multiplies by
+// p_ref (rhs/invscd.py:87-89, 119-131).
 template <typename T>
-__global__ void k_metric_records(const double* __restrict__ kxyz, T* __restrict__ out, int64_t N) {
+__global__ void k_metric_records(const double* __restrict__ kxyz, T* __restrict__ out, int ni, int nj, int nk) {
+  const int64_t N = (int64_t)ni * nj * nk;
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= N) return;
   T rec[kRecK<T>];
@@ -701,7 +728,32 @@ __global__ void k_metric_records(const double* __restrict__ kxyz, T* __restrict_
   for (int lm = 0; lm < 9; ++lm) rec[lm] = (T)kxyz[lm * N + c];
 #pragma unroll
   for (int lm = 9; lm < kRecK<T>; ++lm) rec[lm] = T(0);
+  if (kRecK<T> >= 12) {
+    const int k = (int)(c % nk), j = (int)((c / nk) % nj), i = (int)(c / ((int64_t)nk * nj));
+    const int idx[3] = {i, j, k}, n[3] = {ni, nj, nk};
+    const int64_t st[3] = {(int64_t)nj * nk, nk, 1};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      double g = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (idx[a] >= 2 && idx[a] <= n[a] - 3)
+          g += 0.5 * (kxyz[(3 * a + m) * N + c + st[a]] - kxyz[(3 * a + m) * N + c - st[a]]);
+      if (9 + m < kRecK<T>) rec[9 + m] = (T)g;
+    }
+  }
   st_rec<T, kRecK<T>>(out + c * kRecK<T>, rec);
+}
+
+__global__ void k_pressure_sum(const double* __restrict__ q, int64_t N, double gm1, double* __restrict__ acc) {
+  double s = 0.0;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N; c += (int64_t)gridDim.x * blockDim.x) {
+    const double r = q[c], u = q[N + c] / r, v = q[2 * N + c] / r, w = q[3 * N + c] / r;
+    s += gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
 }
 
 template <typename T, bool K_AOS>
@@ -713,9 +765,10 @@ int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage,
     fm::k_fm_fluxes<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
     fm::k_fm_assemble<double><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R);
   } else {
-    if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R);
+    if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, K_AOS ? ph.p_ref : 0.0);
     k_split_fluxes<T, K_AOS><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
-    k_split_assemble<T, K_AOS><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R);
+    k_split_assemble<T, K_AOS><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
+                                                                 K_AOS ? ph.p_ref : 0.0);
   }
   return prims_ready ? 2 : 3;
 }
@@ -754,14 +807,36 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
 
 }  // namespace
 
-int split_metric_records(const double* kxyz, void* out, int64_t N, int precision, cudaStream_t st) {
+int split_metric_records(const double* kxyz, void* out, int ni, int nj, int nk, int precision, cudaStream_t st) {
+  const int64_t N = (int64_t)ni * nj * nk;
   if (N <= 0) return FJ_OK;
   const int grid = (int)((N + 255) / 256);
   if (precision == FJ_PREC_F32FLUX)
-    k_metric_records<float><<<grid, 256, 0, st>>>(kxyz, (float*)out, N);
+    k_metric_records<float><<<grid, 256, 0, st>>>(kxyz, (float*)out, ni, nj, nk);
   else
-    k_metric_records<double><<<grid, 256, 0, st>>>(kxyz, (double*)out, N);
+    k_metric_records<double><<<grid, 256, 0, st>>>(kxyz, (double*)out, ni, nj, nk);
   return cudaGetLastError() == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
+}
+
+int mean_pressure(const fj_block* blocks, int nblocks, double gm1, double* out) {
+  double* acc = nullptr;
+  if (cudaMalloc(&acc, sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return FJ_ERR_NO_MEMORY;
+  }
+  cudaMemsetAsync(acc, 0, sizeof(double), nullptr);
+  int64_t cells = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    const int64_t N = (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
+    cells += N;
+    k_pressure_sum<<<592, 256, 0, nullptr>>>(blocks[b].q, N, gm1, acc);
+  }
+  double h = 0.0;
+  const cudaError_t e = cudaMemcpy(&h, acc, sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(acc);
+  if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return FJ_ERR_CUDA;
+  *out = cells > 0 ? h / (double)cells : 0.0;
+  return FJ_OK;
 }
 
 size_t split_metric_record_bytes(int precision, int64_t N) {
