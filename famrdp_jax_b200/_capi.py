@@ -75,6 +75,8 @@ SIGNATURES = {
                             ctypes.POINTER(FjParams), ctypes.POINTER(_P)]),
     "fj_plan_step": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_set_ensemble": (_I, [_P, _P, _P]),
+    "fj_plan_set_variant": (_I, [_P, _I]),
+    "fj_plan_autotune": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _I, ctypes.POINTER(_I), _P, _P]),
     "fj_plan_step_graph": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_step_save": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
                                ctypes.POINTER(_P), _D, _P]),
@@ -162,6 +164,7 @@ def ctx(device: torch.device | int | None = None) -> int:
 PIPELINES = {"fused": 0, "staged": 1, "split": 2}
 
 
+NUM_SPLIT_VARIANTS = 6  # FJ_NUM_SPLIT_VARIANTS
 TILES = {"8x32": 0, "4x32": 1, "6x32": 2, "8x16": 3, "16x32": 4, "8x64": 5, "16x16": 6}
 
 

@@ -182,7 +182,7 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
               double* const* q2s, double* const* q_out, int nblocks, const fj_link* links, int nlinks,
               const fj_bc* bcs, int nbcs, const fj_params* p, double dt, void* const* kmet, void* tail,
               size_t tail_b, cudaStream_t st, const double* mu0_b = nullptr, const double* dt_b = nullptr,
-              double p_ref = 0.0) {
+              double p_ref = 0.0, int variant = 0) {
   std::vector<fj_block> out(blocks, blocks + nblocks);
   int s;
   for (int b = 0; b < nblocks; ++b) {
@@ -212,19 +212,19 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
     Phys ph = make_phys(p);
     ph.p_ref = p_ref;
     // the assembly of stages 1 and 2 also writes the next stage's primitives
-    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 1, p->precision, st, false, true);
+    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 1, p->precision, st, false, true, variant);
     if (s != FJ_OK) return s;
     for (int b = 0; b < nblocks; ++b) {
       sb[b].q = q1s[b];
       sb[b].out = q2s[b];
     }
-    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 2, p->precision, st, true, true);
+    s = split_stage(ctx, sb.data(), nblocks, ph, flags, 2, p->precision, st, true, true, variant);
     if (s != FJ_OK) return s;
     for (int b = 0; b < nblocks; ++b) {
       sb[b].q = q2s[b];
       sb[b].out = q_out[b];
     }
-    return split_stage(ctx, sb.data(), nblocks, ph, flags, 3, p->precision, st, true, false);
+    return split_stage(ctx, sb.data(), nblocks, ph, flags, 3, p->precision, st, true, false, variant);
   }
   for (int b = 0; b < nblocks; ++b) {
     const fj_block& B = out[b];
@@ -531,13 +531,19 @@ static int plan_step_impl(fj_plan* pl, double* const* q_in, double* const* q_out
                     pl->links.data(), (int)pl->links.size(), pl->bcs.data(), (int)pl->bcs.size(), &pl->p, dt,
                     pl->kmet.empty() ? nullptr : pl->kmet.data(), tail, pl->halo_bytes, S(stream),
                     pl->mu0_b.empty() ? nullptr : pl->mu0_b.data(), pl->dt_b.empty() ? nullptr : pl->dt_b.data(),
-                    pl->p_ref);
+                    pl->p_ref, pl->variant);
   ctx->pipeline = saved;
   return s;
 }
 
 int fj_plan_step(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, void* stream) {
   return plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);
+}
+
+static void drop_graphs(fj_plan* pl) {
+  for (fj_graph_entry& g : pl->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  pl->graphs.clear();
 }
 
 int fj_plan_set_ensemble(fj_plan* pl, const double* mu0, const double* dt) {
@@ -553,10 +559,57 @@ int fj_plan_set_ensemble(fj_plan* pl, const double* mu0, const double* dt) {
   pl->dt_b.clear();
   if (mu0) pl->mu0_b.assign(mu0, mu0 + nb);
   if (dt) pl->dt_b.assign(dt, dt + nb);
-  for (fj_graph_entry& g : pl->graphs)
-    if (g.exec) cudaGraphExecDestroy(g.exec);
-  pl->graphs.clear();
+  drop_graphs(pl);
   return FJ_OK;
+}
+
+int fj_plan_set_variant(fj_plan* pl, int variant) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  if (variant < 0 || variant >= FJ_NUM_SPLIT_VARIANTS)
+    return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "unknown launch-shape variant");
+  if (variant != pl->variant) drop_graphs(pl);
+  pl->variant = variant;
+  return FJ_OK;
+}
+
+int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, int reps, int* chosen,
+                     double* ms_out, void* stream) {
+  if (!pl || !chosen || reps < 1) return FJ_ERR_INVALID_ARGUMENT;
+  fj_ctx* ctx = pl->ctx;
+  const bool tunable = pl->pipeline == FJ_PIPELINE_SPLIT && pl->p.precision == FJ_PREC_F32FLUX;
+  const int nv = tunable ? FJ_NUM_SPLIT_VARIANTS : 1;
+  cudaStream_t st = S(stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int s = cuda_status(ctx, cudaEventCreate(&e0), "event");
+  if (s == FJ_OK) s = cuda_status(ctx, cudaEventCreate(&e1), "event");
+  const int keep = pl->variant;
+  int best = keep;
+  float best_ms = 0.0f;
+  for (int v = 0; v < nv && s == FJ_OK; ++v) {
+    if (ms_out) ms_out[v] = 0.0;
+    s = fj_plan_set_variant(pl, tunable ? v : keep);
+    if (s == FJ_OK) s = plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);  // untimed
+    if (s == FJ_OK) s = cuda_status(ctx, cudaEventRecord(e0, st), "event record");
+    for (int r = 0; r < reps && s == FJ_OK; ++r)
+      s = plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);
+    if (s == FJ_OK) s = cuda_status(ctx, cudaEventRecord(e1, st), "event record");
+    if (s == FJ_OK) s = cuda_status(ctx, cudaEventSynchronize(e1), "event sync");
+    float ms = 0.0f;
+    if (s == FJ_OK) s = cuda_status(ctx, cudaEventElapsedTime(&ms, e0, e1), "event time");
+    if (s == FJ_OK) {
+      if (ms_out) ms_out[v] = ms / reps;
+      if (v == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = tunable ? v : keep;
+      }
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  const int r = fj_plan_set_variant(pl, s == FJ_OK ? best : keep);
+  if (s == FJ_OK) s = r;
+  *chosen = pl->variant;
+  return s;
 }
 
 int fj_plan_step_graph(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, void* stream) {
@@ -648,7 +701,7 @@ int fj_plan_stage(fj_plan* pl, double* const* q, double* const* q0, double* cons
     split_assign_scratch(pl->p.precision, sb.data(), nb, tail);
     Phys ph = make_phys(&pl->p);
     ph.p_ref = pl->p_ref;
-    s = split_stage(ctx, sb.data(), nb, ph, flags, stage, pl->p.precision, S(stream));
+    s = split_stage(ctx, sb.data(), nb, ph, flags, stage, pl->p.precision, S(stream), false, false, pl->variant);
   } else {
     for (int b = 0; b < nb && s == FJ_OK; ++b) {
       const fj_block& B = pl->blocks[b];

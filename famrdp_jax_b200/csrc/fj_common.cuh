@@ -49,6 +49,7 @@ struct fj_plan {
   int pipeline = 0;
   std::vector<double> mu0_b, dt_b;        // per-block overrides (ensembles), empty = none
   double p_ref = 0.0;                     // FP32-flux split path: momentum-flux pressure offset
+  int variant = 0;                        // launch shape of the FP32 split kernels
   cudaStream_t capture_stream = nullptr;  // private stream for graph capture
   std::vector<fj_graph_entry> graphs;     // most recently used last
 };

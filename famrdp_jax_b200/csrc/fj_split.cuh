@@ -53,7 +53,9 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
 // stage's assembly with next_prims), so the primitive launch is skipped;
 // next_prims (stages 1, 2): the assembly also writes the primitives of its
 // result for the next stage.
+// variant: launch shape of the FP32 record kernels (0 .. FJ_NUM_SPLIT_VARIANTS-1).
 int split_stage(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                int stage, int precision, cudaStream_t st, bool prims_ready = false, bool next_prims = false);
+                int stage, int precision, cudaStream_t st, bool prims_ready = false, bool next_prims = false,
+                int variant = 0);
 
 }  // namespace fj

@@ -234,8 +234,8 @@ __device__ __forceinline__ void face_from_cells(const Cell6<T>& a0, const Cell6<
                             (T)ph.eps_entropy, ph.limiter, F, p_ref);
 }
 
-template <typename T, bool K_AOS>
-__global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::fluxes) k_split_fluxes(const Table tab, const Phys ph,
+template <typename T, bool K_AOS, int OCC = SplitOcc<T>::fluxes>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table tab, const Phys ph,
                                                                                    const int flags) {
   using M = FastMath<T>;
   const int b = find_block(tab, blockIdx.x);
@@ -327,8 +327,8 @@ __global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::fluxes) k_split_fl
 
 // With next_prims, also writes the primitives of the stage result (the next
 // stage's input) in place of a separate k_split_prims launch.
-template <typename T, bool K_AOS>
-__global__ void __launch_bounds__(kSplitThreads, SplitOcc<T>::assemble) k_split_assemble(const Table tab,
+template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Table tab,
                                                                                        const int flags,
                                                                                        const int stage,
                                                                                        const int next_prims,
@@ -756,9 +756,22 @@ __global__ void k_pressure_sum(const double* __restrict__ q, int64_t N, double g
   if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
 }
 
+// Launch shapes of the FP32 record kernels (minimum resident CTAs per SM of
+// the flux and assembly kernels, i.e. their register caps), selected per plan
+// by the autotuner; index 0 is the default.
+constexpr int kSplitVariants[][2] = {{3, 6}, {3, 4}, {4, 4}, {3, 5}, {4, 6}, {3, 8}};
+static_assert(sizeof(kSplitVariants) / sizeof(kSplitVariants[0]) == FJ_NUM_SPLIT_VARIANTS, "variant table");
+
+template <typename T, bool K_AOS, int FO, int AO>
+void launch_pair(const Table& tab, int ctas, const Phys& ph, int flags, int stage, int np, cudaStream_t st) {
+  k_split_fluxes<T, K_AOS, FO><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
+  k_split_assemble<T, K_AOS, AO><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
+                                                                 K_AOS ? ph.p_ref : 0.0);
+}
+
 template <typename T, bool K_AOS>
 int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage, bool prims_ready,
-               bool next_prims, cudaStream_t st) {
+               bool next_prims, int variant, cudaStream_t st) {
   const int np = next_prims ? 1 : 0;
   if constexpr (sizeof(T) == 8) {
     if (!prims_ready) fm::k_fm_prims<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R);
@@ -766,16 +779,21 @@ int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage,
     fm::k_fm_assemble<double><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R);
   } else {
     if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, K_AOS ? ph.p_ref : 0.0);
-    k_split_fluxes<T, K_AOS><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
-    k_split_assemble<T, K_AOS><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
-                                                                 K_AOS ? ph.p_ref : 0.0);
+    switch (K_AOS ? variant : 0) {
+      case 1: launch_pair<T, K_AOS, kSplitVariants[1][0], kSplitVariants[1][1]>(tab, ctas, ph, flags, stage, np, st); break;
+      case 2: launch_pair<T, K_AOS, kSplitVariants[2][0], kSplitVariants[2][1]>(tab, ctas, ph, flags, stage, np, st); break;
+      case 3: launch_pair<T, K_AOS, kSplitVariants[3][0], kSplitVariants[3][1]>(tab, ctas, ph, flags, stage, np, st); break;
+      case 4: launch_pair<T, K_AOS, kSplitVariants[4][0], kSplitVariants[4][1]>(tab, ctas, ph, flags, stage, np, st); break;
+      case 5: launch_pair<T, K_AOS, kSplitVariants[5][0], kSplitVariants[5][1]>(tab, ctas, ph, flags, stage, np, st); break;
+      default: launch_pair<T, K_AOS, kSplitVariants[0][0], kSplitVariants[0][1]>(tab, ctas, ph, flags, stage, np, st);
+    }
   }
   return prims_ready ? 2 : 3;
 }
 
 template <typename T>
 int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                 int stage, bool prims_ready, bool next_prims, cudaStream_t st) {
+                 int stage, bool prims_ready, bool next_prims, int variant, cudaStream_t st) {
   for (int base = 0; base < nblocks; base += kMaxSplitBlocks) {
     Table tab;
     tab.n = std::min(kMaxSplitBlocks, nblocks - base);
@@ -797,8 +815,8 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
     }
     if (k_aos && sizeof(T) == 8)
       return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "the FP64 split path reads kxyz directly");
-    ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, ph, flags, stage, prims_ready, next_prims, st)
-                           : launch_tab<T, false>(tab, ctas, ph, flags, stage, prims_ready, next_prims, st);
+    ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st)
+                           : launch_tab<T, false>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st);
     int s = launch_status(ctx, "split stage launch");
     if (s != FJ_OK) return s;
   }
@@ -888,11 +906,12 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
 }
 
 int split_stage(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                int stage, int precision, cudaStream_t st, bool prims_ready, bool next_prims) {
+                int stage, int precision, cudaStream_t st, bool prims_ready, bool next_prims, int variant) {
   if (next_prims && (stage < 1 || stage > 2)) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "next_prims needs stage 1 or 2");
+  if (variant < 0 || variant >= FJ_NUM_SPLIT_VARIANTS) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown variant");
   if (precision == FJ_PREC_F32FLUX)
-    return launch_split<float>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, st);
-  return launch_split<double>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, st);
+    return launch_split<float>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, variant, st);
+  return launch_split<double>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, variant, st);
 }
 
 }  // namespace fj

@@ -106,6 +106,23 @@ class StepPlan:
         self.mu0s = None if mu0 is None else [float(v) for v in mu0]
         self.dts = None if dt is None else [float(v) for v in dt]
 
+    def autotune(self, qs, outs, dt: float, reps: int = 3):
+        """Times every launch shape of the FP32-flux split kernels over `reps`
+        steps qs -> outs (outs is overwritten) and keeps the fastest; returns
+        (chosen shape, mean step ms per shape)."""
+        n = _capi.NUM_SPLIT_VARIANTS
+        ms = (ctypes.c_double * n)()
+        ch = ctypes.c_int()
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_autotune(self._handle, _topology.ptr_array(qs), _topology.ptr_array(outs),
+                                               float(dt), int(reps), ctypes.byref(ch), ms, _capi.stream(self.device)),
+                    "fj_plan_autotune", c)
+        return ch.value, list(ms)
+
+    def set_variant(self, variant: int) -> None:
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_set_variant(self._handle, int(variant)), "fj_plan_set_variant", c)
+
     def run_save(self, qs, outs, q0s, q1s, q2s, dt: float) -> None:
         """One step that also keeps its intermediate states (the halo-filled
         start state and the first two stage values) for the step adjoint."""

@@ -240,6 +240,19 @@ int fj_plan_set_ensemble(fj_plan* plan, const double* mu0, const double* dt);
  * the FJ_PLAN_MAX_GRAPHS most recently used graphs (a ping-pong loop uses
  * two). */
 #define FJ_PLAN_MAX_GRAPHS 4
+/* Launch shape of the plan's FP32-flux split kernels: the register caps
+ * (minimum resident CTAs per SM) of the flux and assembly kernels, one of
+ * FJ_NUM_SPLIT_VARIANTS; 0 is the default.  Changing it drops captured graphs.
+ * Results do not depend on it. */
+#define FJ_NUM_SPLIT_VARIANTS 6
+int fj_plan_set_variant(fj_plan* plan, int variant);
+/* The autotuner: times `reps` steps q_in -> q_out (after one untimed step) for
+ * every launch shape with CUDA events on `stream`, keeps the fastest in the
+ * plan and reports it (and, if ms_out is non-NULL, the FJ_NUM_SPLIT_VARIANTS
+ * mean step times).  q_out is overwritten; q_in is not changed.  Synchronises
+ * the stream.  Plans of other pipelines or of FP64 have one shape (returns 0). */
+int fj_plan_autotune(fj_plan* plan, double* const* q_in, double* const* q_out, double dt, int reps,
+                     int* chosen, double* ms_out, void* stream);
 int fj_plan_step_graph(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,
                        void* stream);
 int fj_plan_destroy(fj_plan* plan);

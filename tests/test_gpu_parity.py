@@ -442,3 +442,28 @@ def test_residual_and_monitored_run(cuda_device, tmp_path):
     with pytest.raises(FloatingPointError, match="step 1"):
         run(st_bad, cfg, dt, 3, dump_dir=tmp_path / "dumps")
     assert sorted(p.name for p in (tmp_path / "dumps").iterdir()) == ["step0000000_good.pt", "step0000001_bad.pt"]
+
+
+def test_autotune_launch_shapes_agree(cuda_device):
+    """Every launch shape of the FP32-flux split kernels gives the same step
+    bit for bit (only register caps differ); the autotuner keeps one of them."""
+    import dataclasses
+    from famrdp_jax_b200 import _capi
+    from famrdp_jax_b200.solver.step import StepPlan
+    c = cases.tree24(nblocks=4, lo=6, hi=12, seed=2)
+    cfg = dataclasses.replace(c.cfg, precision="f32")
+    st = state_from_case(c)
+    dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], cfg.gas.gamma, c.cfl, 2)
+    plan = StepPlan(st, cfg)
+    qs = [b.q for b in st.blocks]
+    outs = []
+    for v in range(_capi.NUM_SPLIT_VARIANTS):
+        plan.set_variant(v)
+        o = [torch.empty_like(q) for q in qs]
+        plan.run(qs, o, dt)
+        outs.append(o)
+    for o in outs[1:]:
+        for a, b in zip(o, outs[0]):
+            assert torch.equal(a, b)
+    chosen, ms = plan.autotune(qs, [torch.empty_like(q) for q in qs], dt, reps=2)
+    assert 0 <= chosen < _capi.NUM_SPLIT_VARIANTS and len(ms) == _capi.NUM_SPLIT_VARIANTS and min(ms) > 0
