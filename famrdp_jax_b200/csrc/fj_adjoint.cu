@@ -290,11 +290,11 @@ __device__ __forceinline__ double adj_visc_cell(const T* __restrict__ P, const d
   return dot;
 }
 
-template <typename T>
-__global__ void k_adj_visc(const T* __restrict__ P, const double* __restrict__ kxyz,
-                           const double* __restrict__ lam, T* __restrict__ lamD,
-                           T* __restrict__ lamL, ADims d, Phys ph, double* __restrict__ dmu,
-                           double mu_scale) {
+template <typename T, int MB = 1>
+__global__ void __launch_bounds__(kAT, MB) k_adj_visc(const T* __restrict__ P, const double* __restrict__ kxyz,
+                                                     const double* __restrict__ lam, T* __restrict__ lamD,
+                                                     T* __restrict__ lamL, ADims d, Phys ph,
+                                                     double* __restrict__ dmu, double mu_scale) {
   const int N = d.ni * d.nj * d.nk;
   const int y = blockIdx.x * blockDim.x + threadIdx.x;
   double dot = 0.0;
@@ -459,8 +459,9 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
     cudaError_t e = cudaMemsetAsync(lamP, 0, 5 * (size_t)N * sizeof(T), st);
     if (e != cudaSuccess) return cuda_status(ctx, e, "vjp memset");
     // register caps (threads per CTA, minimum CTAs per SM): the FP64 face VJP
-    // needs ~180 registers uncapped; variant 0 trades a few spilled values for
-    // 12 resident warps (FP64) or 24 (FP32)
+    // needs ~180 registers uncapped.  Variant 0 is the fastest measured on
+    // B200 (TGV 96^3 adjoint sweep): FP64 128 x 4 (128 registers), FP32
+    // 256 x 3 (80 registers, a few spilled values)
     auto launch = [&](auto kern, int nt) {
       kern<<<dim3((unsigned)((N + nt - 1) / nt), 3), nt, 0, st>>>(P, kxyz, vol, lam, lamP, d, ph);
     };
@@ -468,17 +469,22 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
     switch (ctx->adj_variant) {
       case 1: launch(k_adj_faces<T, 256, 1>, 256); break;
       case 2:
-        if (f64) launch(k_adj_faces<T, 128, 4>, 128);
+      case 4:
+        if (f64) launch(k_adj_faces<T, 128, 3>, 128);
         else launch(k_adj_faces<T, 256, 2>, 256);
         break;
       default:
-        if (f64) launch(k_adj_faces<T, 128, 3>, 128);
+        if (f64) launch(k_adj_faces<T, 128, 4>, 128);
         else launch(k_adj_faces<T, 256, 3>, 256);
     }
     ctx->launches += 1;
   }
   if (flags & kRhsViscous) {
-    k_adj_visc<T><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale);
+    // variants 0 and 2 cap the viscous VJP at 64 registers (4 CTAs per SM)
+    if (ctx->adj_variant == 0 || ctx->adj_variant == 2)
+      k_adj_visc<T, 4><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale);
+    else
+      k_adj_visc<T><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale);
     ctx->launches += 1;
   }
   k_adj_final<T><<<grid, kAT, 0, st>>>(q, lamP, lamD, lamL, out, d, ph, flags, epi ? *epi : VjpEpilogue{});

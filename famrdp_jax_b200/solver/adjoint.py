@@ -6,8 +6,9 @@ test_grad.py:30-35): reverse-mode AD through every jnp operation of every
 step, storing everything.  Here the reverse mode is written by hand in CUDA
 (``fj_rhs_vjp_f64``, ``fj_step_vjp_f64``) and the trajectory keeps only one
 state every ``checkpoint_every`` steps: the reverse sweep recomputes each
-segment's states from its checkpoint and runs the step adjoints backwards
-through it.
+segment's states from its checkpoint (keeping every step's halo-filled start
+state and stage values) and runs the step adjoints backwards through it; the
+last segment's states are kept by the forward sweep itself.
 
     qN = integrate(state, cfg, dt, nsteps, checkpoint_every=10)   # differentiable
     J = kinetic_energy(State(qN...)) ...; J.backward()
@@ -136,6 +137,9 @@ class _Run:
     # per step of a segment
     _ping: list | None = None
     _saved: list | None = None
+    # the last segment's saved states, kept by the forward sweep (the reverse
+    # sweep starts there, so that segment is not recomputed)
+    _last_states: list | None = None
 
     def buffers(self, like):
         if self._ping is None:
@@ -170,7 +174,10 @@ def _reverse_sweep(run: _Run, checkpoints, lams):
     nseg = len(checkpoints)
     for s in reversed(range(nseg)):
         seg_len = min(run.every, run.nsteps - s * run.every)
-        _, states = _forward_segment(run, checkpoints[s], seg_len, keep=True)
+        if s == nseg - 1 and run._last_states is not None and len(run._last_states) == seg_len:
+            states, run._last_states = run._last_states, None
+        else:
+            _, states = _forward_segment(run, checkpoints[s], seg_len, keep=True)
         while states:
             step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu,
                            mu0s=run.plan.mu0s, dts=run.plan.dts, out=lams)
@@ -181,10 +188,14 @@ def _forward_with_checkpoints(run: _Run, q0s):
     checkpoints = []
     cur = [q.detach() for q in q0s]
     done = 0
+    run._last_states = None
     while done < run.nsteps:
         checkpoints.append([q.clone() for q in cur])
         n = min(run.every, run.nsteps - done)
-        cur, _ = _forward_segment(run, cur, n, keep=False)
+        last = done + n >= run.nsteps
+        cur, states = _forward_segment(run, cur, n, keep=last)
+        if last:
+            run._last_states = states
         done += n
     return [q.clone() for q in cur], checkpoints
 

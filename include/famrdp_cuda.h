@@ -118,11 +118,13 @@ const char* fj_last_error(const fj_ctx* ctx);
  * 8x64, 16x16 (the last three FP32-flux only; FP64 maps them to 8x32/8x16). */
 #define FJ_NUM_TILES 7
 int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg, int tile);
-/* Launch shape of the face kernel of the RHS adjoint (a tuning knob; results
- * agree to the rounding of atomic accumulation order): 0 = register-capped
- * for occupancy (default), 1 = uncapped, 2 = the other cap.  The reference
- * has no counterpart. */
-#define FJ_NUM_ADJ_VARIANTS 3
+/* Launch shape of the RHS adjoint's face and viscous kernels (a tuning knob;
+ * results agree to the rounding of atomic accumulation order): 0 = the
+ * fastest measured (default; face kernel register-capped per precision,
+ * viscous kernel capped at 64 registers), 1 = face kernel uncapped, 2 = the
+ * other face cap, 3 = 0 and 4 = 2 with the viscous kernel uncapped.  The
+ * reference has no counterpart. */
+#define FJ_NUM_ADJ_VARIANTS 5
 int fj_ctx_set_adjoint_variant(fj_ctx* ctx, int variant);
 /* Number of kernels launched through this context so far (instrumentation;
  * the reference has no counterpart). */
