@@ -1,12 +1,17 @@
 """Throughput of the RHS + TVD-RK3 step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload wavy4|tgv32|tree24] [--precision f32|f64] [--n 128]
+                    [--workload wavy4|tgv32|tree24|ensemble64] [--precision f32|f64] [--n 128]
+                    [--no-cpu] [--no-adjoint] [--no-error-table]
+    python bench.py --adjoint-only [--adjoint-n 96] [--adjoint-steps 50] [--adjoint-every 10]
+                    [--adjoint-precision both|f32|f64] [--adjoint-variant 0..4]
 
 One "step" = one full TVD-RK3 time step (halo fill + boundary conditions +
-three RHS/stage evaluations) over every block of the workload.  The default
-workload is 4 curvilinear blocks of 128^3 cells (2 x 2 in i-j, periodic,
-Mach 0.5, Re 1e4, 1 % seeded noise; synthetic data, inputs larger than L2).
+three RHS/stage evaluations) over every block of the workload, replayed from a
+captured CUDA graph.  The default workload is 4 curvilinear blocks of 128^3
+cells (2 x 2 in i-j, periodic, Mach 0.5, Re 1e4, 1 % seeded noise; synthetic
+data, inputs larger than L2).  Before timing, each plan's launch shape is
+picked by the autotuner (fj_plan_autotune).
 
 Printed on rank 0 as ONE JSON line:
   value        whole-job Mcell-stages/s of the selected precision (default the
@@ -24,7 +29,12 @@ Printed on rank 0 as ONE JSON line:
                written: 164 B per padded cell with the FP32 metric copy, 200 B
                in FP64) / its CUDA-event duration, against the measured HBM
                copy bandwidth;
-  cpu_baseline the NumPy FP64 oracle (1 core) on one block for one step.
+  cpu_baseline the NumPy FP64 oracle (1 core) on one block for one step;
+  fp32_error_table  FP32-flux against FP64 per conserved variable, full and
+               interior, at steps 1, 10, 100 (and 200 for tree24);
+  adjoint      adjoint/forward time of the checkpointed trajectory adjoint on
+               the 96^3 Taylor-Green case (50 steps, a checkpoint every 10),
+               FP64 and FP32-flux, with dJ/dmu0 and dJ/dM0.
 
 ``--impl reference`` times the reference algorithm on the host cores (the
 PyTorch-CPU FP64 port of the reference, all threads; the reference itself is
@@ -56,9 +66,11 @@ UNIT = "Mcell-stages/s"
 # q0 (40), metrics (72 FP64 or 36 as the FP32 copy), vol (8); write 40
 STAGE_BYTES = {"f64": 200.0, "f32": 164.0}
 STEP_BYTES = {"f64": 560.0, "f32": 452.0}
-# DRAM bytes per padded cell of one stage (sum over the three split-pipeline
-# kernels) from the ncu capture summarised in profiles/split_stage_128.md
-STAGE_TRAFFIC = {"f32": 474.0, "f64": None}
+# DRAM bytes per padded cell of one stage-2 launch group (dram__bytes_read +
+# dram__bytes_write summed over the primitive, flux and assembly kernels),
+# measured by ncu on the 96^3 Taylor-Green case (1.0 M padded cells) and
+# scaled per cell: FP32 41 + 136 + 289 B, FP64 43 + 268 + 384 B
+STAGE_TRAFFIC = {"f32": 466.0, "f64": 695.0}
 
 
 def _peaks():
@@ -236,7 +248,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_desc(c, args) | {"sample": "block 0 only"},
+            "config": {k: v for k, v in workload_desc(c, args).items() if k != "cuda_graph"}
+                      | {"sample": "block 0 only", "precision": "f64"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference (JAX) not installable in this image: no jax/jaxlib wheel, no network"}
