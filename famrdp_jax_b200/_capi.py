@@ -76,6 +76,7 @@ SIGNATURES = {
     "fj_plan_step": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_set_ensemble": (_I, [_P, _P, _P]),
     "fj_plan_set_variant": (_I, [_P, _I]),
+    "fj_plan_set_streams": (_I, [_P, _I]),
     "fj_plan_autotune": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _I, ctypes.POINTER(_I), _P, _P]),
     "fj_plan_step_graph": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_step_save": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),

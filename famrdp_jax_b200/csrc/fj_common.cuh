@@ -50,6 +50,9 @@ struct fj_plan {
   std::vector<double> mu0_b, dt_b;        // per-block overrides (ensembles), empty = none
   double p_ref = 0.0;                     // FP32-flux split path: momentum-flux pressure offset
   int variant = 0;                        // launch shape of the FP32 split kernels
+  int streams = 1;                        // 1, or 2: block groups on two streams
+  cudaStream_t side_stream = nullptr;     // the second stream and its fork/join events
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t capture_stream = nullptr;  // private stream for graph capture
   std::vector<fj_graph_entry> graphs;     // most recently used last
 };

@@ -53,9 +53,10 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
 // stage's assembly with next_prims), so the primitive launch is skipped;
 // next_prims (stages 1, 2): the assembly also writes the primitives of its
 // result for the next stage.
-// variant: launch shape of the FP32 record kernels (0 .. FJ_NUM_SPLIT_VARIANTS-1).
+// variant: launch shape of the FP32 record kernels (0 .. FJ_NUM_SPLIT_VARIANTS-1);
+// after_fluxes (optional): recorded on st right after the (first) flux launch.
 int split_stage(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
                 int stage, int precision, cudaStream_t st, bool prims_ready = false, bool next_prims = false,
-                int variant = 0);
+                int variant = 0, cudaEvent_t after_fluxes = nullptr);
 
 }  // namespace fj

@@ -327,46 +327,48 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
 
 // With next_prims, also writes the primitives of the stage result (the next
 // stage's input) in place of a separate k_split_prims launch.
-template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
-__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Table tab,
-                                                                                       const int flags,
-                                                                                       const int stage,
-                                                                                       const int next_prims,
-                                                                                       const double gm1,
-                                                                                       const double R,
-                                                                                       const double ph_p_ref) {
-  const int b = find_block(tab, blockIdx.x);
-  Cell x;
-  if (!decode(tab.b[b], blockIdx.x, x)) return;
-  const SplitBlock& B = tab.b[b].blk;
+// Where the assembly reads the intermediates of a cell from: the scratch
+// arrays through L1/L2 (the interface lets another source, e.g. a
+// shared-memory copy, feed the same arithmetic).
+template <typename T, bool K_AOS>
+struct GlobalSrc {
+  const SplitBlock& B;
+  int32_t N;
+  __device__ __forceinline__ void F_rec(int32_t c, T* o) const { ld_rec<T, kRecF>((const T*)B.F + (size_t)c * kRecF, o); }
+  __device__ __forceinline__ T F_val(int32_t c, int off) const { return ((const T*)B.F)[(size_t)c * kRecF + off]; }
+  __device__ __forceinline__ void G_rec(int32_t c, T* o) const { ld_rec<T, kRecG>((const T*)B.G + (size_t)c * kRecG, o); }
+  __device__ __forceinline__ void K9(int32_t c, T* kk, T* gcl) const { metric9<T, K_AOS>(B, N, c, kk, gcl); }
+};
+
+// The assembly of one cell (rhs/invscd.py:119-131, rhs/viscous.py:86-117,
+// solver/step.py:45-53) from the intermediates Src provides.
+template <typename T, bool K_AOS, class Src>
+__device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x, const Src& src, int flags,
+                                              int stage, int next_prims, double gm1, double R, double ph_p_ref) {
   const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
   const int32_t si = x.nj * x.nk, sj = x.nk;
   const int n[3] = {x.ni, x.nj, x.nk};
   const int idx[3] = {x.i, x.j, x.k};
   const int32_t st[3] = {si, sj, 1};
   double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  T kk[9], gcl[3] = {T(0), T(0), T(0)};
+  src.K9(c, kk, K_AOS ? gcl : nullptr);
   if (flags & kRhsInvscd) {
-    const T* F = (const T*)B.F;
     const bool on[3] = {idx[0] >= 2 && idx[0] <= n[0] - 3, idx[1] >= 2 && idx[1] <= n[1] - 3,
                         idx[2] >= 2 && idx[2] <= n[2] - 3};
     if (on[0] || on[1] || on[2]) {
       const double ivd = 1.0 / (B.vol[c] + 1e-300);
       T Fc[kRecF];
-      ld_rec<T, kRecF>(F + (size_t)c * kRecF, Fc);
-      // sum over the active axes of the face-normal differences, from the
-      // FP64 metrics (the p_ref n part the face fluxes left out)
-      double pg[3] = {0.0, 0.0, 0.0};
-      if constexpr (K_AOS) {
-        const T* rec = (const T*)B.kaos + (size_t)c * kRecK<T>;
-        pg[0] = ph_p_ref * (double)rec[9];
-        pg[1] = ph_p_ref * (double)rec[10];
-        pg[2] = ph_p_ref * (double)rec[11];
-      }
+      src.F_rec(c, Fc);
+      // the p_ref n part the face fluxes left out: p_ref times the sum over
+      // the active axes of the face-normal differences, evaluated in FP64 when
+      // the records were built
+      const double pg[3] = {ph_p_ref * (double)gcl[0], ph_p_ref * (double)gcl[1], ph_p_ref * (double)gcl[2]};
       T Fm[3][5];
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int v = 0; v < 5; ++v) Fm[a][v] = on[a] ? F[(size_t)(c - st[a]) * kRecF + 5 * a + v] : T(0);
+        for (int v = 0; v < 5; ++v) Fm[a][v] = on[a] ? src.F_val(c - st[a], 5 * a + v) : T(0);
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
         double dsum;
@@ -381,7 +383,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
           for (int a = 0; a < 3; ++a)
             if (on[a]) s += Fc[5 * a + v] - Fm[a][v];
           dsum = (double)s;
-          if (v >= 1 && v <= 3) dsum += pg[v - 1];
+          if (K_AOS && v >= 1 && v <= 3) dsum += pg[v - 1];
         }
         r[v] = -dsum * ivd;
       }
@@ -390,10 +392,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
   if (flags & kRhsViscous) {
     // sum_l 0.5 kxyz[l][jj] (G(c+e_l) - G(c-e_l)) per equation, one
     // neighbour record at a time (rhs/viscous.py:86-117)
-    const T* G = (const T*)B.G;
     const T* Gz = (const T*)B.Gz;
-    T kk[9];
-    metric9<T, K_AOS>(B, N, c, kk);
     T acc[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
     for (int l = 0; l < 3; ++l) {
@@ -403,7 +402,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
                                      : (idx[l] == 0 ? c + (n[l] - 1) * st[l] : c - st[l]);
         const T s = side == 0 ? T(0.5) : T(-0.5);
         T g[kRecG];
-        ld_rec<T, kRecG>(G + (size_t)nb * kRecG, g);
+        src.G_rec(nb, g);
         const T gz = Gz[nb];
         const T k0 = s * kk[3 * l], k1 = s * kk[3 * l + 1], k2 = s * kk[3 * l + 2];
         acc[0] += g[0] * k0 + g[1] * k1 + g[2] * k2;
@@ -438,6 +437,21 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
       st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
     }
   }
+}
+
+// With next_prims, also writes the primitives of the stage result (the next
+// stage's input) in place of a separate k_split_prims launch.
+template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Table tab, const int flags,
+                                                                       const int stage, const int next_prims,
+                                                                       const double gm1, const double R,
+                                                                       const double ph_p_ref) {
+  const int b = find_block(tab, blockIdx.x);
+  Cell x;
+  if (!decode(tab.b[b], blockIdx.x, x)) return;
+  const SplitBlock& B = tab.b[b].blk;
+  const GlobalSrc<T, K_AOS> src{B, (int32_t)x.N};
+  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, ph_p_ref);
 }
 
 // ---- field-major variant (the FP64 path) ----------------------------------
@@ -756,36 +770,43 @@ __global__ void k_pressure_sum(const double* __restrict__ q, int64_t N, double g
   if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
 }
 
-// Launch shapes of the FP32 record kernels (minimum resident CTAs per SM of
-// the flux and assembly kernels, i.e. their register caps), selected per plan
-// by the autotuner; index 0 is the default.
-constexpr int kSplitVariants[][2] = {{3, 6}, {3, 4}, {4, 4}, {3, 5}, {4, 6}, {3, 8}};
+// Launch shapes of the FP32 record kernels, selected per plan by the
+// autotuner (index 0 is the default): the minimum resident CTAs per SM of the
+// flux and assembly kernels, i.e. their register caps.
+struct SplitShape {
+  int flux_occ, asm_occ;
+};
+constexpr SplitShape kSplitVariants[] = {{3, 6}, {3, 4}, {4, 4}, {3, 5}, {4, 6}, {3, 8}};
 static_assert(sizeof(kSplitVariants) / sizeof(kSplitVariants[0]) == FJ_NUM_SPLIT_VARIANTS, "variant table");
 
-template <typename T, bool K_AOS, int FO, int AO>
-void launch_pair(const Table& tab, int ctas, const Phys& ph, int flags, int stage, int np, cudaStream_t st) {
-  k_split_fluxes<T, K_AOS, FO><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
-  k_split_assemble<T, K_AOS, AO><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
-                                                                 K_AOS ? ph.p_ref : 0.0);
+template <typename T, bool K_AOS, int V>
+void launch_pair(const Table& tab, int ctas, const Phys& ph, int flags, int stage, int np, cudaStream_t st,
+                 cudaEvent_t after_fluxes) {
+  constexpr SplitShape sh = kSplitVariants[V];
+  k_split_fluxes<T, K_AOS, sh.flux_occ><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
+  if (after_fluxes) cudaEventRecord(after_fluxes, st);
+  k_split_assemble<T, K_AOS, sh.asm_occ><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
+                                                                        K_AOS ? ph.p_ref : 0.0);
 }
 
 template <typename T, bool K_AOS>
 int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage, bool prims_ready,
-               bool next_prims, int variant, cudaStream_t st) {
+               bool next_prims, int variant, cudaStream_t st, cudaEvent_t after_fluxes) {
   const int np = next_prims ? 1 : 0;
   if constexpr (sizeof(T) == 8) {
     if (!prims_ready) fm::k_fm_prims<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R);
     fm::k_fm_fluxes<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
+    if (after_fluxes) cudaEventRecord(after_fluxes, st);
     fm::k_fm_assemble<double><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R);
   } else {
     if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, K_AOS ? ph.p_ref : 0.0);
     switch (K_AOS ? variant : 0) {
-      case 1: launch_pair<T, K_AOS, kSplitVariants[1][0], kSplitVariants[1][1]>(tab, ctas, ph, flags, stage, np, st); break;
-      case 2: launch_pair<T, K_AOS, kSplitVariants[2][0], kSplitVariants[2][1]>(tab, ctas, ph, flags, stage, np, st); break;
-      case 3: launch_pair<T, K_AOS, kSplitVariants[3][0], kSplitVariants[3][1]>(tab, ctas, ph, flags, stage, np, st); break;
-      case 4: launch_pair<T, K_AOS, kSplitVariants[4][0], kSplitVariants[4][1]>(tab, ctas, ph, flags, stage, np, st); break;
-      case 5: launch_pair<T, K_AOS, kSplitVariants[5][0], kSplitVariants[5][1]>(tab, ctas, ph, flags, stage, np, st); break;
-      default: launch_pair<T, K_AOS, kSplitVariants[0][0], kSplitVariants[0][1]>(tab, ctas, ph, flags, stage, np, st);
+      case 1: launch_pair<T, K_AOS, 1>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 2: launch_pair<T, K_AOS, 2>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 3: launch_pair<T, K_AOS, 3>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 4: launch_pair<T, K_AOS, 4>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 5: launch_pair<T, K_AOS, 5>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
+      default: launch_pair<T, K_AOS, 0>(tab, ctas, ph, flags, stage, np, st, after_fluxes);
     }
   }
   return prims_ready ? 2 : 3;
@@ -793,7 +814,8 @@ int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage,
 
 template <typename T>
 int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                 int stage, bool prims_ready, bool next_prims, int variant, cudaStream_t st) {
+                 int stage, bool prims_ready, bool next_prims, int variant, cudaStream_t st,
+                 cudaEvent_t after_fluxes) {
   for (int base = 0; base < nblocks; base += kMaxSplitBlocks) {
     Table tab;
     tab.n = std::min(kMaxSplitBlocks, nblocks - base);
@@ -815,8 +837,11 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
     }
     if (k_aos && sizeof(T) == 8)
       return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "the FP64 split path reads kxyz directly");
-    ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st)
-                           : launch_tab<T, false>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st);
+    // the event marks the first chunk's flux launch
+    cudaEvent_t ev = base == 0 ? after_fluxes : nullptr;
+    ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st, ev)
+                           : launch_tab<T, false>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st,
+                                                  ev);
     int s = launch_status(ctx, "split stage launch");
     if (s != FJ_OK) return s;
   }
@@ -906,12 +931,15 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
 }
 
 int split_stage(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
-                int stage, int precision, cudaStream_t st, bool prims_ready, bool next_prims, int variant) {
+                int stage, int precision, cudaStream_t st, bool prims_ready, bool next_prims, int variant,
+                cudaEvent_t after_fluxes) {
   if (next_prims && (stage < 1 || stage > 2)) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "next_prims needs stage 1 or 2");
   if (variant < 0 || variant >= FJ_NUM_SPLIT_VARIANTS) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "unknown variant");
   if (precision == FJ_PREC_F32FLUX)
-    return launch_split<float>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, variant, st);
-  return launch_split<double>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, variant, st);
+    return launch_split<float>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, variant, st,
+                               after_fluxes);
+  return launch_split<double>(ctx, blocks, nblocks, ph, flags, stage, prims_ready, next_prims, variant, st,
+                              after_fluxes);
 }
 
 }  // namespace fj

@@ -107,10 +107,11 @@ class StepPlan:
         self.dts = None if dt is None else [float(v) for v in dt]
 
     def autotune(self, qs, outs, dt: float, reps: int = 3):
-        """Times every launch shape of the FP32-flux split kernels over `reps`
-        steps qs -> outs (outs is overwritten) and keeps the fastest; returns
-        (chosen shape, mean step ms per shape)."""
-        n = _capi.NUM_SPLIT_VARIANTS
+        """Times every launch shape of the FP32-flux split kernels and both
+        stream counts over `reps` steps qs -> outs (outs is overwritten) and
+        keeps the fastest; returns (chosen, mean step ms per candidate), the
+        candidate index being shape + NUM_SPLIT_VARIANTS * (streams - 1)."""
+        n = 2 * _capi.NUM_SPLIT_VARIANTS
         ms = (ctypes.c_double * n)()
         ch = ctypes.c_int()
         c = _capi.ctx(self.device)
@@ -118,6 +119,10 @@ class StepPlan:
                                                float(dt), int(reps), ctypes.byref(ch), ms, _capi.stream(self.device)),
                     "fj_plan_autotune", c)
         return ch.value, list(ms)
+
+    def set_streams(self, n: int) -> None:
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_set_streams(self._handle, int(n)), "fj_plan_set_streams", c)
 
     def set_variant(self, variant: int) -> None:
         c = _capi.ctx(self.device)

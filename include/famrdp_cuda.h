@@ -248,11 +248,19 @@ int fj_plan_set_ensemble(fj_plan* plan, const double* mu0, const double* dt);
  * Results do not depend on it. */
 #define FJ_NUM_SPLIT_VARIANTS 6
 int fj_plan_set_variant(fj_plan* plan, int variant);
+/* Split-pipeline plans of two or more blocks: n = 2 splits the blocks into two
+ * groups of about equal cells whose three stages run on two streams (forked
+ * from and joined back into the step's stream), so one group's flux kernels
+ * overlap the other group's assemblies; n = 1 (default) runs all blocks per
+ * launch on one stream.  Results do not depend on it.  Drops captured graphs. */
+int fj_plan_set_streams(fj_plan* plan, int n);
 /* The autotuner: times `reps` steps q_in -> q_out (after one untimed step) for
- * every launch shape with CUDA events on `stream`, keeps the fastest in the
- * plan and reports it (and, if ms_out is non-NULL, the FJ_NUM_SPLIT_VARIANTS
- * mean step times).  q_out is overwritten; q_in is not changed.  Synchronises
- * the stream.  Plans of other pipelines or of FP64 have one shape (returns 0). */
+ * every launch shape (FP32-flux split plans) and stream count (split plans of
+ * two or more blocks) with CUDA events on `stream`, keeps the fastest in the
+ * plan and reports it as shape + FJ_NUM_SPLIT_VARIANTS * (streams - 1) (and,
+ * if ms_out is non-NULL, the 2 * FJ_NUM_SPLIT_VARIANTS mean step times at that
+ * index; 0 where not timed).  q_out is overwritten; q_in is not changed.
+ * Synchronises the stream. */
 int fj_plan_autotune(fj_plan* plan, double* const* q_in, double* const* q_out, double dt, int reps,
                      int* chosen, double* ms_out, void* stream);
 int fj_plan_step_graph(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,

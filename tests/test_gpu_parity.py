@@ -445,8 +445,9 @@ def test_residual_and_monitored_run(cuda_device, tmp_path):
 
 
 def test_autotune_launch_shapes_agree(cuda_device):
-    """Every launch shape of the FP32-flux split kernels gives the same step
-    bit for bit (only register caps differ); the autotuner keeps one of them."""
+    """Every launch shape of the FP32-flux split kernels and both stream counts
+    (block groups on two streams, also captured as a graph) give the same step
+    bit for bit; the autotuner keeps one of them."""
     import dataclasses
     from famrdp_jax_b200 import _capi
     from famrdp_jax_b200.solver.step import StepPlan
@@ -457,13 +458,17 @@ def test_autotune_launch_shapes_agree(cuda_device):
     plan = StepPlan(st, cfg)
     qs = [b.q for b in st.blocks]
     outs = []
-    for v in range(_capi.NUM_SPLIT_VARIANTS):
-        plan.set_variant(v)
-        o = [torch.empty_like(q) for q in qs]
-        plan.run(qs, o, dt)
-        outs.append(o)
+    for streams in (1, 2):
+        plan.set_streams(streams)
+        for v in range(_capi.NUM_SPLIT_VARIANTS):
+            plan.set_variant(v)
+            for graph in (False, True):
+                o = [torch.empty_like(q) for q in qs]
+                plan.run(qs, o, dt, graph=graph)
+                outs.append(o)
     for o in outs[1:]:
         for a, b in zip(o, outs[0]):
             assert torch.equal(a, b)
     chosen, ms = plan.autotune(qs, [torch.empty_like(q) for q in qs], dt, reps=2)
-    assert 0 <= chosen < _capi.NUM_SPLIT_VARIANTS and len(ms) == _capi.NUM_SPLIT_VARIANTS and min(ms) > 0
+    n = _capi.NUM_SPLIT_VARIANTS
+    assert 0 <= chosen < 2 * n and len(ms) == 2 * n and min(ms) > 0
