@@ -181,6 +181,21 @@ def set_pipeline(pipeline: str = DEFAULT_PIPELINE, seg: int = 0, tile: str | int
     c = ctx(device)
     t = TILES[tile] if isinstance(tile, str) else int(tile)
     check(lib().fj_ctx_set_pipeline(c, PIPELINES[pipeline], int(seg), t), "fj_ctx_set_pipeline", c)
+    _PIPELINE_SETTING[_dev_key(device)] = (pipeline, int(seg), t)
+
+
+_PIPELINE_SETTING: dict = {}
+
+
+def _dev_key(device):
+    import torch
+    d = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    return (d.type, d.index if d.index is not None else torch.cuda.current_device())
+
+
+def pipeline_setting(device=None):
+    """(pipeline, seg, tile) last set on the device's context."""
+    return _PIPELINE_SETTING.get(_dev_key(device), (DEFAULT_PIPELINE, 0, 0))
 
 
 def set_adjoint_variant(variant: int = 0, device=None) -> None:

@@ -379,37 +379,6 @@ __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ 
   }
 }
 
-// out = a x + b y + c z (y, z may be null)
-__global__ void k_axpy3(double* __restrict__ out, const double* __restrict__ x, double a,
-                        const double* __restrict__ y, double b, const double* __restrict__ z, double c,
-                        int64_t n) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  double r = a * x[t];
-  if (y) r += b * y[t];
-  if (z) r += c * z[t];
-  out[t] = r;
-}
-
-// *acc += scale * sum(x * y) (FP64 warp-shuffle reduction + one atomic per CTA)
-__global__ void k_dot_acc(const double* __restrict__ x, const double* __restrict__ y, int64_t n,
-                          double scale, double* __restrict__ acc) {
-  __shared__ double sh[32];
-  double s = 0.0;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-    s += x[t] * y[t];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) atomicAdd(acc, scale * s);
-  }
-}
-
 // dJ/dq of J = sum_interior vol * 0.5 |m|^2 / rho
 __global__ void k_ke_grad(const double* __restrict__ q, const double* __restrict__ vol,
                           double* __restrict__ grad, int ni, int nj, int nk, int g) {
@@ -508,25 +477,11 @@ int rhs_vjp(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol,
   return rhs_vjp_impl<double>(ctx, q, kxyz, vol, lam, out, ni, nj, nk, ph, flags, ws, st, dmu, mu_scale, epi);
 }
 
-int dot_acc(fj_ctx* ctx, const double* x, const double* y, int64_t n, double scale, double* acc,
-            cudaStream_t st) {
-  k_dot_acc<<<592, kThreads, 0, st>>>(x, y, n, scale, acc);
-  ctx->launches += 1;
-  return launch_status(ctx, "dot launch");
-}
-
 int ke_grad(fj_ctx* ctx, const double* q, const double* vol, double* grad, int ni, int nj, int nk, int g,
             cudaStream_t st) {
   k_ke_grad<<<grid_for((int64_t)ni * nj * nk), kThreads, 0, st>>>(q, vol, grad, ni, nj, nk, g);
   ctx->launches += 1;
   return launch_status(ctx, "ke grad launch");
-}
-
-int axpy3(fj_ctx* ctx, double* out, const double* x, double a, const double* y, double b,
-          const double* z, double c, int64_t n, cudaStream_t st) {
-  k_axpy3<<<grid_for(n), kThreads, 0, st>>>(out, x, a, y, b, z, c, n);
-  ctx->launches += 1;
-  return launch_status(ctx, "axpy launch");
 }
 
 }  // namespace fj

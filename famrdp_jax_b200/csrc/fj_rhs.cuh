@@ -66,15 +66,9 @@ size_t rhs_vjp_ws_bytes(int precision, int ni, int nj, int nk);
 int rhs_vjp(fj_ctx* ctx, const double* q, const double* kxyz, const double* vol, const double* lam,
             double* out, int ni, int nj, int nk, const fj_params* p, int flags, void* ws,
             cudaStream_t st, double* dmu = nullptr, double mu_scale = 0.0, const VjpEpilogue* epi = nullptr);
-// *acc (device) += scale * dot(x, y)
-int dot_acc(fj_ctx* ctx, const double* x, const double* y, int64_t n, double scale, double* acc,
-            cudaStream_t st);
 // grad = dJ/dq of the interior kinetic-energy integral
 int ke_grad(fj_ctx* ctx, const double* q, const double* vol, double* grad, int ni, int nj, int nk, int g,
             cudaStream_t st);
-// out = a x + b y + c z elementwise (y, z may be null)
-int axpy3(fj_ctx* ctx, double* out, const double* x, double a, const double* y, double b,
-          const double* z, double c, int64_t n, cudaStream_t st);
 // In-place transposes of the halo fill and of the (linear) boundary conditions
 // on per-block adjoint arrays; the blocks' q pointers hold the adjoints.
 int halo_transpose(fj_ctx* ctx, const fj_block* lam, int nblocks, const fj_link* links, int nlinks,

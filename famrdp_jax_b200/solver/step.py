@@ -3,8 +3,12 @@
 ``step(state, cfg, dt)`` keeps the reference's signature and semantics: halo
 fill and boundary conditions once per step, then three Shu-Osher TVD-RK3
 stages over all padded cells of every block, returning a new State with
-t + dt and step + 1 (the input state is not modified).  The whole step is one
-call into libfamrdp_cuda.so (fj_step_f64).
+t + dt and step + 1 (the input state is not modified).  The step runs through
+a prepared plan (fj_plan_*: tables, FP32 metric records and scratch built
+once); step() keeps the plans of the last few (block layout, metrics, cfg)
+combinations it saw, so a time loop of step() calls prepares one plan.  The
+metrics are constants of a plan: arrays changed in place after a step() call
+need a new Metrics object (or an explicit StepPlan).
 """
 from __future__ import annotations
 
@@ -152,9 +156,31 @@ class StepPlan:
             self._handle = None
 
 
+_PLANS: list = []  # (key, cfg, metrics, plan), most recent last
+_MAX_PLANS = 4
+
+
+def _cached_plan(state: State, cfg: Config) -> StepPlan:
+    """The plan for this block layout, these metric arrays, this cfg object
+    (kept alive by the cache entry, so their ids stay unique while cached) and
+    the context's current pipeline setting."""
+    dev = state.blocks[0].q.device
+    key = (id(cfg), id(state.metrics), tuple((tuple(b.q.shape), str(b.q.device)) for b in state.blocks),
+           tuple((m.kxyz.data_ptr(), m.vol.data_ptr()) for m in state.metrics), _capi.pipeline_setting(dev))
+    for n, (k, _, _, plan) in enumerate(_PLANS):
+        if k == key:
+            _PLANS.append(_PLANS.pop(n))
+            return plan
+    plan = StepPlan(state, cfg)
+    _PLANS.append((key, cfg, state.metrics, plan))
+    if len(_PLANS) > _MAX_PLANS:
+        _PLANS.pop(0)
+    return plan
+
+
 def step(state: State, cfg: Config, dt: float, *, plan: StepPlan | None = None) -> State:
     """Advance by dt with TVD-RK3 (solver/step.py:18-56)."""
-    plan = plan or StepPlan(state, cfg)
+    plan = plan or _cached_plan(state, cfg)
     qs = [b.q for b in state.blocks]
     outs = [torch.empty_like(q) for q in qs]
     plan.run(qs, outs, dt)
