@@ -272,7 +272,27 @@ def test_metrics_uniform_cube(cuda_device):
 
 
 # ---------------------------------------------------------------- step
+def _rel_per_variable(got, ref, g=2):
+    """Relative L2 per conserved variable over the full padded blocks and over
+    the interiors (all blocks together)."""
+    out = {}
+    for part in ("full", "interior"):
+        for v in range(5):
+            num = den = 0.0
+            for a, b in zip(got, ref):
+                x, y = a[v], b[v]
+                if part == "interior":
+                    x, y = x[g:-g, g:-g, g:-g], y[g:-g, g:-g, g:-g]
+                num += float(np.sum((x - y) ** 2))
+                den += float(np.sum(y ** 2))
+            out[(part, v)] = (num / den) ** 0.5 if den > 0 else num ** 0.5
+    return out
+
+
 def _run_steps(case, nsteps, dt, tol_fp64=1e-12):
+    """nsteps GPU steps against the oracle's: returns the whole-state relative
+    L2 after every step; for FP64 also checks every variable, full and interior,
+    against tol_fp64 after every step."""
     st = state_from_case(case)
     qs = [q.copy() for q in case.qs]
     mets = [(m[1], m[2]) for m in case.metrics]
@@ -280,7 +300,12 @@ def _run_steps(case, nsteps, dt, tol_fp64=1e-12):
     for _ in range(nsteps):
         st = step(st, case.cfg, dt)
         qs = NP.step(qs, mets, case.cfg, dt)
-        errs.append(max(rel_l2(host(b.q), r) for b, r in zip(st.blocks, qs)))
+        got = [host(b.q) for b in st.blocks]
+        errs.append(max(rel_l2(a, r) for a, r in zip(got, qs)))
+        if getattr(case.cfg, "precision", "f64") == "f64":
+            per = _rel_per_variable(got, qs)
+            worst = max(per.values())
+            assert worst <= tol_fp64, {k: v for k, v in per.items() if v > tol_fp64}
     return errs, st
 
 
