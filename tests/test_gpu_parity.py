@@ -497,3 +497,50 @@ def test_autotune_launch_shapes_agree(cuda_device):
     chosen, ms = plan.autotune(qs, [torch.empty_like(q) for q in qs], dt, reps=2)
     n = _capi.NUM_SPLIT_VARIANTS
     assert 0 <= chosen < 2 * n and len(ms) == 2 * n and min(ms) > 0
+
+
+def test_plan_argument_errors(cuda_device):
+    """The plan entry points reject bad arguments with the mapped exceptions
+    and leave the plan usable."""
+    import ctypes
+    import dataclasses
+    from famrdp_jax_b200 import _capi
+    from famrdp_jax_b200.solver import adjoint
+    from famrdp_jax_b200.solver.step import StepPlan
+    c = cases.tree24(nblocks=2, lo=6, hi=9, seed=4)
+    cfg = dataclasses.replace(c.cfg, precision="f32")
+    st = state_from_case(c)
+    dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], cfg.gas.gamma, c.cfl, 2)
+    plan = StepPlan(st, cfg)
+    qs = [b.q for b in st.blocks]
+    with pytest.raises(ValueError):
+        plan.set_variant(_capi.NUM_SPLIT_VARIANTS)
+    with pytest.raises(ValueError):
+        plan.set_variant(-1)
+    with pytest.raises(ValueError):
+        plan.set_streams(3)
+    with pytest.raises(ValueError):
+        plan.set_ensemble([1e-3])  # one value for two blocks
+    with pytest.raises(ValueError):
+        plan.set_ensemble(None, [1e-3, -1.0])
+    with pytest.raises(ValueError):
+        plan.run(qs, [torch.empty((5, 3, 3, 3), dtype=torch.float64, device="cuda")] * 2, dt)
+    lib = _capi.lib()
+    ch = ctypes.c_int()
+    assert lib.fj_plan_autotune(plan._handle, _topology_ptrs(qs), _topology_ptrs(qs), dt, 0, ctypes.byref(ch),
+                                None, None) == _capi.FJ_ERR_INVALID_ARGUMENT
+    # still usable
+    out = [torch.empty_like(q) for q in qs]
+    plan.run(qs, out, dt)
+    assert all(torch.isfinite(o).all() for o in out)
+    # the ensemble adjoint wants one dJ/dmu0 slot per block
+    saved = tuple([torch.empty_like(q) for q in qs] for _ in range(3))
+    plan.run_save(qs, out, *saved, dt)
+    with pytest.raises(ValueError):
+        adjoint.step_vjp_saved(saved, st.metrics, cfg, dt, [torch.ones_like(q) for q in qs],
+                               dmu=torch.zeros(1, dtype=torch.float64, device="cuda"), mu0s=[1e-3, 1e-3])
+
+
+def _topology_ptrs(qs):
+    from famrdp_jax_b200 import _topology
+    return _topology.ptr_array(qs)
