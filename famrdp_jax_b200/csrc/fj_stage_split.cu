@@ -759,15 +759,41 @@ __global__ void k_metric_records(const double* __restrict__ kxyz, T* __restrict_
   st_rec<T, kRecK<T>>(out + c * kRecK<T>, rec);
 }
 
-__global__ void k_pressure_sum(const double* __restrict__ q, int64_t N, double gm1, double* __restrict__ acc) {
+// Sum of (pressure) over a block, one partial per CTA (fixed grid, fixed
+// summation order: the result does not depend on scheduling).
+constexpr int kPsumCtas = 592, kPsumThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;
+}
+
+__global__ void k_pressure_partial(const double* __restrict__ q, int64_t N, double gm1, double* __restrict__ part) {
+  __shared__ double sh[32];
   double s = 0.0;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N; c += (int64_t)gridDim.x * blockDim.x) {
     const double r = q[c], u = q[N + c] / r, v = q[2 * N + c] / r, w = q[3 * N + c] / r;
     s += gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(acc, s);
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_fold_sum(const double* __restrict__ part, int n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) s += part[t];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) *out = s;
 }
 
 // Launch shapes of the FP32 record kernels, selected per plan by the
@@ -862,21 +888,22 @@ int split_metric_records(const double* kxyz, void* out, int ni, int nj, int nk, 
 }
 
 int mean_pressure(const fj_block* blocks, int nblocks, double gm1, double* out) {
-  double* acc = nullptr;
-  if (cudaMalloc(&acc, sizeof(double)) != cudaSuccess) {
+  double* part = nullptr;
+  const size_t n = (size_t)kPsumCtas * nblocks;
+  if (cudaMalloc(&part, (n + 1) * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();
     return FJ_ERR_NO_MEMORY;
   }
-  cudaMemsetAsync(acc, 0, sizeof(double), nullptr);
   int64_t cells = 0;
   for (int b = 0; b < nblocks; ++b) {
     const int64_t N = (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
     cells += N;
-    k_pressure_sum<<<592, 256, 0, nullptr>>>(blocks[b].q, N, gm1, acc);
+    k_pressure_partial<<<kPsumCtas, kPsumThreads, 0, nullptr>>>(blocks[b].q, N, gm1, part + (size_t)b * kPsumCtas);
   }
+  k_fold_sum<<<1, 1024, 0, nullptr>>>(part, (int)n, part + n);
   double h = 0.0;
-  const cudaError_t e = cudaMemcpy(&h, acc, sizeof(double), cudaMemcpyDeviceToHost);
-  cudaFree(acc);
+  const cudaError_t e = cudaMemcpy(&h, part + n, sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(part);
   if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return FJ_ERR_CUDA;
   *out = cells > 0 ? h / (double)cells : 0.0;
   return FJ_OK;

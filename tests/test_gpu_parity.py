@@ -566,3 +566,22 @@ def test_host_stepper_matches_step(cuda_device):
         ref = step(s_i, c.cfg, dt, plan=plan)
         for h, b in zip(outs[i], ref.blocks):
             assert torch.equal(h, b.q.cpu()), i
+
+
+def test_plans_are_reproducible(cuda_device):
+    """Two plans made from the same state give bit-identical FP32-flux steps
+    (the plan's pressure offset comes from a fixed-order reduction)."""
+    import dataclasses
+    from famrdp_jax_b200.solver.step import StepPlan
+    c = cases.tree24(nblocks=5, lo=8, hi=14, seed=7)
+    cfg = dataclasses.replace(c.cfg, precision="f32")
+    st = state_from_case(c)
+    dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], cfg.gas.gamma, c.cfl, 2)
+    outs = []
+    for _ in range(2):
+        plan = StepPlan(st, cfg)
+        o = [torch.empty_like(b.q) for b in st.blocks]
+        plan.run([b.q for b in st.blocks], o, dt)
+        outs.append(o)
+    for a, b in zip(*outs):
+        assert torch.equal(a, b)
