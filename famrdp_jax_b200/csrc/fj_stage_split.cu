@@ -98,6 +98,7 @@ __device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x) {
 
 // ---- record access -------------------------------------------------------
 constexpr int kRecP = 8, kRecF = 16, kRecG = 8;  // G: 8 components per record + 1 in Gz
+constexpr int kRecP64 = 6;  // FP64 primitive record: rho, u, v, w, p, T (48 bytes)
 
 // Minimum resident CTAs per SM (register caps): FP64 face arithmetic needs
 // more registers than FP32 at the same occupancy.
@@ -455,9 +456,10 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
 }
 
 // ---- field-major variant (the FP64 path) ----------------------------------
-// The FP64 path keeps its intermediates field-major (6 + 15 + 9 arrays of N):
-// 16-byte records would cost it more registers (two doubles per vector lane)
-// and padding bytes than the index arithmetic they save.
+// The FP64 path keeps its primitives as 48-byte records (three 16-byte loads
+// per neighbour) and its face and viscous fluxes field-major (15 + 9 arrays of
+// N): flux records would cost FP64 more registers (two doubles per vector
+// lane) and padding bytes than the index arithmetic they save.
 namespace fm {
 
 template <typename T>
@@ -474,13 +476,8 @@ __global__ void __launch_bounds__(kSplitThreads) k_fm_prims(const Table tab, con
   const double u = q[N + c] * ir, v = q[2 * N + c] * ir, w = q[3 * N + c] * ir;
   const double p = gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
   const double Tt = r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300;
-  T* P = (T*)B.prim;
-  P[c] = (T)r;
-  P[N + c] = (T)u;
-  P[2 * N + c] = (T)v;
-  P[3 * N + c] = (T)w;
-  P[4 * N + c] = (T)p;
-  P[5 * N + c] = (T)Tt;
+  const T rec[kRecP64] = {(T)r, (T)u, (T)v, (T)w, (T)p, (T)Tt};
+  st_rec<T, kRecP64>((T*)B.prim + c * kRecP64, rec);
 }
 
 template <typename T>
@@ -496,14 +493,10 @@ struct Cell6 {
 
 template <typename T, bool WITH_T>
 __device__ __forceinline__ Cell6<T> load_cell(const T* __restrict__ P, int32_t N, int32_t c) {
-  Cell6<T> x;
-  x.r = P[c];
-  x.u = P[N + c];
-  x.v = P[2 * N + c];
-  x.w = P[3 * N + c];
-  x.p = P[4 * N + c];
-  x.t = WITH_T ? P[5 * N + c] : T(0);
-  return x;
+  (void)N;
+  T x[kRecP64];
+  ld_rec<T, kRecP64>(P + (size_t)c * kRecP64, x);
+  return Cell6<T>{x[0], x[1], x[2], x[3], x[4], WITH_T ? x[5] : T(0)};
 }
 
 // Roe face c | c+e_a from the primitives of c-e_a, c, c+e_a, c+2e_a and the
@@ -717,9 +710,10 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table ta
     if (next_prims) {
       double pv[6];
       prims_of(qn, gm1, R, pv);
-      T* P = (T*)B.prim;
+      T rec[kRecP64];
 #pragma unroll
-      for (int v = 0; v < 6; ++v) P[v * N + c] = (T)pv[v];
+      for (int v = 0; v < kRecP64; ++v) rec[v] = (T)pv[v];
+      st_rec<T, kRecP64>((T*)B.prim + c * kRecP64, rec);
     }
   }
 }
@@ -918,7 +912,7 @@ size_t split_metric_record_bytes(int precision, int64_t N) {
 // arrays (FP64).
 static void split_counts(int precision, int& nP, int& nF, int& nG) {
   const bool rec = precision == FJ_PREC_F32FLUX;
-  nP = rec ? kRecP : 6;
+  nP = rec ? kRecP : kRecP64;
   nF = rec ? kRecF : 15;
   nG = 9;  // records: kRecG per cell in G, then one per cell in Gz
 }
