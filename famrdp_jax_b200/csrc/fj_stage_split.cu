@@ -100,6 +100,89 @@ __device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x) {
 constexpr int kRecP = 8, kRecF = 16, kRecG = 8;  // G: 8 components per record + 1 in Gz
 constexpr int kRecP64 = 6;  // FP64 primitive record: rho, u, v, w, p, T (48 bytes)
 
+// Starts an L2 fill of the bytes [p, p + n) of one contiguous range, clipped
+// inward to 16-byte boundaries so that nothing outside the range is touched.
+// Issued by one thread for a CTA's whole cell range, it puts every stream the
+// CTA will read in flight at once; the threads' own loads then hit L2 (or
+// join the fill) instead of each waiting for DRAM in turn.
+__device__ __forceinline__ void l2_prefetch(const void* p, int64_t n) {
+  const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+  const uintptr_t e = ((uintptr_t)p + n) & ~(uintptr_t)15;
+  if (e > a)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
+// The L2 fills of the flux CTA `cta` of block d (thread 0 only): the
+// primitives two i-planes ahead (MUSCL's farthest upwind cell) and the
+// metrics one i-plane ahead (the right cell of the i-face); nearer ranges were
+// fetched by earlier CTAs.  FIELD: the FP64 path (48-byte primitive records,
+// FP64 field-major kxyz).
+template <typename T, bool K_AOS, bool FIELD>
+__device__ __forceinline__ void prefetch_fluxes(const Dev& d, int cta) {
+  const SplitBlock& B = d.blk;
+  const int64_t N = (int64_t)B.ni * B.nj * B.nk, si = (int64_t)B.nj * B.nk;
+  const int64_t c0 = (int64_t)(cta - B.cta_begin) * kSplitThreads;
+  const int64_t n = min((int64_t)kSplitThreads, N - c0);
+  const int64_t a2 = c0 + 2 * si, m2 = min(n, N - a2);
+  const int rec = FIELD ? kRecP64 : kRecP;
+  if (m2 > 0) l2_prefetch((const T*)B.prim + a2 * rec, m2 * rec * (int64_t)sizeof(T));
+  const int64_t a1 = c0 + si, m1 = min(n, N - a1);
+  if (m1 > 0) {
+    if (K_AOS && !FIELD)
+      l2_prefetch((const T*)B.kaos + a1 * kRecK<T>, m1 * kRecK<T> * (int64_t)sizeof(T));
+    else
+      for (int lm = 0; lm < 9; ++lm) l2_prefetch(B.kxyz + lm * N + a1, m1 * 8);
+  }
+}
+
+// The L2 fill of the state range of primitive CTA `cta` (thread 0 only).
+__device__ __forceinline__ void prefetch_state(const Dev& d, int cta) {
+  const SplitBlock& B = d.blk;
+  const int64_t N = (int64_t)B.ni * B.nj * B.nk;
+  const int64_t c0 = (int64_t)(cta - B.cta_begin) * kSplitThreads;
+  const int64_t n = min((int64_t)kSplitThreads, N - c0);
+  for (int v = 0; v < 5; ++v) l2_prefetch(B.q + v * N + c0, n * 8);
+}
+
+// The L2 fills of the assembly CTA `cta` of block d (thread 0 only): its own
+// range of q, q0, vol, metrics and face fluxes, and the viscous components
+// one i-plane ahead (the ones behind were fetched by earlier CTAs).  FIELD:
+// field-major intermediates and FP64 kxyz (the FP64 path), else records.
+template <typename T, bool K_AOS, bool FIELD>
+__device__ __forceinline__ void prefetch_assembly(const Dev& d, int cta, int flags, int stage) {
+  const SplitBlock& B = d.blk;
+  const int64_t N = (int64_t)B.ni * B.nj * B.nk;
+  const int64_t c0 = (int64_t)(cta - B.cta_begin) * kSplitThreads;
+  const int64_t n = min((int64_t)kSplitThreads, N - c0);
+  if (n <= 0) return;
+  if (stage != 0)
+    for (int v = 0; v < 5; ++v) l2_prefetch(B.q + v * N + c0, n * 8);
+  if (stage == 2 || stage == 3)
+    for (int v = 0; v < 5; ++v) l2_prefetch(B.q0 + v * N + c0, n * 8);
+  const int64_t a = c0 + (int64_t)B.nj * B.nk, m = min(n, N - a);
+  if (FIELD) {
+    if (flags & kRhsInvscd) {
+      l2_prefetch(B.vol + c0, n * 8);
+      for (int v = 0; v < 15; ++v) l2_prefetch((const T*)B.F + v * N + c0, n * (int64_t)sizeof(T));
+    }
+    if (flags & kRhsViscous) {
+      for (int lm = 0; lm < 9; ++lm) l2_prefetch(B.kxyz + lm * N + c0, n * 8);
+      if (m > 0)
+        for (int v = 0; v < 9; ++v) l2_prefetch((const T*)B.G + v * N + a, m * (int64_t)sizeof(T));
+    }
+  } else {
+    if (K_AOS) l2_prefetch((const T*)B.kaos + c0 * kRecK<T>, n * kRecK<T> * (int64_t)sizeof(T));
+    if (flags & kRhsInvscd) {
+      l2_prefetch(B.vol + c0, n * 8);
+      l2_prefetch((const T*)B.F + c0 * kRecF, n * kRecF * (int64_t)sizeof(T));
+    }
+    if ((flags & kRhsViscous) && m > 0) {
+      l2_prefetch((const T*)B.G + a * kRecG, m * kRecG * (int64_t)sizeof(T));
+      l2_prefetch((const T*)B.Gz + a, m * (int64_t)sizeof(T));
+    }
+  }
+}
+
 // Minimum resident CTAs per SM (register caps): FP64 face arithmetic needs
 // more registers than FP32 at the same occupancy.
 template <typename T>
@@ -210,6 +293,7 @@ template <typename T>
 __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, const double gm1,
                                                               const double R, const double p_ref) {
   const int b = find_block(tab, blockIdx.x);
+  if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
   const SplitBlock& B = tab.b[b].blk;
   const int32_t N = B.ni * B.nj * B.nk;
   const int32_t c = (blockIdx.x - B.cta_begin) * kSplitThreads + threadIdx.x;
@@ -240,6 +324,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
                                                                                    const int flags) {
   using M = FastMath<T>;
   const int b = find_block(tab, blockIdx.x);
+  if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x);
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
@@ -448,6 +533,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
                                                                        const double gm1, const double R,
                                                                        const double ph_p_ref) {
   const int b = find_block(tab, blockIdx.x);
+  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(tab.b[b], blockIdx.x, flags, stage);
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
@@ -466,6 +552,7 @@ template <typename T>
 __global__ void __launch_bounds__(kSplitThreads) k_fm_prims(const Table tab, const double gm1,
                                                               const double R) {
   const int b = find_block(tab, blockIdx.x);
+  if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
   const SplitBlock& B = tab.b[b].blk;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
   const int64_t c = (int64_t)(blockIdx.x - B.cta_begin) * kSplitThreads + threadIdx.x;
@@ -524,6 +611,7 @@ __global__ void __launch_bounds__(kSplitThreads, 2) k_fm_fluxes(const Table tab,
                                                                const int flags) {
   using M = FastMath<T>;
   const int b = find_block(tab, blockIdx.x);
+  if (threadIdx.x == 0) prefetch_fluxes<T, false, true>(tab.b[b], blockIdx.x);
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
@@ -625,6 +713,7 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table ta
                                                                  const double gm1, const double R) {
   const int b = find_block(tab, blockIdx.x);
   Cell x;
+  if (threadIdx.x == 0) prefetch_assembly<T, false, true>(tab.b[b], blockIdx.x, flags, stage);
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
   const int64_t N = x.N, c = x.c;
