@@ -194,7 +194,15 @@ struct SplitOcc {
 // n values of a 16-byte aligned record (n a multiple of 16 / sizeof(T)).
 template <typename T, int n>
 __device__ __forceinline__ void ld_rec(const T* __restrict__ p, T* v) {
-  if constexpr (sizeof(T) == 4) {
+  if constexpr (sizeof(T) == 4 && n % 8 == 0) {
+    // 32-byte records (32-byte aligned): one 256-bit load per 8 floats
+#pragma unroll
+    for (int i = 0; i < n / 8; ++i)
+      asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+          : "=f"(v[8 * i]), "=f"(v[8 * i + 1]), "=f"(v[8 * i + 2]), "=f"(v[8 * i + 3]), "=f"(v[8 * i + 4]),
+            "=f"(v[8 * i + 5]), "=f"(v[8 * i + 6]), "=f"(v[8 * i + 7])
+          : "l"(p + 8 * i));
+  } else if constexpr (sizeof(T) == 4) {
 #pragma unroll
     for (int i = 0; i < n / 4; ++i) {
       const float4 x = __ldg(reinterpret_cast<const float4*>(p) + i);
@@ -215,7 +223,15 @@ __device__ __forceinline__ void ld_rec(const T* __restrict__ p, T* v) {
 
 template <typename T, int n>
 __device__ __forceinline__ void st_rec(T* __restrict__ p, const T* v) {
-  if constexpr (sizeof(T) == 4) {
+  if constexpr (sizeof(T) == 4 && n % 8 == 0) {
+    // one 256-bit store per 8 floats: whole 32-byte sectors per instruction
+#pragma unroll
+    for (int i = 0; i < n / 8; ++i)
+      asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p + 8 * i), "f"(v[8 * i]),
+                   "f"(v[8 * i + 1]), "f"(v[8 * i + 2]), "f"(v[8 * i + 3]), "f"(v[8 * i + 4]), "f"(v[8 * i + 5]),
+                   "f"(v[8 * i + 6]), "f"(v[8 * i + 7])
+                   : "memory");
+  } else if constexpr (sizeof(T) == 4) {
 #pragma unroll
     for (int i = 0; i < n / 4; ++i)
       reinterpret_cast<float4*>(p)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
@@ -421,7 +437,22 @@ struct GlobalSrc {
   const SplitBlock& B;
   int32_t N;
   __device__ __forceinline__ void F_rec(int32_t c, T* o) const { ld_rec<T, kRecF>((const T*)B.F + (size_t)c * kRecF, o); }
-  __device__ __forceinline__ T F_val(int32_t c, int off) const { return ((const T*)B.F)[(size_t)c * kRecF + off]; }
+  // the five components of face a of the record of cell c (floats 5a..5a+4),
+  // as two aligned 16-byte loads
+  __device__ __forceinline__ void F_axis(int32_t c, int a, T* o) const {
+    const T* p = (const T*)B.F + (size_t)c * kRecF;
+    if constexpr (sizeof(T) == 4) {
+      const int q = (5 * a) >> 2, s = (5 * a) & 3;  // first float4 and the offset in it
+      const float4 x = __ldg(reinterpret_cast<const float4*>(p) + q);
+      const float4 y = __ldg(reinterpret_cast<const float4*>(p) + q + 1);
+      const float w[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+#pragma unroll
+      for (int v = 0; v < 5; ++v) o[v] = w[s + v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) o[v] = p[5 * a + v];
+    }
+  }
   __device__ __forceinline__ void G_rec(int32_t c, T* o) const { ld_rec<T, kRecG>((const T*)B.G + (size_t)c * kRecG, o); }
   __device__ __forceinline__ void K9(int32_t c, T* kk, T* gcl) const { metric9<T, K_AOS>(B, N, c, kk, gcl); }
 };
@@ -452,9 +483,14 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
       const double pg[3] = {ph_p_ref * (double)gcl[0], ph_p_ref * (double)gcl[1], ph_p_ref * (double)gcl[2]};
       T Fm[3][5];
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+      for (int a = 0; a < 3; ++a) {
+        if (on[a]) {
+          src.F_axis(c - st[a], a, Fm[a]);
+        } else {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) Fm[a][v] = on[a] ? src.F_val(c - st[a], 5 * a + v) : T(0);
+          for (int v = 0; v < 5; ++v) Fm[a][v] = T(0);
+        }
+      }
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
         double dsum;
