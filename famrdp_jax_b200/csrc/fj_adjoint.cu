@@ -130,6 +130,19 @@ __global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, c
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int n_a = a == 0 ? d.ni : (a == 1 ? d.nj : d.nk);
   const int sa = a == 0 ? d.nj * d.nk : (a == 1 ? d.nk : 1);
+  if (threadIdx.x == 0) {
+    // L2 fills of the ranges this CTA reaches first: lam, vol and the metric
+    // row one cell ahead along a, the primitives two ahead
+    const int c0 = blockIdx.x * blockDim.x, n = min((int)blockDim.x, N - c0);
+    const int a1 = c0 + sa, m1 = min(n, N - a1), a2 = c0 + 2 * sa, m2 = min(n, N - a2);
+    if (m1 > 0) {
+      for (int v = 0; v < 5; ++v) l2_prefetch(lam + (size_t)v * N + a1, m1 * 8);
+      l2_prefetch(vol + a1, m1 * 8);
+      for (int m = 0; m < 3; ++m) l2_prefetch(kxyz + (size_t)(3 * a + m) * N + a1, m1 * 8);
+    }
+    if (m2 > 0)
+      for (int v = 0; v < 5; ++v) l2_prefetch(P + (size_t)v * N + a2, m2 * (int)sizeof(T));
+  }
   T lc[4][5];
 #pragma unroll
   for (int s = 0; s < 4; ++s)
@@ -297,6 +310,16 @@ __global__ void __launch_bounds__(kAT, MB) k_adj_visc(const T* __restrict__ P, c
                                                      double* __restrict__ dmu, double mu_scale) {
   const int N = d.ni * d.nj * d.nk;
   const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (threadIdx.x == 0) {
+    // L2 fills one i-plane ahead (nearer neighbours were fetched by earlier CTAs)
+    const int a1 = blockIdx.x * blockDim.x + d.nj * d.nk, m1 = min((int)blockDim.x, N - a1);
+    if (m1 > 0) {
+      for (int v = 1; v < 5; ++v) l2_prefetch(lam + (size_t)v * N + a1, m1 * 8);
+      for (int lm = 0; lm < 9; ++lm) l2_prefetch(kxyz + (size_t)lm * N + a1, m1 * 8);
+      const int fld[4] = {1, 2, 3, 5};
+      for (int s = 0; s < 4; ++s) l2_prefetch(P + (size_t)fld[s] * N + a1, m1 * (int)sizeof(T));
+    }
+  }
   double dot = 0.0;
   if (y < N) dot = adj_visc_cell<T>(P, kxyz, lam, lamD, lamL, d, ph, y, dmu != nullptr);
   if (dmu) {  // warp reduction (all lanes take part), one atomic per warp
@@ -313,6 +336,23 @@ __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ 
   const int N = d.ni * d.nj * d.nk;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= N) return;
+  if (threadIdx.x == 0) {
+    // L2 fills of this CTA's own ranges, and of lamD one i-plane ahead
+    const int c0 = x, n = min((int)blockDim.x, N - c0);
+    const int a1 = c0 + d.nj * d.nk, m1 = min(n, N - a1);
+    for (int f = 0; f < 5; ++f) l2_prefetch(q + (size_t)f * N + c0, n * 8);
+    if (flags & kRhsInvscd)
+      for (int f = 0; f < 5; ++f) l2_prefetch(lamP + (size_t)f * N + c0, n * (int)sizeof(T));
+    if (flags & kRhsViscous) {
+      for (int s = 0; s < 4; ++s) l2_prefetch(lamL + (size_t)s * N + c0, n * (int)sizeof(T));
+      if (m1 > 0)
+        for (int f = 0; f < 12; ++f) l2_prefetch(lamD + (size_t)f * N + a1, m1 * (int)sizeof(T));
+    }
+    const double* ep[4] = {e.x1, e.y1, e.x2, e.y2};
+    for (int t = 0; t < 4; ++t)
+      if ((t < 2 ? e.o1 : e.o2) && ep[t])
+        for (int f = 0; f < 5; ++f) l2_prefetch(ep[t] + (size_t)f * N + c0, n * 8);
+  }
   double lr = 0, lu = 0, lv = 0, lw = 0, lp = 0, lT = 0;
   if (flags & kRhsInvscd) {
     lr = lamP[x];

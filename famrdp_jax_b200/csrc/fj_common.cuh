@@ -172,4 +172,16 @@ inline Phys make_phys(const fj_params* p) {
   return f;
 }
 
+// Starts an L2 fill of the bytes [p, p + n) of one contiguous range, clipped
+// inward to 16-byte boundaries so that nothing outside the range is touched.
+// Issued by one thread for a CTA's whole cell range, it puts every stream the
+// CTA will read in flight at once; the threads' own loads then hit L2 (or
+// join the fill) instead of each waiting for DRAM in turn.
+__device__ __forceinline__ void l2_prefetch(const void* p, int64_t n) {
+  const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+  const uintptr_t e = ((uintptr_t)p + n) & ~(uintptr_t)15;
+  if (e > a)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
 }  // namespace fj

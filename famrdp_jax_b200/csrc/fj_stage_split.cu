@@ -100,18 +100,6 @@ __device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x) {
 constexpr int kRecP = 8, kRecF = 16, kRecG = 8;  // G: 8 components per record + 1 in Gz
 constexpr int kRecP64 = 6;  // FP64 primitive record: rho, u, v, w, p, T (48 bytes)
 
-// Starts an L2 fill of the bytes [p, p + n) of one contiguous range, clipped
-// inward to 16-byte boundaries so that nothing outside the range is touched.
-// Issued by one thread for a CTA's whole cell range, it puts every stream the
-// CTA will read in flight at once; the threads' own loads then hit L2 (or
-// join the fill) instead of each waiting for DRAM in turn.
-__device__ __forceinline__ void l2_prefetch(const void* p, int64_t n) {
-  const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15;
-  const uintptr_t e = ((uintptr_t)p + n) & ~(uintptr_t)15;
-  if (e > a)
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
-}
-
 // The L2 fills of the flux CTA `cta` of block d (thread 0 only): the
 // primitives two i-planes ahead (MUSCL's farthest upwind cell) and the
 // metrics one i-plane ahead (the right cell of the i-face); nearer ranges were
