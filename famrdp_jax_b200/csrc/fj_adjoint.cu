@@ -57,11 +57,23 @@ __device__ __forceinline__ void wrapped(int c, int i, int j, int k, const ADims&
   nb[5] = k == 0 ? c + (d.nk - 1) : c - 1;
 }
 
+// With lv, also lv = lam / (vol + 1e-300) per cell, in FP64: the face adjoint
+// -lam(c)/vol(c) + lam(c+e_a)/vol(c+e_a) of every axis then costs one FP64
+// subtraction per face instead of two divisions.
 template <typename T>
 __global__ void k_adj_prims(const double* __restrict__ q, T* __restrict__ P, int N, double gm1,
-                            double R) {
+                            double R, const double* __restrict__ lam, const double* __restrict__ vol,
+                            double* __restrict__ lv, T* __restrict__ lamP) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= N) return;
+  if (lamP)  // cleared here for the face kernel's atomic sums
+#pragma unroll
+    for (int v = 0; v < 5; ++v) lamP[v * N + c] = T(0);
+  if (lv) {
+    const double iv = 1.0 / (vol[c] + 1e-300);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) lv[v * N + c] = lam[v * N + c] * iv;
+  }
   const double r = q[c], ir = 1.0 / r;
   const double u = q[N + c] * ir, v = q[2 * N + c] * ir, w = q[3 * N + c] * ir;
   const double p = gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
@@ -122,8 +134,8 @@ __device__ __forceinline__ void add_cell(T* __restrict__ lamP, int N, int c, con
 // cells' adjoints atomically.
 template <typename T, int NT, int MB>
 __global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, const double* __restrict__ kxyz,
-                                                      const double* __restrict__ vol, const double* __restrict__ lam,
-                                                      T* __restrict__ lamP, ADims d, Phys ph) {
+                                                      const double* __restrict__ lv, T* __restrict__ lamP, ADims d,
+                                                      Phys ph) {
   const int N = d.ni * d.nj * d.nk;
   if (blockIdx.x * blockDim.x >= (unsigned)N) return;  // whole block past the end (uniform)
   const int a = blockIdx.y;
@@ -131,13 +143,12 @@ __global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, c
   const int n_a = a == 0 ? d.ni : (a == 1 ? d.nj : d.nk);
   const int sa = a == 0 ? d.nj * d.nk : (a == 1 ? d.nk : 1);
   if (threadIdx.x == 0) {
-    // L2 fills of the ranges this CTA reaches first: lam, vol and the metric
+    // L2 fills of the ranges this CTA reaches first: lam/vol and the metric
     // row one cell ahead along a, the primitives two ahead
     const int c0 = blockIdx.x * blockDim.x, n = min((int)blockDim.x, N - c0);
     const int a1 = c0 + sa, m1 = min(n, N - a1), a2 = c0 + 2 * sa, m2 = min(n, N - a2);
     if (m1 > 0) {
-      for (int v = 0; v < 5; ++v) l2_prefetch(lam + (size_t)v * N + a1, m1 * 8);
-      l2_prefetch(vol + a1, m1 * 8);
+      for (int v = 0; v < 5; ++v) l2_prefetch(lv + (size_t)v * N + a1, m1 * 8);
       for (int m = 0; m < 3; ++m) l2_prefetch(kxyz + (size_t)(3 * a + m) * N + a1, m1 * 8);
     }
     if (m2 > 0)
@@ -153,13 +164,11 @@ __global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, c
     if (ia >= 1 && ia <= n_a - 3) {
       const bool inL = ia >= 2, inR = ia + 1 <= n_a - 3;
       const int cr = c + sa;
-      const double ivl = inL ? 1.0 / (vol[c] + 1e-300) : 0.0;
-      const double ivr = inR ? 1.0 / (vol[cr] + 1e-300) : 0.0;
       T lF[5];
       bool any = false;
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const double x = (inL ? -lam[v * N + c] * ivl : 0.0) + (inR ? lam[v * N + cr] * ivr : 0.0);
+        const double x = (inL ? -lv[v * N + c] : 0.0) + (inR ? lv[v * N + cr] : 0.0);
         lF[v] = (T)x;
         any |= x != 0.0;
       }
@@ -443,7 +452,7 @@ __global__ void k_ke_grad(const double* __restrict__ q, const double* __restrict
 
 template <typename T>
 size_t vjp_ws(int64_t N) {
-  return ((6 + 5 + 12 + 4) * (size_t)N) * sizeof(T) + 4 * 256;
+  return ((6 + 5 + 12 + 4) * (size_t)N) * sizeof(T) + 5 * (size_t)N * sizeof(double) + 5 * 256;
 }
 
 template <typename T>
@@ -460,19 +469,20 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
   T* lamD = (T*)p;
   p = al(p + 12 * (size_t)N * sizeof(T));
   T* lamL = (T*)p;
+  p = al(p + 4 * (size_t)N * sizeof(T));
+  double* lv = (double*)p;
   const ADims d{ni, nj, nk};
   const int grid = grid_for(N, kAT);
-  k_adj_prims<T><<<grid, kAT, 0, st>>>(q, P, N, ph.gm1, ph.R);
+  const bool inv = (flags & kRhsInvscd) != 0;
+  k_adj_prims<T><<<grid, kAT, 0, st>>>(q, P, N, ph.gm1, ph.R, lam, vol, inv ? lv : nullptr, inv ? lamP : nullptr);
   ctx->launches += 1;
   if (flags & kRhsInvscd) {
-    cudaError_t e = cudaMemsetAsync(lamP, 0, 5 * (size_t)N * sizeof(T), st);
-    if (e != cudaSuccess) return cuda_status(ctx, e, "vjp memset");
     // register caps (threads per CTA, minimum CTAs per SM): the FP64 face VJP
     // needs ~180 registers uncapped.  Variant 0 is the fastest measured on
     // B200 (TGV 96^3 adjoint sweep): FP64 128 x 4 (128 registers), FP32
     // 256 x 3 (80 registers, a few spilled values)
     auto launch = [&](auto kern, int nt) {
-      kern<<<dim3((unsigned)((N + nt - 1) / nt), 3), nt, 0, st>>>(P, kxyz, vol, lam, lamP, d, ph);
+      kern<<<dim3((unsigned)((N + nt - 1) / nt), 3), nt, 0, st>>>(P, kxyz, lv, lamP, d, ph);
     };
     constexpr bool f64 = sizeof(T) == 8;
     switch (ctx->adj_variant) {

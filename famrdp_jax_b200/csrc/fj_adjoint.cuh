@@ -268,7 +268,7 @@ __device__ __forceinline__ void roe_prim_vjp(const Prim<T>& L, const Prim<T>& R,
   lvh += lunh * n1;
   lwh += lunh * n2;
   // ic2 = 1/c2; ch = sqrt(c2); c2 = max(c2r, tiny)
-  T lc2 = -lic2 * ic2 * ic2 + lch * h / ch;
+  T lc2 = -lic2 * ic2 * ic2 + lch * h * (ch * ic2);  // 1/ch = ch / c2
   const T lc2r = cc2 ? lc2 : T(0);
   // c2r = gm1 (Hh - 0.5 q2)
   lHh += gm1 * lc2r;
@@ -297,8 +297,8 @@ __device__ __forceinline__ void roe_prim_vjp(const Prim<T>& L, const Prim<T>& R,
   lsqL += lssum;
   lsqR += lssum;
   // sq = sqrt(rho)
-  lrhoL += lsqL * h / sqL;
-  lrhoR += lsqR * h / sqR;
+  lrhoL += lsqL * h * (sqL * irL);  // 1/sqL = sqL / rhoL
+  lrhoR += lsqR * h * (sqR * irR);
   // H = (E + p) ir; ir = 1/rho
   lEL += lHL * irL;
   lpL += lHL * irL;

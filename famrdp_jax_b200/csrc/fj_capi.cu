@@ -913,11 +913,28 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
   if (s != FJ_OK) return s;
   char* base = (char*)ctx->ws;
   std::vector<fj_block> q0(blocks, blocks + nblocks), l0(blocks, blocks + nblocks);
+  // The adjoint accumulates in lam_out itself when no lam_out array overlaps
+  // any array the sweep reads (lam_in, the states); else in scratch, copied
+  // out at the end.
+  auto bytes5 = [&](int b) { return 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double); };
+  auto overlap = [](const void* a, size_t na, const void* b, size_t nb) {
+    const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+    return b != nullptr && x < y + nb && y < x + na;
+  };
+  bool direct = true;
+  for (int b = 0; b < nblocks && direct; ++b)
+    for (int c = 0; c < nblocks && direct; ++c) {
+      const size_t nb = bytes5(b), nc = bytes5(c);
+      if (overlap(lam_out[b], nb, lam_in[c], nc) || overlap(lam_out[b], nb, blocks[c].q, nc) ||
+          (saved && (overlap(lam_out[b], nb, q1_saved[c], nc) || overlap(lam_out[b], nb, q2_saved[c], nc))) ||
+          (c != b && overlap(lam_out[b], nb, lam_out[c], nc)))
+        direct = false;
+    }
   size_t off = 0;
   for (int b = 0; b < nblocks; ++b) {
     if (!saved) q0[b].q = (double*)(base + off);
-    l0[b].q = (double*)(base + q0_bytes + off);
-    off += align256(5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double));
+    l0[b].q = direct ? lam_out[b] : (double*)(base + q0_bytes + off);
+    off += align256(bytes5(b));
   }
   char* tail = base + q0_bytes + sum5;
   double* Q1w = saved ? nullptr : (double*)tail;
@@ -985,6 +1002,7 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
   if (s != FJ_OK) return s;
   s = halo_transpose(ctx, l0.data(), nblocks, links, nlinks, p->ghost, (double*)wk, work, st);
   if (s != FJ_OK) return s;
+  if (direct) return FJ_OK;
   for (int b = 0; b < nblocks; ++b) {
     const size_t bytes = 5 * (size_t)blocks[b].ni * blocks[b].nj * blocks[b].nk * sizeof(double);
     s = cuda_status(ctx, cudaMemcpyAsync(lam_out[b], l0[b].q, bytes, cudaMemcpyDeviceToDevice, st), "copy");

@@ -169,8 +169,10 @@ def _forward_segment(run: _Run, qs, nsteps, keep: bool):
 def _reverse_sweep(run: _Run, checkpoints, lams):
     """Segments in reverse: recompute the segment's states from its checkpoint
     (keeping each step's stage states), then apply the step adjoints
-    backwards.  The adjoint is updated in place in one working copy."""
+    backwards.  The adjoint ping-pongs between two working copies, so each
+    step adjoint writes its result straight into the other copy."""
     lams = [l.clone() for l in lams]
+    spare = [torch.empty_like(l) for l in lams]
     nseg = len(checkpoints)
     for s in reversed(range(nseg)):
         seg_len = min(run.every, run.nsteps - s * run.every)
@@ -180,7 +182,8 @@ def _reverse_sweep(run: _Run, checkpoints, lams):
             _, states = _forward_segment(run, checkpoints[s], seg_len, keep=True)
         while states:
             step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu,
-                           mu0s=run.plan.mu0s, dts=run.plan.dts, out=lams)
+                           mu0s=run.plan.mu0s, dts=run.plan.dts, out=spare)
+            lams, spare = spare, lams
     return lams
 
 
