@@ -309,6 +309,7 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"))
         run = adjoint._Run(cfg=cfg, metrics=st.metrics, dt=float(dt), nsteps=nsteps, every=every, plan=plan,
                            tables=adjoint._Tables(cfg), dmu=torch.zeros(1, dtype=torch.float64, device=device))
         run.buffers([st.blocks[0].q])  # the driver's reusable buffers, outside the timed region
+        run.reverse_buffers([st.blocks[0].q])
         (final, checkpoints), t_ckpt = timed(lambda: adjoint._forward_with_checkpoints(run, [st.blocks[0].q]))
         lams = adjoint.kinetic_energy_grad(final, st.metrics, cfg.ghost)
         g, t_rev = timed(lambda: adjoint._reverse_sweep(run, checkpoints, lams))

@@ -140,6 +140,10 @@ class _Run:
     # the last segment's saved states, kept by the forward sweep (the reverse
     # sweep starts there, so that segment is not recomputed)
     _last_states: list | None = None
+    # the reverse sweep's second saved-state pool and the stream it recomputes
+    # segments on
+    _saved2: list | None = None
+    _side: object = None
 
     def buffers(self, like):
         if self._ping is None:
@@ -147,12 +151,22 @@ class _Run:
             self._saved = [tuple([torch.empty_like(q) for q in like] for _ in range(3)) for _ in range(self.every)]
         return self._ping, self._saved
 
+    def reverse_buffers(self, like):
+        """The second saved-state pool and the recompute stream (first use)."""
+        self.buffers(like)
+        if self._saved2 is None:
+            self._saved2 = [tuple([torch.empty_like(q) for q in like] for _ in range(3)) for _ in range(self.every)]
+            self._side = torch.cuda.Stream(like[0].device)
+        return self._saved2, self._side
 
-def _forward_segment(run: _Run, qs, nsteps, keep: bool):
+
+def _forward_segment(run: _Run, qs, nsteps, keep: bool, pool=None):
     """nsteps steps from qs through the run's ping-pong buffers; returns the
     final state (a ping-pong buffer) and, if keep, each step's saved
-    intermediate states (halo-filled start state, stage 1 and 2)."""
-    ping, pool = run.buffers(qs)
+    intermediate states (halo-filled start state, stage 1 and 2) in ``pool``
+    (default: the run's first pool)."""
+    ping, first = run.buffers(qs)
+    pool = first if pool is None else pool
     states = []
     cur = list(qs)
     for n in range(nsteps):
@@ -167,23 +181,42 @@ def _forward_segment(run: _Run, qs, nsteps, keep: bool):
 
 
 def _reverse_sweep(run: _Run, checkpoints, lams):
-    """Segments in reverse: recompute the segment's states from its checkpoint
-    (keeping each step's stage states), then apply the step adjoints
-    backwards.  The adjoint ping-pongs between two working copies, so each
-    step adjoint writes its result straight into the other copy."""
+    """Segments in reverse: the step adjoints of segment s run backwards
+    through its saved states while segment s-1 is recomputed from its
+    checkpoint on a second stream into the other saved-state pool (the two
+    chains are independent, so the recompute's memory-bound kernels share the
+    GPU with the adjoint's arithmetic-bound ones).  The last segment's states
+    come from the forward sweep.  The adjoint ping-pongs between two working
+    copies, so each step adjoint writes its result straight into the other."""
     lams = [l.clone() for l in lams]
     spare = [torch.empty_like(l) for l in lams]
     nseg = len(checkpoints)
+    seg_len = [min(run.every, run.nsteps - s * run.every) for s in range(nseg)]
+    _, pool_a = run.buffers(checkpoints[0])
+    pool_b, side = run.reverse_buffers(checkpoints[0])
+    main = torch.cuda.current_stream(lams[0].device)
+    s = nseg - 1
+    if run._last_states is not None and len(run._last_states) == seg_len[s]:
+        states, run._last_states = run._last_states, None
+    else:
+        _, states = _forward_segment(run, checkpoints[s], seg_len[s], keep=True, pool=pool_a)
+    pools = (pool_a, pool_b) if states[0] is pool_a[0] else (pool_b, pool_a)
     for s in reversed(range(nseg)):
-        seg_len = min(run.every, run.nsteps - s * run.every)
-        if s == nseg - 1 and run._last_states is not None and len(run._last_states) == seg_len:
-            states, run._last_states = run._last_states, None
-        else:
-            _, states = _forward_segment(run, checkpoints[s], seg_len, keep=True)
+        done = None
+        if s > 0:
+            # the other pool was last read by segment s+1's adjoints, queued on main
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                _, nxt = _forward_segment(run, checkpoints[s - 1], seg_len[s - 1], keep=True, pool=pools[1])
+            done = torch.cuda.Event()
+            done.record(side)
         while states:
             step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu,
                            mu0s=run.plan.mu0s, dts=run.plan.dts, out=spare)
             lams, spare = spare, lams
+        if done is not None:
+            main.wait_event(done)
+            states, pools = nxt, (pools[1], pools[0])
     return lams
 
 
