@@ -426,16 +426,25 @@ struct GlobalSrc {
   int32_t N;
   __device__ __forceinline__ void F_rec(int32_t c, T* o) const { ld_rec<T, kRecF>((const T*)B.F + (size_t)c * kRecF, o); }
   // the five components of face a of the record of cell c (floats 5a..5a+4),
-  // as two aligned 16-byte loads
+  // (faces 0 and 2: one 256-bit load of their half; face 1: two 16-byte loads)
   __device__ __forceinline__ void F_axis(int32_t c, int a, T* o) const {
     const T* p = (const T*)B.F + (size_t)c * kRecF;
     if constexpr (sizeof(T) == 4) {
-      const int q = (5 * a) >> 2, s = (5 * a) & 3;  // first float4 and the offset in it
-      const float4 x = __ldg(reinterpret_cast<const float4*>(p) + q);
-      const float4 y = __ldg(reinterpret_cast<const float4*>(p) + q + 1);
-      const float w[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+      if (a != 1) {
+        // faces 0 and 2 lie in one 32-byte half of the record: one 256-bit load
+        float w[8];
+        ld_rec<T, 8>(p + (a == 0 ? 0 : 8), w);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) o[v] = w[s + v];
+        for (int v = 0; v < 5; ++v) o[v] = w[(a == 0 ? 0 : 2) + v];
+      } else {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(p) + 1);  // floats 4..7
+        const float4 y = __ldg(reinterpret_cast<const float4*>(p) + 2);  // floats 8..11
+        o[0] = x.y;
+        o[1] = x.z;
+        o[2] = x.w;
+        o[3] = y.x;
+        o[4] = y.y;
+      }
     } else {
 #pragma unroll
       for (int v = 0; v < 5; ++v) o[v] = p[5 * a + v];
