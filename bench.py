@@ -68,9 +68,10 @@ STAGE_BYTES = {"f64": 200.0, "f32": 164.0}
 STEP_BYTES = {"f64": 560.0, "f32": 452.0}
 # DRAM bytes per padded cell of one stage-2 launch group (dram__bytes_read +
 # dram__bytes_write summed over the primitive, flux and assembly kernels),
-# measured by ncu on the 96^3 Taylor-Green case (1.0 M padded cells) and
-# scaled per cell: FP32 41 + 136 + 289 B, FP64 43 + 268 + 384 B
-STAGE_TRAFFIC = {"f32": 466.0, "f64": 695.0}
+# measured by ncu on `bench.py --stage-only --n 96` (4 blocks of 100^3 padded
+# cells, 4.0 M) and scaled per cell: FP32 59 + 169 + 274 B, FP64 74 + 301 +
+# 401 B
+STAGE_TRAFFIC = {"f32": 502.0, "f64": 777.0}
 
 
 def _peaks():
@@ -412,6 +413,23 @@ def run_ours(args):
     cells = case.interior_cells
     st0 = cases.to_state(case, device)
     dt = diagnostics.cfl_dt(st0, case.cfg, case.cfl)
+    if args.stage_only:
+        # four standalone stage-2 evaluations of all blocks (the launch group
+        # the roofline line times), for a profiler to capture: nothing else
+        cfg = dataclasses.replace(case.cfg, precision=args.precision)
+        plan = StepPlan(st0, cfg)
+        if args.precision == "f32":
+            plan.set_variant(args.shape)
+        q0s = [b.q for b in st0.blocks]
+        qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state
+        outs = [torch.empty_like(q) for q in q0s]
+        for _ in range(4):
+            plan.stage(qin, q0s, outs, dt, 2)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"stage_only": True, "precision": args.precision, "shape": args.shape,
+                              "padded_cells": case.padded_cells}), flush=True)
+        return 0
     ens = None
     if "mu0" in case.meta and isinstance(case.meta["mu0"], list):  # independent instances
         ens = (case.meta["mu0"], [diagnostics.cfl_dt(State(blocks=(b,), metrics=(m,)), case.cfg, case.cfl)
@@ -466,16 +484,17 @@ def run_ours(args):
     # ---- dominant kernel group: one RK stage of all blocks ------------------
     plan, cfg, state = plans[args.precision]
     q0s = finals[args.precision]
+    qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state q0
     outs = [torch.empty_like(q) for q in q0s]
     for _ in range(3):
-        plan.stage(q0s, q0s, outs, dt, 2)
+        plan.stage(qin, q0s, outs, dt, 2)
     torch.cuda.synchronize()
     reps = 10
     s = torch.cuda.current_stream()
     a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a0.record(s)
     for _ in range(reps):
-        plan.stage(q0s, q0s, outs, dt, 2)
+        plan.stage(qin, q0s, outs, dt, 2)
     a1.record(s)
     torch.cuda.synchronize()
     stage_ms = a0.elapsed_time(a1) / reps
@@ -564,6 +583,9 @@ def main(argv=None):
     ap.add_argument("--workload", choices=["wavy4", "tgv32", "tree24", "ensemble64"], default="wavy4")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--stage-only", action="store_true",
+                    help="only run four standalone stage-2 evaluations (for a profiler)")
+    ap.add_argument("--shape", type=int, default=1, help="FP32 launch shape for --stage-only")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
