@@ -16,12 +16,14 @@ import ctypes
 import torch
 
 from famrdp_jax_b200 import _capi
-from famrdp_jax_b200.core.constants import BCType, Face
+from famrdp_jax_b200.core.constants import BCType, Face, orientation_supported
 
 
 def links(topos) -> list[tuple[int, int, int, int, int]]:
     """(tgt_block, tgt_face, src_block, src_face, orient) in halo order.
-    ``orient != 0`` raises NotImplementedError (mesh/halo.py:86-87)."""
+    An orientation other than 0 (the reference's copy) or a mapped code
+    (``core.constants.ORIENT_MAPPED``) raises NotImplementedError
+    (mesh/halo.py:86-87)."""
     id_to_idx = {t.block_id: i for i, t in enumerate(topos)}
     out = []
     for i, topo in enumerate(topos):
@@ -31,7 +33,7 @@ def links(topos) -> list[tuple[int, int, int, int, int]]:
             if topo.bc_type.get(face) != BCType.CUT1TO1:
                 continue
             nb_id, src_face, orient = info
-            if orient != 0:
+            if not orientation_supported(orient):
                 raise NotImplementedError(f"orient={orient} not supported in stage 1")
             out.append((i, int(face), id_to_idx[nb_id], int(src_face), int(orient)))
     return out

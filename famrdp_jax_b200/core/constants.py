@@ -39,3 +39,29 @@ class Face(IntEnum):
 
 N_EQN = 5  # rho, rho*u, rho*v, rho*w, rho*E
 N_DIM = 3
+
+# Interface orientation codes (``neighbors[face] = (block_id, face, orient)``):
+# 0 is the reference's element-by-element slab copy (mesh/halo.py:36-53); the
+# reference rejects every other value (mesh/halo.py:86-87), including the 1 its
+# topology reader stores.  ORIENT_MAPPED | bits is this library's face-to-face
+# mapping, for interfaces whose index directions differ between the two
+# blocks (no counterpart in the reference): the ghost layer at distance d from
+# the interface takes the source's interior layer at distance d, and the
+# target face's two tangential axes, in i, j, k order, map onto the source
+# face's, ORIENT_SWAP pairing the first with the second and ORIENT_REV_A /
+# ORIENT_REV_B running the target's first / second one backwards on the source.
+ORIENT_MAPPED = 8
+ORIENT_SWAP = 1
+ORIENT_REV_A = 2
+ORIENT_REV_B = 4
+
+
+def mapped_orientation(swap: bool = False, reverse_a: bool = False, reverse_b: bool = False) -> int:
+    """The orientation code of a mapped interface (see ORIENT_MAPPED)."""
+    return ORIENT_MAPPED | (ORIENT_SWAP if swap else 0) | (ORIENT_REV_A if reverse_a else 0) | \
+        (ORIENT_REV_B if reverse_b else 0)
+
+
+def orientation_supported(orient: int) -> bool:
+    """0 (the reference's copy) or a mapped code ORIENT_MAPPED | bits."""
+    return orient == 0 or (int(orient) & ~7) == ORIENT_MAPPED

@@ -13,6 +13,15 @@
 //   * links apply in list order, so where two target slabs overlap (edges and
 //     corners) the later link wins: the scatter kernel skips a cell that a
 //     later link of the same target block also writes.
+// Orientation: 0 is the reference's element-by-element slab copy; 1 (the
+// marker the reference's topology reader stores) is rejected as there.  Codes
+// 8..15 are this library's face-to-face mapping (the reference has none): the
+// ghost layer at distance d from the interface takes the source's interior
+// layer at distance d, and the target's two tangential axes (in i, j, k
+// order) map onto the source's with bit 0 = swapped, bit 1 / bit 2 = the
+// first / second target tangential axis runs backwards on the source.  Each
+// link is reduced on the host to an affine map from the target slab's
+// coordinates to a source cell index (base + signed stride per axis).
 // Boundary conditions run after the halo, one launch per face in Face enum
 // order (physics/bc/dispatch.py:15), each launch covering that face of every
 // block (blocks are independent).
@@ -31,9 +40,11 @@ constexpr int kMaxBcPerLaunch = 128;
 struct HaloDesc {
   double* tgt;
   const double* src;
-  long long off;   // slab offset in scratch (doubles)
+  long long off;      // slab offset in scratch (doubles)
+  long long s0;       // source cell index of the slab's first element
+  long long sstr[3];  // source index step per step along target slab axis 0, 1, 2
   int tn[3], sn[3];
-  int tlo[3], slo[3], ext[3];
+  int tlo[3], ext[3];
   int tgt_block;
 };
 
@@ -71,8 +82,7 @@ __global__ void k_halo_gather(const HaloTable tab, double* __restrict__ scratch)
     const int c = (int)(r % d.ext[2]);
     const int b = (int)((r / d.ext[2]) % d.ext[1]);
     const int a = (int)(r / ((int64_t)d.ext[2] * d.ext[1]));
-    scratch[d.off + t] =
-        d.src[v * NS + cell_index(d.sn, d.slo[0] + a, d.slo[1] + b, d.slo[2] + c)];
+    scratch[d.off + t] = d.src[v * NS + d.s0 + a * d.sstr[0] + b * d.sstr[1] + c * d.sstr[2]];
   }
 }
 
@@ -192,7 +202,8 @@ int build_links(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link*
       return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "link block index out of range");
     if (l.tgt_face < 0 || l.tgt_face > 5 || l.src_face < 0 || l.src_face > 5)
       return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "link face out of range");
-    if (l.orient != 0)
+    const bool mapped = (l.orient & ~7) == 8;
+    if (l.orient != 0 && !mapped)
       return set_err(ctx, FJ_ERR_NOT_IMPLEMENTED,
                      "orient=" + std::to_string(l.orient) + " not supported in stage 1");
     const fj_block& tb = blocks[l.tgt_block];
@@ -202,15 +213,51 @@ int build_links(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link*
     d.src = sb.q;
     d.tn[0] = tb.ni; d.tn[1] = tb.nj; d.tn[2] = tb.nk;
     d.sn[0] = sb.ni; d.sn[1] = sb.nj; d.sn[2] = sb.nk;
-    int sext[3];
+    const long long sst[3] = {(long long)d.sn[1] * d.sn[2], d.sn[2], 1};  // source array strides
     face_box(l.tgt_face, d.tn, ghost, false, d.tlo, d.ext);
-    face_box(l.src_face, d.sn, ghost, true, d.slo, sext);
-    if (sext[0] != d.ext[0] || sext[1] != d.ext[1] || sext[2] != d.ext[2])
-      return set_err(ctx, FJ_ERR_SHAPE,
-                     "halo slab shape mismatch: target (5," + std::to_string(d.ext[0]) + "," +
-                         std::to_string(d.ext[1]) + "," + std::to_string(d.ext[2]) +
-                         ") vs source (5," + std::to_string(sext[0]) + "," +
-                         std::to_string(sext[1]) + "," + std::to_string(sext[2]) + ")");
+    if (!mapped) {  // the reference's element-by-element copy of equal-shaped slabs
+      int slo[3], sext[3];
+      face_box(l.src_face, d.sn, ghost, true, slo, sext);
+      if (sext[0] != d.ext[0] || sext[1] != d.ext[1] || sext[2] != d.ext[2])
+        return set_err(ctx, FJ_ERR_SHAPE,
+                       "halo slab shape mismatch: target (5," + std::to_string(d.ext[0]) + "," +
+                           std::to_string(d.ext[1]) + "," + std::to_string(d.ext[2]) +
+                           ") vs source (5," + std::to_string(sext[0]) + "," +
+                           std::to_string(sext[1]) + "," + std::to_string(sext[2]) + ")");
+      d.s0 = slo[0] * sst[0] + slo[1] * sst[1] + slo[2];
+      for (int a = 0; a < 3; ++a) d.sstr[a] = sst[a];
+    } else {
+      const int aT = l.tgt_face >> 1, aS = l.src_face >> 1;
+      const bool tmin = (l.tgt_face & 1) == 0, smin = (l.src_face & 1) == 0;
+      if (d.sn[aS] < 2 * ghost)
+        return set_err(ctx, FJ_ERR_SHAPE, "halo source block thinner than two ghost widths");
+      // normal axis: target layer r (0..g-1 from the slab's low end) is at
+      // distance d = g - r (MIN face) or r + 1 (MAX face) from the interface;
+      // the source layer at distance d is g + d - 1 (MIN) or n - g - d (MAX)
+      long long base, dir;
+      if (tmin && smin) base = 2 * ghost - 1, dir = -1;
+      else if (tmin) base = d.sn[aS] - 2 * ghost, dir = 1;
+      else if (smin) base = ghost, dir = 1;
+      else base = d.sn[aS] - ghost - 1, dir = -1;
+      d.s0 = base * sst[aS];
+      d.sstr[aT] = dir * sst[aS];
+      int tt[2], ss[2], nt = 0, ns = 0;  // tangential axes in i, j, k order
+      for (int a = 0; a < 3; ++a) {
+        if (a != aT) tt[nt++] = a;
+        if (a != aS) ss[ns++] = a;
+      }
+      const bool swap = (l.orient & 1) != 0;
+      for (int m = 0; m < 2; ++m) {
+        const int t = tt[m], sa = ss[swap ? 1 - m : m];
+        const bool rev = (l.orient & (2 << m)) != 0;
+        if (d.ext[t] != d.sn[sa])
+          return set_err(ctx, FJ_ERR_SHAPE,
+                         "halo slab shape mismatch: target tangential extent " + std::to_string(d.ext[t]) +
+                             " vs source " + std::to_string(d.sn[sa]));
+        d.s0 += (rev ? (long long)(d.sn[sa] - 1) : 0) * sst[sa];
+        d.sstr[t] = (rev ? -1 : 1) * sst[sa];
+      }
+    }
     d.tgt_block = l.tgt_block;
     d.off = (long long)scratch_doubles;
     scratch_doubles += 5ull * d.ext[0] * d.ext[1] * d.ext[2];
@@ -362,7 +409,7 @@ __global__ void k_halo_transpose(const HaloTable tab, double* __restrict__ scrat
 #pragma unroll
       for (int v = 0; v < 5; ++v) tgt[v * NT + tc] = 0.0;
     } else {
-      const int64_t sc = cell_index(d.sn, d.slo[0] + a, d.slo[1] + b, d.slo[2] + c);
+      const int64_t sc = d.s0 + a * d.sstr[0] + b * d.sstr[1] + c * d.sstr[2];
 #pragma unroll
       for (int v = 0; v < 5; ++v) atomicAdd(src + v * NS + sc, scratch[d.off + v * V + r]);
     }

@@ -3,8 +3,11 @@
 Every CUT1TO1 face copies the source block's 2-layer slab next to the source
 face into the target's ghost slab (full extent along the other two axes),
 reading all sources from the pre-exchange arrays; faces apply in (block,
-neighbors-dict) order so later faces overwrite edges and corners;
-``orient != 0`` raises NotImplementedError.
+neighbors-dict) order so later faces overwrite edges and corners.
+Orientation 0 is the reference's element-by-element copy; a mapped code
+(``core.constants.mapped_orientation``, no counterpart in the reference)
+connects faces whose index directions differ; any other value raises
+NotImplementedError as the reference does.
 """
 from __future__ import annotations
 

@@ -82,11 +82,31 @@ typedef struct fj_block {
 
 /* One CUT1TO1 face (a BlockTopology.neighbors entry, mesh/halo.py:79-90).
  * Links are applied in array order; the caller lists them in the reference's
- * (block, neighbors-dict) iteration order. */
+ * (block, neighbors-dict) iteration order.
+ * orient:
+ *   0      the reference's copy (mesh/halo.py:36-53): the source's 2-layer
+ *          slab next to src_face, element by element in array order, into
+ *          the target's ghost slab; the two slabs must have equal shapes;
+ *   1      the marker the reference's topology reader stores for every
+ *          interface (mesh/io_top.py:183): FJ_ERR_NOT_IMPLEMENTED, as the
+ *          reference's halo fill raises (mesh/halo.py:86-87);
+ *   8..15  FJ_ORIENT_MAPPED | bits (no counterpart in the reference): the
+ *          ghost layer at distance d from the interface takes the source's
+ *          interior layer at distance d (any pair of faces), and the target
+ *          face's two tangential axes, in i, j, k order, map onto the source
+ *          face's: FJ_ORIENT_SWAP pairs the first with the second,
+ *          FJ_ORIENT_REV_A / FJ_ORIENT_REV_B run the target's first / second
+ *          tangential axis backwards on the source.  Tangential extents must
+ *          match (full extents, ghosts included), else FJ_ERR_SHAPE;
+ *   other  FJ_ERR_NOT_IMPLEMENTED. */
+#define FJ_ORIENT_MAPPED 8
+#define FJ_ORIENT_SWAP 1
+#define FJ_ORIENT_REV_A 2
+#define FJ_ORIENT_REV_B 4
 typedef struct fj_link {
   int tgt_block, tgt_face;
   int src_block, src_face;
-  int orient;           /* must be 0 */
+  int orient;
 } fj_link;
 
 /* One physical boundary face (physics/bc/dispatch.py:11-32).  The caller lists
