@@ -279,9 +279,11 @@ __device__ __forceinline__ void metric_row(const SplitBlock& B, int32_t N, int l
 
 // Primitives rho u v w p T of one cell from its conserved values, in FP64
 // (physics/eos.py:12-17; T = p / max(rho R, 1e-300), rhs/viscous.py:36).
-__device__ __forceinline__ void prims_of(const double q[5], double gm1, double R, double out[6]) {
+// (iR = 1/R from the host; __drcp_rn is the IEEE round-to-nearest reciprocal,
+// the same value as 1.0 / r without a general division.)
+__device__ __forceinline__ void prims_of(const double q[5], double gm1, double R, double iR, double out[6]) {
   const double r = q[0];
-  const double ir = 1.0 / r;
+  const double ir = __drcp_rn(r);
   const double u = q[1] * ir, v = q[2] * ir, w = q[3] * ir;
   const double p = gm1 * (q[4] - r * (0.5 * (u * u + v * v + w * w)));
   out[0] = r;
@@ -289,13 +291,14 @@ __device__ __forceinline__ void prims_of(const double q[5], double gm1, double R
   out[2] = v;
   out[3] = w;
   out[4] = p;
-  out[5] = r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300;
+  out[5] = r * R > 1e-300 ? p * ir * iR : p * 1e300;
 }
 
 // p_ref != 0 (the record path): the pressure slot holds p - p_ref.
 template <typename T>
 __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, const double gm1,
-                                                              const double R, const double p_ref) {
+                                                              const double R, const double iR,
+                                                              const double p_ref) {
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
   const SplitBlock& B = tab.b[b].blk;
@@ -305,7 +308,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, 
   const double* q = B.q + c;
   const double qc[5] = {q[0], q[N], q[2 * (size_t)N], q[3 * (size_t)N], q[4 * (size_t)N]};
   double pv[6];
-  prims_of(qc, gm1, R, pv);
+  prims_of(qc, gm1, R, iR, pv);
   const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)(pv[4] - p_ref), (T)pv[5], T(0), T(0)};
   st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
 }
@@ -458,7 +461,8 @@ struct GlobalSrc {
 // solver/step.py:45-53) from the intermediates Src provides.
 template <typename T, bool K_AOS, class Src>
 __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x, const Src& src, int flags,
-                                              int stage, int next_prims, double gm1, double R, double ph_p_ref) {
+                                              int stage, int next_prims, double gm1, double R, double iR,
+                                              double ph_p_ref) {
   const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
   const int32_t si = x.nj * x.nk, sj = x.nk;
   const int n[3] = {x.ni, x.nj, x.nk};
@@ -471,7 +475,7 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
     const bool on[3] = {idx[0] >= 2 && idx[0] <= n[0] - 3, idx[1] >= 2 && idx[1] <= n[1] - 3,
                         idx[2] >= 2 && idx[2] <= n[2] - 3};
     if (on[0] || on[1] || on[2]) {
-      const double ivd = 1.0 / (B.vol[c] + 1e-300);
+      const double ivd = __drcp_rn(B.vol[c] + 1e-300);
       T Fc[kRecF];
       src.F_rec(c, Fc);
       // the p_ref n part the face fluxes left out: p_ref times the sum over
@@ -551,7 +555,7 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
     }
     if (next_prims) {
       double pv[6];
-      prims_of(qn, gm1, R, pv);
+      prims_of(qn, gm1, R, iR, pv);
       const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)(pv[4] - ph_p_ref), (T)pv[5], T(0), T(0)};
       st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
     }
@@ -564,14 +568,14 @@ template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
 __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Table tab, const int flags,
                                                                        const int stage, const int next_prims,
                                                                        const double gm1, const double R,
-                                                                       const double ph_p_ref) {
+                                                                       const double iR, const double ph_p_ref) {
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(tab.b[b], blockIdx.x, flags, stage);
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
   const GlobalSrc<T, K_AOS> src{B, (int32_t)x.N};
-  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, ph_p_ref);
+  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, iR, ph_p_ref);
 }
 
 // ---- field-major variant (the FP64 path) ----------------------------------
@@ -583,7 +587,7 @@ namespace fm {
 
 template <typename T>
 __global__ void __launch_bounds__(kSplitThreads) k_fm_prims(const Table tab, const double gm1,
-                                                              const double R) {
+                                                              const double R, const double iR) {
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
   const SplitBlock& B = tab.b[b].blk;
@@ -592,10 +596,10 @@ __global__ void __launch_bounds__(kSplitThreads) k_fm_prims(const Table tab, con
   if (c >= N) return;
   const double* q = B.q;
   const double r = q[c];
-  const double ir = 1.0 / r;
+  const double ir = __drcp_rn(r);
   const double u = q[N + c] * ir, v = q[2 * N + c] * ir, w = q[3 * N + c] * ir;
   const double p = gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
-  const double Tt = r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300;
+  const double Tt = r * R > 1e-300 ? p * ir * iR : p * 1e300;
   const T rec[kRecP64] = {(T)r, (T)u, (T)v, (T)w, (T)p, (T)Tt};
   st_rec<T, kRecP64>((T*)B.prim + c * kRecP64, rec);
 }
@@ -743,7 +747,8 @@ __global__ void __launch_bounds__(kSplitThreads, 2) k_fm_fluxes(const Table tab,
 template <typename T>
 __global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table tab, const int flags,
                                                                  const int stage, const int next_prims,
-                                                                 const double gm1, const double R) {
+                                                                 const double gm1, const double R,
+                                                                 const double iR) {
   const int b = find_block(tab, blockIdx.x);
   Cell x;
   if (threadIdx.x == 0) prefetch_assembly<T, false, true>(tab.b[b], blockIdx.x, flags, stage);
@@ -757,7 +762,7 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table ta
   double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (flags & kRhsInvscd) {
     const T* F = (const T*)B.F;
-    const double ivd = 1.0 / (B.vol[c] + 1e-300);
+    const double ivd = __drcp_rn(B.vol[c] + 1e-300);
     const bool on[3] = {idx[0] >= 2 && idx[0] <= n[0] - 3, idx[1] >= 2 && idx[1] <= n[1] - 3,
                         idx[2] >= 2 && idx[2] <= n[2] - 3};
 #pragma unroll
@@ -831,7 +836,7 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table ta
     }
     if (next_prims) {
       double pv[6];
-      prims_of(qn, gm1, R, pv);
+      prims_of(qn, gm1, R, iR, pv);
       T rec[kRecP64];
 #pragma unroll
       for (int v = 0; v < kRecP64; ++v) rec[v] = (T)pv[v];
@@ -928,6 +933,7 @@ void launch_pair(const Table& tab, int ctas, const Phys& ph, int flags, int stag
   k_split_fluxes<T, K_AOS, sh.flux_occ><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
   if (after_fluxes) cudaEventRecord(after_fluxes, st);
   k_split_assemble<T, K_AOS, sh.asm_occ><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
+                                                                          1.0 / ph.R,
                                                                         K_AOS ? ph.p_ref : 0.0);
 }
 
@@ -936,12 +942,14 @@ int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage,
                bool next_prims, int variant, cudaStream_t st, cudaEvent_t after_fluxes) {
   const int np = next_prims ? 1 : 0;
   if constexpr (sizeof(T) == 8) {
-    if (!prims_ready) fm::k_fm_prims<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R);
+    if (!prims_ready) fm::k_fm_prims<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, 1.0 / ph.R);
     fm::k_fm_fluxes<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
     if (after_fluxes) cudaEventRecord(after_fluxes, st);
-    fm::k_fm_assemble<double><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R);
+    fm::k_fm_assemble<double><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
+                                                                1.0 / ph.R);
   } else {
-    if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, K_AOS ? ph.p_ref : 0.0);
+    if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, 1.0 / ph.R,
+                                                                       K_AOS ? ph.p_ref : 0.0);
     switch (K_AOS ? variant : 0) {
       case 1: launch_pair<T, K_AOS, 1>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
       case 2: launch_pair<T, K_AOS, 2>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
