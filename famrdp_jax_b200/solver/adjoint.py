@@ -141,7 +141,9 @@ class _Run:
     # sweep starts there, so that segment is not recomputed)
     _last_states: list | None = None
     # the reverse sweep's second saved-state pool and the stream it recomputes
-    # segments on
+    # segments on (overlap=False, or too little memory for the second pool:
+    # segments are recomputed on the caller's stream between the adjoints)
+    overlap: bool = True
     _saved2: list | None = None
     _side: object = None
 
@@ -152,12 +154,20 @@ class _Run:
         return self._ping, self._saved
 
     def reverse_buffers(self, like):
-        """The second saved-state pool and the recompute stream (first use)."""
+        """The second saved-state pool and the recompute stream (first use),
+        or (None, None) when the sweep runs without overlap: by request, or
+        because the device has no room for the pool (it doubles the memory of
+        the saved states)."""
         self.buffers(like)
-        if self._saved2 is None:
-            self._saved2 = [tuple([torch.empty_like(q) for q in like] for _ in range(3)) for _ in range(self.every)]
-            self._side = torch.cuda.Stream(like[0].device)
-        return self._saved2, self._side
+        if self.overlap and self._saved2 is None:
+            try:
+                self._saved2 = [tuple([torch.empty_like(q) for q in like] for _ in range(3))
+                                for _ in range(self.every)]
+                self._side = torch.cuda.Stream(like[0].device)
+            except torch.cuda.OutOfMemoryError:
+                self._saved2, self.overlap = None, False
+                torch.cuda.empty_cache()
+        return (self._saved2, self._side) if self.overlap else (None, None)
 
 
 def _forward_segment(run: _Run, qs, nsteps, keep: bool, pool=None):
@@ -194,6 +204,8 @@ def _reverse_sweep(run: _Run, checkpoints, lams):
     seg_len = [min(run.every, run.nsteps - s * run.every) for s in range(nseg)]
     _, pool_a = run.buffers(checkpoints[0])
     pool_b, side = run.reverse_buffers(checkpoints[0])
+    if pool_b is None:
+        return _reverse_sweep_serial(run, checkpoints, lams, spare, seg_len, pool_a)
     main = torch.cuda.current_stream(lams[0].device)
     s = nseg - 1
     if run._last_states is not None and len(run._last_states) == seg_len[s]:
@@ -217,6 +229,22 @@ def _reverse_sweep(run: _Run, checkpoints, lams):
         if done is not None:
             main.wait_event(done)
             states, pools = nxt, (pools[1], pools[0])
+    return lams
+
+
+def _reverse_sweep_serial(run: _Run, checkpoints, lams, spare, seg_len, pool):
+    """The reverse sweep with one saved-state pool: each segment is recomputed
+    on the caller's stream after the previous segment's adjoints."""
+    nseg = len(checkpoints)
+    for s in reversed(range(nseg)):
+        if s == nseg - 1 and run._last_states is not None and len(run._last_states) == seg_len[s]:
+            states, run._last_states = run._last_states, None
+        else:
+            _, states = _forward_segment(run, checkpoints[s], seg_len[s], keep=True, pool=pool)
+        while states:
+            step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu,
+                           mu0s=run.plan.mu0s, dts=run.plan.dts, out=spare)
+            lams, spare = spare, lams
     return lams
 
 
@@ -254,29 +282,32 @@ class _Trajectory(torch.autograd.Function):
 
 
 def integrate(state: State, cfg: Config, dt: float, nsteps: int, *, checkpoint_every: int = 10,
-              plan: StepPlan | None = None) -> State:
+              plan: StepPlan | None = None, overlap: bool = True) -> State:
     """nsteps TVD-RK3 steps, differentiable with respect to the blocks' q
     through the hand-written adjoint (one checkpoint every checkpoint_every
-    steps, recomputation in the reverse sweep)."""
+    steps, recomputation in the reverse sweep).  overlap: recompute the next
+    segment on a second stream during the adjoints (a second set of
+    checkpoint_every saved-state triples; skipped when it does not fit)."""
     plan = plan or StepPlan(state, cfg)
     run = _Run(cfg=cfg, metrics=state.metrics, dt=float(dt), nsteps=int(nsteps), every=max(1, int(checkpoint_every)),
-               plan=plan, tables=_Tables(cfg))
+               plan=plan, tables=_Tables(cfg), overlap=overlap)
     final = _Trajectory.apply(run, *[b.q for b in state.blocks])
     blocks = tuple(Block(q=q, xyz=b.xyz) for q, b in zip(final, state.blocks))
     return State(blocks=blocks, metrics=state.metrics, t=state.t + nsteps * dt, step=state.step + nsteps)
 
 
 def adjoint_kinetic_energy(state: State, cfg: Config, dt: float, nsteps: int, checkpoint_every: int = 10,
-                           plan: StepPlan | None = None):
+                           plan: StepPlan | None = None, overlap: bool = True):
     """(J, dJ/dq0 per block, dJ/dmu0) for J = the interior kinetic-energy
-    integral after nsteps steps, by the checkpointed adjoint."""
+    integral after nsteps steps, by the checkpointed adjoint (``overlap`` as
+    in ``integrate``)."""
     from famrdp_jax_b200.solver import diagnostics
 
     plan = plan or StepPlan(state, cfg)
     dev = state.blocks[0].q.device
     dmu = torch.zeros(1, dtype=torch.float64, device=dev)
     run = _Run(cfg=cfg, metrics=state.metrics, dt=float(dt), nsteps=int(nsteps), every=max(1, int(checkpoint_every)),
-               plan=plan, tables=_Tables(cfg), dmu=dmu)
+               plan=plan, tables=_Tables(cfg), dmu=dmu, overlap=overlap)
     final, checkpoints = _forward_with_checkpoints(run, [b.q for b in state.blocks])
     fstate = State(blocks=tuple(Block(q=q, xyz=b.xyz) for q, b in zip(final, state.blocks)), metrics=state.metrics)
     J = diagnostics.kinetic_energy(fstate, cfg.ghost)
@@ -286,7 +317,7 @@ def adjoint_kinetic_energy(state: State, cfg: Config, dt: float, nsteps: int, ch
 
 
 def adjoint_kinetic_energy_ensemble(state: State, cfg: Config, nsteps: int, *, mu0s, dts,
-                                    checkpoint_every: int = 10, plan: StepPlan | None = None):
+                                    checkpoint_every: int = 10, plan: StepPlan | None = None, overlap: bool = True):
     """Per-instance adjoint of an ensemble of independent blocks (block b with
     its own mu0s[b] and dts[b]): J_b = kinetic energy of block b after nsteps
     steps, and dJ_b/dq0_b and dJ_b/dmu0_b for every b, from one checkpointed
@@ -297,7 +328,7 @@ def adjoint_kinetic_energy_ensemble(state: State, cfg: Config, nsteps: int, *, m
     nb = len(state.blocks)
     dmu = torch.zeros(nb, dtype=torch.float64, device=dev)
     run = _Run(cfg=cfg, metrics=state.metrics, dt=0.0, nsteps=int(nsteps), every=max(1, int(checkpoint_every)),
-               plan=plan, tables=_Tables(cfg), dmu=dmu)
+               plan=plan, tables=_Tables(cfg), dmu=dmu, overlap=overlap)
     final, checkpoints = _forward_with_checkpoints(run, [b.q for b in state.blocks])
     from famrdp_jax_b200.solver import diagnostics
     Js = [diagnostics.kinetic_energy(State(blocks=(Block(q=q, xyz=b.xyz),), metrics=(m,)), cfg.ghost)

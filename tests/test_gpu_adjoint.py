@@ -233,13 +233,15 @@ def test_checkpoint_spacing_leaves_the_gradient_unchanged(cuda_device, precision
     """The reverse sweep recomputes segment s-1 on a second stream into the
     second saved-state pool while the adjoints of segment s run: with a
     checkpoint every 2 or 3 steps (several overlapped segments, a short last
-    one) or none (one segment, nothing recomputed) the 7-step gradient and
-    dJ/dmu0 are the same to the atomics' rounding."""
+    one), none (one segment, nothing recomputed) or without the overlap (one
+    pool, recompute between the adjoints) the 7-step gradient and dJ/dmu0 are
+    the same to the atomics' rounding."""
     import dataclasses
     c, st = _tgv_state(n=10)
     cfg = dataclasses.replace(c.cfg, precision=precision)
     dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], 1.4, 0.5, 2)
     runs = [adjoint.adjoint_kinetic_energy(st, cfg, dt, 7, checkpoint_every=k) for k in (7, 2, 3)]
+    runs.append(adjoint.adjoint_kinetic_energy(st, cfg, dt, 7, checkpoint_every=2, overlap=False))
     tol = 1e-13 if precision == "f64" else 1e-6
     J0, g0, m0 = runs[0]
     for J, g, m in runs[1:]:
