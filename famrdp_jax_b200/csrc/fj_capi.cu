@@ -251,6 +251,8 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
       std::vector<SplitBlock> v;
       for (int b : groups[g]) {
         SplitBlock e = sb[b];
+        // the primitives alternate between the two buffers from stage to stage
+        if (stage == 2) std::swap(e.prim, e.prim_next);
         e.q = stage == 1 ? out[b].q : (stage == 2 ? q1s[b] : q2s[b]);
         e.out = stage == 1 ? q1s[b] : (stage == 2 ? q2s[b] : q_out[b]);
         v.push_back(e);

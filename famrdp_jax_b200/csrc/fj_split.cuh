@@ -23,7 +23,10 @@ struct SplitBlock {
   const double* kxyz;    // (3, 3, ni, nj, nk)
   const void* kaos;      // FP32-flux only: optional FP32 metric records (kRecK per cell), or nullptr
   const double* vol;     // (ni, nj, nk)
-  void* prim;            // scratch: 6 x N flux-type values
+  void* prim;            // scratch: the primitives of the stage input (records in FP32)
+  void* prim_next;       // where the assembly writes the next stage's primitives: a
+                         // second buffer in FP32 (the FP32 assembly also reads prim),
+                         // prim itself in FP64
   void* F;               // scratch: 15 x N (face c | c+e_a, axis-major)
   void* G;               // scratch: viscous flux components (records: 8 per cell)
   void* Gz;              // records only: the ninth component, one per cell
@@ -31,6 +34,7 @@ struct SplitBlock {
   double dt;             // time step of this block (stages 1..3)
   int ni, nj, nk;
   int cta_begin;         // filled by the launcher
+  int cta_begin_asm;     // the same for the FP32 assembly's 248-cell CTAs
 };
 
 // Metric records (kRecK values of the flux type per cell) from the caller's

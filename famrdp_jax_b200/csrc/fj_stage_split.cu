@@ -137,11 +137,12 @@ __device__ __forceinline__ void prefetch_state(const Dev& d, int cta) {
 // one i-plane ahead (the ones behind were fetched by earlier CTAs).  FIELD:
 // field-major intermediates and FP64 kxyz (the FP64 path), else records.
 template <typename T, bool K_AOS, bool FIELD>
-__device__ __forceinline__ void prefetch_assembly(const Dev& d, int cta, int flags, int stage) {
+__device__ __forceinline__ void prefetch_assembly(const Dev& d, int cta, int flags, int stage,
+                                                  int cells = kSplitThreads, int begin = -1) {
   const SplitBlock& B = d.blk;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
-  const int64_t c0 = (int64_t)(cta - B.cta_begin) * kSplitThreads;
-  const int64_t n = min((int64_t)kSplitThreads, N - c0);
+  const int64_t c0 = (int64_t)(cta - (begin < 0 ? B.cta_begin : begin)) * cells;
+  const int64_t n = min((int64_t)cells, N - c0);
   if (n <= 0) return;
   if (stage != 0)
     for (int v = 0; v < 5; ++v) l2_prefetch(B.q + v * N + c0, n * 8);
@@ -390,8 +391,9 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
     ((T*)B.Gz)[c] = C0.u * t02 + C0.v * t12 + C0.w * t22 + kappa * g[3][2];
   }
   if (inv) {
-    // the three faces c | c+e_a for c_a in [1, n_a - 3]; invalid faces are
-    // stored as zeros (never read)
+    // the faces c | c+e_i and c | c+e_j for c_a in [1, n_a - 3]; invalid faces
+    // are stored as zeros (never read).  The k faces are left to the
+    // assembly, whose issue slots are mostly idle (this kernel is issue-bound)
     T Fr[kRecF];
 #pragma unroll
     for (int v = 0; v < kRecF; ++v) Fr[v] = T(0);
@@ -408,11 +410,6 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
       const Cell6<T> J2 = load_cell<T>(P, c + 2 * sj);
       metric_row<T, K_AOS>(B, N, 1, c + sj, kn);
       face_from_cells<T, K_AOS>(Jm, C0, Jp, J2, kk + 3, kn, ph, Fr + 5, p_ref);
-    }
-    if (x.k >= 1 && x.k <= x.nk - 3) {
-      const Cell6<T> K2 = load_cell<T>(P, c + 2);
-      metric_row<T, K_AOS>(B, N, 2, c + 1, kn);
-      face_from_cells<T, K_AOS>(Km, C0, Kp, K2, kk + 6, kn, ph, Fr + 10, p_ref);
     }
     st_rec<T, kRecF>((T*)B.F + (size_t)c * kRecF, Fr);
   }
@@ -459,10 +456,12 @@ struct GlobalSrc {
 
 // The assembly of one cell (rhs/invscd.py:119-131, rhs/viscous.py:86-117,
 // solver/step.py:45-53) from the intermediates Src provides.
+// fk_m / fk_p: the k faces c-1 | c and c | c+1 (the flux records hold only the
+// i and j faces).
 template <typename T, bool K_AOS, class Src>
 __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x, const Src& src, int flags,
                                               int stage, int next_prims, double gm1, double R, double iR,
-                                              double ph_p_ref) {
+                                              double ph_p_ref, const T fk_m[5], const T fk_p[5]) {
   const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
   const int32_t si = x.nj * x.nk, sj = x.nk;
   const int n[3] = {x.ni, x.nj, x.nk};
@@ -478,6 +477,8 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
       const double ivd = __drcp_rn(B.vol[c] + 1e-300);
       T Fc[kRecF];
       src.F_rec(c, Fc);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) Fc[10 + v] = fk_p[v];
       // the p_ref n part the face fluxes left out: p_ref times the sum over
       // the active axes of the face-normal differences, evaluated in FP64 when
       // the records were built
@@ -485,7 +486,10 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
       T Fm[3][5];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        if (on[a]) {
+        if (on[a] && a == 2) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) Fm[2][v] = fk_m[v];
+        } else if (on[a]) {
           src.F_axis(c - st[a], a, Fm[a]);
         } else {
 #pragma unroll
@@ -557,25 +561,80 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
       double pv[6];
       prims_of(qn, gm1, R, iR, pv);
       const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)(pv[4] - ph_p_ref), (T)pv[5], T(0), T(0)};
-      st_rec<T, kRecP>((T*)B.prim + (size_t)c * kRecP, rec);
+      st_rec<T, kRecP>((T*)B.prim_next + (size_t)c * kRecP, rec);
     }
   }
 }
 
 // With next_prims, also writes the primitives of the stage result (the next
 // stage's input) in place of a separate k_split_prims launch.
+// The k face c | c+1 (rhs/invscd.py:62-100) from the stage input's primitive
+// records of c-1 .. c+2 and the k rows of the metrics of c and c+1.
+template <typename T, bool K_AOS>
+__device__ __forceinline__ void k_face(const SplitBlock& B, int32_t N, int32_t c, const Phys& ph, T F[5]) {
+  const T* __restrict__ P = (const T*)B.prim;
+  const Cell6<T> a0 = load_cell<T>(P, c - 1), a1 = load_cell<T>(P, c), a2 = load_cell<T>(P, c + 1),
+                 a3 = load_cell<T>(P, c + 2);
+  T kl[3], kr[3];
+  metric_row<T, K_AOS>(B, N, 2, c, kl);
+  metric_row<T, K_AOS>(B, N, 2, c + 1, kr);
+  face_from_cells<T, K_AOS>(a0, a1, a2, a3, kl, kr, ph, F, K_AOS ? (T)ph.p_ref : T(0));
+}
+
+// Cells per assembly CTA: each warp assembles 31 consecutive cells; its 32nd
+// lane only evaluates the k face its 31st cell needs on the right.
+constexpr int kAsmCells = kSplitThreads / 32 * 31;
+
+// The last b with cta_begin_asm <= cta (the assembly's CTA ranges).
+__device__ __forceinline__ int find_block_asm(const Table& t, int cta) {
+  int lo = 0, hi = t.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (t.b[mid].blk.cta_begin_asm <= cta) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The k faces are computed here rather than in the issue-bound flux kernel
+// (the assembly's issue slots are mostly idle): lane l of a warp evaluates the
+// face on the left of its cell (c-1 | c) and takes the one on its right from
+// lane l+1 by shuffle, so no face is evaluated twice and no barrier is needed;
+// lane 31's cell is the next warp's first, for which it only supplies the face.
 template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
 __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Table tab, const int flags,
                                                                        const int stage, const int next_prims,
                                                                        const double gm1, const double R,
-                                                                       const double iR, const double ph_p_ref) {
-  const int b = find_block(tab, blockIdx.x);
-  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(tab.b[b], blockIdx.x, flags, stage);
+                                                                       const double iR, const Phys ph) {
+  const int b = find_block_asm(tab, blockIdx.x);
+  const Dev& d = tab.b[b];
+  const SplitBlock& B = d.blk;
+  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t N = (int64_t)B.ni * B.nj * B.nk;
+  const int64_t c = (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells + warp * 31 + lane;
   Cell x;
-  if (!decode(tab.b[b], blockIdx.x, x)) return;
-  const SplitBlock& B = tab.b[b].blk;
-  const GlobalSrc<T, K_AOS> src{B, (int32_t)x.N};
-  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, iR, ph_p_ref);
+  const bool alive = c < N;
+  if (alive) {
+    const uint32_t t1 = d.dk.div((uint32_t)c);
+    x.k = (int)((uint32_t)c - t1 * (uint32_t)B.nk);
+    x.i = (int)d.dj.div(t1);
+    x.j = (int)(t1 - (uint32_t)x.i * (uint32_t)B.nj);
+    x.c = c;
+    x.N = N;
+    x.ni = B.ni;
+    x.nj = B.nj;
+    x.nk = B.nk;
+  }
+  T fl[5] = {T(0), T(0), T(0), T(0), T(0)}, fr[5];
+  // face c-1 | c exists for k-1 in [1, nk-3]
+  if ((flags & kRhsInvscd) && alive && x.k >= 2 && x.k <= x.nk - 2)
+    k_face<T, K_AOS>(B, (int32_t)N, (int32_t)c - 1, ph, fl);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) fr[v] = __shfl_down_sync(0xffffffffu, fl[v], 1);
+  if (lane == 31 || !alive) return;
+  const GlobalSrc<T, K_AOS> src{B, (int32_t)N};
+  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, iR, K_AOS ? ph.p_ref : 0.0, fl, fr);
 }
 
 // ---- field-major variant (the FP64 path) ----------------------------------
@@ -927,18 +986,17 @@ constexpr SplitShape kSplitVariants[] = {{3, 6}, {3, 4}, {4, 4}, {3, 5}, {4, 6},
 static_assert(sizeof(kSplitVariants) / sizeof(kSplitVariants[0]) == FJ_NUM_SPLIT_VARIANTS, "variant table");
 
 template <typename T, bool K_AOS, int V>
-void launch_pair(const Table& tab, int ctas, const Phys& ph, int flags, int stage, int np, cudaStream_t st,
-                 cudaEvent_t after_fluxes) {
+void launch_pair(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, int np,
+                 cudaStream_t st, cudaEvent_t after_fluxes) {
   constexpr SplitShape sh = kSplitVariants[V];
   k_split_fluxes<T, K_AOS, sh.flux_occ><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
   if (after_fluxes) cudaEventRecord(after_fluxes, st);
-  k_split_assemble<T, K_AOS, sh.asm_occ><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
-                                                                          1.0 / ph.R,
-                                                                        K_AOS ? ph.p_ref : 0.0);
+  k_split_assemble<T, K_AOS, sh.asm_occ><<<asm_ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1,
+                                                                              ph.R, 1.0 / ph.R, ph);
 }
 
 template <typename T, bool K_AOS>
-int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage, bool prims_ready,
+int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, bool prims_ready,
                bool next_prims, int variant, cudaStream_t st, cudaEvent_t after_fluxes) {
   const int np = next_prims ? 1 : 0;
   if constexpr (sizeof(T) == 8) {
@@ -951,12 +1009,12 @@ int launch_tab(const Table& tab, int ctas, const Phys& ph, int flags, int stage,
     if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, 1.0 / ph.R,
                                                                        K_AOS ? ph.p_ref : 0.0);
     switch (K_AOS ? variant : 0) {
-      case 1: launch_pair<T, K_AOS, 1>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
-      case 2: launch_pair<T, K_AOS, 2>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
-      case 3: launch_pair<T, K_AOS, 3>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
-      case 4: launch_pair<T, K_AOS, 4>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
-      case 5: launch_pair<T, K_AOS, 5>(tab, ctas, ph, flags, stage, np, st, after_fluxes); break;
-      default: launch_pair<T, K_AOS, 0>(tab, ctas, ph, flags, stage, np, st, after_fluxes);
+      case 1: launch_pair<T, K_AOS, 1>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 2: launch_pair<T, K_AOS, 2>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 3: launch_pair<T, K_AOS, 3>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 4: launch_pair<T, K_AOS, 4>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 5: launch_pair<T, K_AOS, 5>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      default: launch_pair<T, K_AOS, 0>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes);
     }
   }
   return prims_ready ? 2 : 3;
@@ -969,7 +1027,7 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
   for (int base = 0; base < nblocks; base += kMaxSplitBlocks) {
     Table tab;
     tab.n = std::min(kMaxSplitBlocks, nblocks - base);
-    int ctas = 0;
+    int ctas = 0, asm_ctas = 0;
     const bool k_aos = blocks[base].kaos != nullptr;
     for (int t = 0; t < tab.n; ++t) {
       const SplitBlock& sb = blocks[base + t];
@@ -980,18 +1038,21 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
         return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "metric records on some blocks only");
       tab.b[t].blk = sb;
       tab.b[t].blk.cta_begin = ctas;
+      tab.b[t].blk.cta_begin_asm = asm_ctas;
       tab.b[t].dk.init((uint32_t)sb.nk);
       tab.b[t].dj.init((uint32_t)sb.nj);
       const int64_t N = (int64_t)sb.ni * sb.nj * sb.nk;
       ctas += (int)((N + kSplitThreads - 1) / kSplitThreads);
+      asm_ctas += (int)((N + kAsmCells - 1) / kAsmCells);
     }
     if (k_aos && sizeof(T) == 8)
       return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "the FP64 split path reads kxyz directly");
     // the event marks the first chunk's flux launch
     cudaEvent_t ev = base == 0 ? after_fluxes : nullptr;
-    ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st, ev)
-                           : launch_tab<T, false>(tab, ctas, ph, flags, stage, prims_ready, next_prims, variant, st,
-                                                  ev);
+    ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, asm_ctas, ph, flags, stage, prims_ready, next_prims,
+                                                 variant, st, ev)
+                           : launch_tab<T, false>(tab, ctas, asm_ctas, ph, flags, stage, prims_ready, next_prims,
+                                                  variant, st, ev);
     int s = launch_status(ctx, "split stage launch");
     if (s != FJ_OK) return s;
   }
@@ -1042,7 +1103,7 @@ size_t split_metric_record_bytes(int precision, int64_t N) {
 // arrays (FP64).
 static void split_counts(int precision, int& nP, int& nF, int& nG) {
   const bool rec = precision == FJ_PREC_F32FLUX;
-  nP = rec ? kRecP : kRecP64;
+  nP = rec ? 2 * kRecP : kRecP64;  // FP32: the stage input's primitives and the next stage's
   nF = rec ? kRecF : 15;
   nG = 9;  // records: kRecG per cell in G, then one per cell in Gz
 }
@@ -1068,7 +1129,9 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
   int64_t off = 0;
   for (int b = 0; b < nblocks; ++b) {
     const int64_t N = (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
-    blocks[b].prim = prim + nP * off * t;  // records are multiples of 16 bytes
+    // records are multiples of 16 bytes; FP32: [input | next] primitive records
+    blocks[b].prim = prim + (precision == FJ_PREC_F32FLUX ? kRecP : nP) * off * t;
+    blocks[b].prim_next = precision == FJ_PREC_F32FLUX ? prim + (kRecP * total + kRecP * off) * t : blocks[b].prim;
     blocks[b].F = F + nF * off * t;
     if (precision == FJ_PREC_F32FLUX) {
       blocks[b].G = G + kRecG * off * t;
