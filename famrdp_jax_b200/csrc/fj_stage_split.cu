@@ -457,19 +457,18 @@ struct GlobalSrc {
 // The assembly of one cell (rhs/invscd.py:119-131, rhs/viscous.py:86-117,
 // solver/step.py:45-53) from the intermediates Src provides.
 // fk_m / fk_p: the k faces c-1 | c and c | c+1 (the flux records hold only the
-// i and j faces).
+// i and j faces); kk / gcl: the metric record of c, loaded by the caller.
 template <typename T, bool K_AOS, class Src>
 __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x, const Src& src, int flags,
                                               int stage, int next_prims, double gm1, double R, double iR,
-                                              double ph_p_ref, const T fk_m[5], const T fk_p[5]) {
+                                              double ph_p_ref, const T fk_m[5], const T fk_p[5], const T kk[9],
+                                              const T gcl[3]) {
   const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
   const int32_t si = x.nj * x.nk, sj = x.nk;
   const int n[3] = {x.ni, x.nj, x.nk};
   const int idx[3] = {x.i, x.j, x.k};
   const int32_t st[3] = {si, sj, 1};
   double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  T kk[9], gcl[3] = {T(0), T(0), T(0)};
-  src.K9(c, kk, K_AOS ? gcl : nullptr);
   if (flags & kRhsInvscd) {
     const bool on[3] = {idx[0] >= 2 && idx[0] <= n[0] - 3, idx[1] >= 2 && idx[1] <= n[1] - 3,
                         idx[2] >= 2 && idx[2] <= n[2] - 3};
@@ -568,16 +567,16 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
 
 // With next_prims, also writes the primitives of the stage result (the next
 // stage's input) in place of a separate k_split_prims launch.
-// The k face c | c+1 (rhs/invscd.py:62-100) from the stage input's primitive
-// records of c-1 .. c+2 and the k rows of the metrics of c and c+1.
+// The k face c-1 | c (rhs/invscd.py:62-100) from the stage input's primitive
+// records of c-2 .. c+1, the k row of the metrics of c-1 and kr, that of c.
 template <typename T, bool K_AOS>
-__device__ __forceinline__ void k_face(const SplitBlock& B, int32_t N, int32_t c, const Phys& ph, T F[5]) {
+__device__ __forceinline__ void k_face_left(const SplitBlock& B, int32_t N, int32_t c, const T kr[3],
+                                            const Phys& ph, T F[5]) {
   const T* __restrict__ P = (const T*)B.prim;
-  const Cell6<T> a0 = load_cell<T>(P, c - 1), a1 = load_cell<T>(P, c), a2 = load_cell<T>(P, c + 1),
-                 a3 = load_cell<T>(P, c + 2);
-  T kl[3], kr[3];
-  metric_row<T, K_AOS>(B, N, 2, c, kl);
-  metric_row<T, K_AOS>(B, N, 2, c + 1, kr);
+  const Cell6<T> a0 = load_cell<T>(P, c - 2), a1 = load_cell<T>(P, c - 1), a2 = load_cell<T>(P, c),
+                 a3 = load_cell<T>(P, c + 1);
+  T kl[3];
+  metric_row<T, K_AOS>(B, N, 2, c - 1, kl);
   face_from_cells<T, K_AOS>(a0, a1, a2, a3, kl, kr, ph, F, K_AOS ? (T)ph.p_ref : T(0));
 }
 
@@ -626,15 +625,18 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
     x.nj = B.nj;
     x.nk = B.nk;
   }
+  const GlobalSrc<T, K_AOS> src{B, (int32_t)N};
+  T kk[9], gcl[3] = {T(0), T(0), T(0)};
+  if (alive) src.K9((int32_t)c, kk, K_AOS ? gcl : nullptr);
   T fl[5] = {T(0), T(0), T(0), T(0), T(0)}, fr[5];
   // face c-1 | c exists for k-1 in [1, nk-3]
   if ((flags & kRhsInvscd) && alive && x.k >= 2 && x.k <= x.nk - 2)
-    k_face<T, K_AOS>(B, (int32_t)N, (int32_t)c - 1, ph, fl);
+    k_face_left<T, K_AOS>(B, (int32_t)N, (int32_t)c, kk + 6, ph, fl);
 #pragma unroll
   for (int v = 0; v < 5; ++v) fr[v] = __shfl_down_sync(0xffffffffu, fl[v], 1);
   if (lane == 31 || !alive) return;
-  const GlobalSrc<T, K_AOS> src{B, (int32_t)N};
-  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, iR, K_AOS ? ph.p_ref : 0.0, fl, fr);
+  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, iR, K_AOS ? ph.p_ref : 0.0, fl, fr, kk,
+                          gcl);
 }
 
 // ---- field-major variant (the FP64 path) ----------------------------------
