@@ -984,7 +984,7 @@ __global__ void k_fold_sum(const double* __restrict__ part, int n, double* __res
 struct SplitShape {
   int flux_occ, asm_occ;
 };
-constexpr SplitShape kSplitVariants[] = {{3, 6}, {3, 4}, {4, 4}, {3, 5}, {4, 6}, {3, 8}};
+constexpr SplitShape kSplitVariants[] = {{4, 4}, {3, 4}, {3, 6}, {3, 5}, {4, 6}, {3, 8}};
 static_assert(sizeof(kSplitVariants) / sizeof(kSplitVariants[0]) == FJ_NUM_SPLIT_VARIANTS, "variant table");
 
 template <typename T, bool K_AOS, int V>
