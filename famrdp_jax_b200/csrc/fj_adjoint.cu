@@ -57,6 +57,37 @@ __device__ __forceinline__ void wrapped(int c, int i, int j, int k, const ADims&
   nb[5] = k == 0 ? c + (d.nk - 1) : c - 1;
 }
 
+// The primitives (rho, u, v, w, p, T) of the forward evaluation: in FP32 one
+// 32-byte record per cell (two pad values), moved with one 256-bit load or
+// store that covers whole sectors; in FP64 six field-major arrays.
+template <typename T>
+constexpr int kPVals = sizeof(T) == 4 ? 8 : 6;  // values per cell in the primitive buffer
+
+template <typename T>
+__device__ __forceinline__ void load_prims(const T* __restrict__ P, int N, int c, T x[6]) {
+  if constexpr (sizeof(T) == 4) {
+    float v6, v7;
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(x[0]), "=f"(x[1]), "=f"(x[2]), "=f"(x[3]), "=f"(x[4]), "=f"(x[5]), "=f"(v6), "=f"(v7)
+        : "l"(P + (size_t)c * 8));
+  } else {
+#pragma unroll
+    for (int f = 0; f < 6; ++f) x[f] = P[(size_t)f * N + c];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_prims(T* __restrict__ P, int N, int c, const T x[6]) {
+  if constexpr (sizeof(T) == 4) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(P + (size_t)c * 8), "f"(x[0]),
+                 "f"(x[1]), "f"(x[2]), "f"(x[3]), "f"(x[4]), "f"(x[5]), "f"(0.0f), "f"(0.0f)
+                 : "memory");
+  } else {
+#pragma unroll
+    for (int f = 0; f < 6; ++f) P[(size_t)f * N + c] = x[f];
+  }
+}
+
 // With lv, also lv = lam / (vol + 1e-300) per cell, in FP64: the face adjoint
 // -lam(c)/vol(c) + lam(c+e_a)/vol(c+e_a) of every axis then costs one FP64
 // subtraction per face instead of two divisions.
@@ -77,12 +108,8 @@ __global__ void k_adj_prims(const double* __restrict__ q, T* __restrict__ P, int
   const double r = q[c], ir = 1.0 / r;
   const double u = q[N + c] * ir, v = q[2 * N + c] * ir, w = q[3 * N + c] * ir;
   const double p = gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
-  P[c] = (T)r;
-  P[N + c] = (T)u;
-  P[2 * N + c] = (T)v;
-  P[3 * N + c] = (T)w;
-  P[4 * N + c] = (T)p;
-  P[5 * N + c] = (T)(r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300);
+  const T x[6] = {(T)r, (T)u, (T)v, (T)w, (T)p, (T)(r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300)};
+  store_prims<T>(P, N, c, x);
 }
 
 __device__ __forceinline__ void atomic_add(float* a, float v) { atomicAdd(a, v); }
@@ -98,7 +125,9 @@ __device__ __forceinline__ void face_vjp_cells(const T* __restrict__ P, const do
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
     const int cc = c + (s - 1) * sa;
-    cell[s] = Prim<T>{P[cc], P[N + cc], P[2 * N + cc], P[3 * N + cc], P[4 * N + cc]};
+    T x[6];
+    load_prims<T>(P, N, cc, x);
+    cell[s] = Prim<T>{x[0], x[1], x[2], x[3], x[4]};
     l4[s] = Prim<T>{T(0), T(0), T(0), T(0), T(0)};
   }
   const int cr = c + sa;
@@ -152,7 +181,10 @@ __global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, c
       for (int m = 0; m < 3; ++m) l2_prefetch(kxyz + (size_t)(3 * a + m) * N + a1, m1 * 8);
     }
     if (m2 > 0)
-      for (int v = 0; v < 5; ++v) l2_prefetch(P + (size_t)v * N + a2, m2 * (int)sizeof(T));
+      if constexpr (sizeof(T) == 4)
+        l2_prefetch(P + (size_t)a2 * 8, m2 * 32);
+      else
+        for (int v = 0; v < 5; ++v) l2_prefetch(P + (size_t)v * N + a2, m2 * (int)sizeof(T));
   }
   T lc[4][5];
 #pragma unroll
@@ -239,10 +271,13 @@ __device__ __forceinline__ double adj_visc_cell(const T* __restrict__ P, const d
   const int fld[4] = {1, 2, 3, 5};
   T dd[4][3];
 #pragma unroll
-  for (int s = 0; s < 4; ++s)
+  for (int l = 0; l < 3; ++l) {
+    T xp[6], xm[6];
+    load_prims<T>(P, N, nb[2 * l], xp);
+    load_prims<T>(P, N, nb[2 * l + 1], xm);
 #pragma unroll
-    for (int l = 0; l < 3; ++l)
-      dd[s][l] = T(0.5) * (P[fld[s] * N + nb[2 * l]] - P[fld[s] * N + nb[2 * l + 1]]);
+    for (int s = 0; s < 4; ++s) dd[s][l] = T(0.5) * (xp[fld[s]] - xm[fld[s]]);
+  }
   T kk[9];
 #pragma unroll
   for (int lm = 0; lm < 9; ++lm) kk[lm] = (T)kxyz[lm * N + y];
@@ -251,7 +286,9 @@ __device__ __forceinline__ double adj_visc_cell(const T* __restrict__ P, const d
   for (int s = 0; s < 4; ++s)
 #pragma unroll
     for (int m = 0; m < 3; ++m) g[s][m] = dd[s][0] * kk[m] + dd[s][1] * kk[3 + m] + dd[s][2] * kk[6 + m];
-  const T u = P[N + y], v = P[2 * N + y], w = P[3 * N + y], Tt = P[5 * N + y];
+  T xy[6];
+  load_prims<T>(P, N, y, xy);
+  const T u = xy[1], v = xy[2], w = xy[3], Tt = xy[5];
   T mu = (T)ph.mu0, dmu_dT = T(0);
   if (ph.visc_law == 0) {
     const T r = Tt * (T)ph.inv_T0;
@@ -325,8 +362,12 @@ __global__ void __launch_bounds__(kAT, MB) k_adj_visc(const T* __restrict__ P, c
     if (m1 > 0) {
       for (int v = 1; v < 5; ++v) l2_prefetch(lam + (size_t)v * N + a1, m1 * 8);
       for (int lm = 0; lm < 9; ++lm) l2_prefetch(kxyz + (size_t)lm * N + a1, m1 * 8);
-      const int fld[4] = {1, 2, 3, 5};
-      for (int s = 0; s < 4; ++s) l2_prefetch(P + (size_t)fld[s] * N + a1, m1 * (int)sizeof(T));
+      if constexpr (sizeof(T) == 4) {
+        l2_prefetch(P + (size_t)a1 * 8, m1 * 32);
+      } else {
+        const int fld[4] = {1, 2, 3, 5};
+        for (int s = 0; s < 4; ++s) l2_prefetch(P + (size_t)fld[s] * N + a1, m1 * (int)sizeof(T));
+      }
     }
   }
   double dot = 0.0;
@@ -452,7 +493,7 @@ __global__ void k_ke_grad(const double* __restrict__ q, const double* __restrict
 
 template <typename T>
 size_t vjp_ws(int64_t N) {
-  return ((6 + 5 + 12 + 4) * (size_t)N) * sizeof(T) + 5 * (size_t)N * sizeof(double) + 5 * 256;
+  return ((kPVals<T> + 5 + 12 + 4) * (size_t)N) * sizeof(T) + 5 * (size_t)N * sizeof(double) + 5 * 256;
 }
 
 template <typename T>
@@ -463,7 +504,7 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
   auto al = [](char* p) { return (char*)(((uintptr_t)p + 255) & ~(uintptr_t)255); };
   char* p = al((char*)ws);
   T* P = (T*)p;
-  p = al(p + 6 * (size_t)N * sizeof(T));
+  p = al(p + kPVals<T> * (size_t)N * sizeof(T));
   T* lamP = (T*)p;
   p = al(p + 5 * (size_t)N * sizeof(T));
   T* lamD = (T*)p;
