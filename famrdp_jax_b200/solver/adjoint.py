@@ -138,8 +138,10 @@ class _Run:
     _ping: list | None = None
     _saved: list | None = None
     # the last segment's saved states, kept by the forward sweep (the reverse
-    # sweep starts there, so that segment is not recomputed)
+    # sweep starts there, so that segment is not recomputed), and the one
+    # before it when the second pool exists
     _last_states: list | None = None
+    _prev_states: list | None = None
     # the reverse sweep's second saved-state pool and the stream it recomputes
     # segments on (overlap=False, or too little memory for the second pool:
     # segments are recomputed on the caller's stream between the adjoints)
@@ -195,9 +197,10 @@ def _reverse_sweep(run: _Run, checkpoints, lams):
     through its saved states while segment s-1 is recomputed from its
     checkpoint on a second stream into the other saved-state pool (the two
     chains are independent, so the recompute's memory-bound kernels share the
-    GPU with the adjoint's arithmetic-bound ones).  The last segment's states
-    come from the forward sweep.  The adjoint ping-pongs between two working
-    copies, so each step adjoint writes its result straight into the other."""
+    GPU with the adjoint's arithmetic-bound ones).  The last two segments'
+    states come from the forward sweep (one in each pool).  The adjoint
+    ping-pongs between two working copies, so each step adjoint writes its
+    result straight into the other."""
     lams = [l.clone() for l in lams]
     spare = [torch.empty_like(l) for l in lams]
     nseg = len(checkpoints)
@@ -213,9 +216,12 @@ def _reverse_sweep(run: _Run, checkpoints, lams):
     else:
         _, states = _forward_segment(run, checkpoints[s], seg_len[s], keep=True, pool=pool_a)
     pools = (pool_a, pool_b) if states[0] is pool_a[0] else (pool_b, pool_a)
+    prev, run._prev_states = run._prev_states, None
     for s in reversed(range(nseg)):
         done = None
-        if s > 0:
+        if s == nseg - 1 and s > 0 and prev is not None and len(prev) == seg_len[s - 1] and prev[0] is pools[1][0]:
+            nxt = prev  # kept by the forward sweep in the other pool
+        elif s > 0:
             # the other pool was last read by segment s+1's adjoints, queued on main
             side.wait_stream(main)
             with torch.cuda.stream(side):
@@ -226,8 +232,9 @@ def _reverse_sweep(run: _Run, checkpoints, lams):
             step_vjp_saved(states.pop(), run.metrics, run.cfg, run.dt, lams, tables=run.tables, dmu=run.dmu,
                            mu0s=run.plan.mu0s, dts=run.plan.dts, out=spare)
             lams, spare = spare, lams
-        if done is not None:
-            main.wait_event(done)
+        if s > 0:
+            if done is not None:
+                main.wait_event(done)
             states, pools = nxt, (pools[1], pools[0])
     return lams
 
@@ -249,17 +256,25 @@ def _reverse_sweep_serial(run: _Run, checkpoints, lams, spare, seg_len, pool):
 
 
 def _forward_with_checkpoints(run: _Run, q0s):
+    """The forward sweep: a checkpoint at the start of every segment; the last
+    segment keeps its stage states in the first pool and, when the reverse
+    sweep's second pool is available (it is allocated here), the segment
+    before it keeps its own there, so the reverse sweep recomputes neither."""
     checkpoints = []
     cur = [q.detach() for q in q0s]
     done = 0
-    run._last_states = None
-    while done < run.nsteps:
+    run._last_states = run._prev_states = None
+    nseg = -(-run.nsteps // run.every)
+    pool_b = run.reverse_buffers(cur)[0] if nseg >= 2 else None
+    for seg in range(nseg):
         checkpoints.append([q.clone() for q in cur])
         n = min(run.every, run.nsteps - done)
-        last = done + n >= run.nsteps
-        cur, states = _forward_segment(run, cur, n, keep=last)
-        if last:
-            run._last_states = states
+        if seg == nseg - 1:
+            cur, run._last_states = _forward_segment(run, cur, n, keep=True)
+        elif seg == nseg - 2 and pool_b is not None:
+            cur, run._prev_states = _forward_segment(run, cur, n, keep=True, pool=pool_b)
+        else:
+            cur, _ = _forward_segment(run, cur, n, keep=False)
         done += n
     return [q.clone() for q in cur], checkpoints
 
