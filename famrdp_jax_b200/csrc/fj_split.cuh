@@ -27,7 +27,9 @@ struct SplitBlock {
   void* prim_next;       // where the assembly writes the next stage's primitives: a
                          // second buffer in FP32 (the FP32 assembly also reads prim),
                          // prim itself in FP64
-  void* F;               // scratch: 15 x N (face c | c+e_a, axis-major)
+  void* F;               // scratch: FP64 15 x N (face c | c+e_a, axis-major); FP32 records of
+                         // the i face and the first three j-face components (8 per cell)
+  void* Fz;              // FP32 only: the last two j-face components, two per cell
   void* G;               // scratch: viscous flux components (records: 8 per cell)
   void* Gz;              // records only: the ninth component, one per cell
   double mu0;            // viscosity scale of this block (per-instance ensembles)

@@ -98,6 +98,9 @@ __device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x) {
 
 // ---- record access -------------------------------------------------------
 constexpr int kRecP = 8, kRecF = 16, kRecG = 8;  // G: 8 components per record + 1 in Gz
+// FP32 face fluxes (the k faces are evaluated in the assembly): a 32-byte record
+// (i face 0..4, j face 0..2) and a pair (j face 3..4) per cell
+constexpr int kRecFA = 8, kRecFB = 2;
 constexpr int kRecP64 = 6;  // FP64 primitive record: rho, u, v, w, p, T (48 bytes)
 
 // The L2 fills of the flux CTA `cta` of block d (thread 0 only): the
@@ -163,7 +166,8 @@ __device__ __forceinline__ void prefetch_assembly(const Dev& d, int cta, int fla
     if (K_AOS) l2_prefetch((const T*)B.kaos + c0 * kRecK<T>, n * kRecK<T> * (int64_t)sizeof(T));
     if (flags & kRhsInvscd) {
       l2_prefetch(B.vol + c0, n * 8);
-      l2_prefetch((const T*)B.F + c0 * kRecF, n * kRecF * (int64_t)sizeof(T));
+      l2_prefetch((const T*)B.F + c0 * kRecFA, n * kRecFA * (int64_t)sizeof(T));
+      l2_prefetch((const T*)B.Fz + c0 * kRecFB, n * kRecFB * (int64_t)sizeof(T));
     }
     if ((flags & kRhsViscous) && m > 0) {
       l2_prefetch((const T*)B.G + a * kRecG, m * kRecG * (int64_t)sizeof(T));
@@ -394,9 +398,9 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
     // the faces c | c+e_i and c | c+e_j for c_a in [1, n_a - 3]; invalid faces
     // are stored as zeros (never read).  The k faces are left to the
     // assembly, whose issue slots are mostly idle (this kernel is issue-bound)
-    T Fr[kRecF];
+    T Fr[kRecFA + kRecFB];
 #pragma unroll
-    for (int v = 0; v < kRecF; ++v) Fr[v] = T(0);
+    for (int v = 0; v < kRecFA + kRecFB; ++v) Fr[v] = T(0);
     T kn[3];
     // with metric records the primitives carry p' = p - p_ref and the FP64
     // correction of the momentum fluxes is in the records
@@ -411,7 +415,8 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
       metric_row<T, K_AOS>(B, N, 1, c + sj, kn);
       face_from_cells<T, K_AOS>(Jm, C0, Jp, J2, kk + 3, kn, ph, Fr + 5, p_ref);
     }
-    st_rec<T, kRecF>((T*)B.F + (size_t)c * kRecF, Fr);
+    st_rec<T, kRecFA>((T*)B.F + (size_t)c * kRecFA, Fr);
+    reinterpret_cast<float2*>(B.Fz)[c] = make_float2(Fr[8], Fr[9]);
   }
 }
 
@@ -424,30 +429,29 @@ template <typename T, bool K_AOS>
 struct GlobalSrc {
   const SplitBlock& B;
   int32_t N;
-  __device__ __forceinline__ void F_rec(int32_t c, T* o) const { ld_rec<T, kRecF>((const T*)B.F + (size_t)c * kRecF, o); }
-  // the five components of face a of the record of cell c (floats 5a..5a+4),
-  // (faces 0 and 2: one 256-bit load of their half; face 1: two 16-byte loads)
+  // the i and j faces of cell c: o[0..9]
+  __device__ __forceinline__ void F_rec(int32_t c, T* o) const {
+    ld_rec<T, kRecFA>((const T*)B.F + (size_t)c * kRecFA, o);
+    const float2 z = __ldg(reinterpret_cast<const float2*>(B.Fz) + c);
+    o[8] = z.x;
+    o[9] = z.y;
+  }
+  // the five components of face a (0: i, 1: j) of cell c
   __device__ __forceinline__ void F_axis(int32_t c, int a, T* o) const {
-    const T* p = (const T*)B.F + (size_t)c * kRecF;
-    if constexpr (sizeof(T) == 4) {
-      if (a != 1) {
-        // faces 0 and 2 lie in one 32-byte half of the record: one 256-bit load
-        float w[8];
-        ld_rec<T, 8>(p + (a == 0 ? 0 : 8), w);
+    const T* p = (const T*)B.F + (size_t)c * kRecFA;
+    if (a == 0) {  // one 256-bit load of the record
+      float w[8];
+      ld_rec<T, 8>(p, w);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) o[v] = w[(a == 0 ? 0 : 2) + v];
-      } else {
-        const float4 x = __ldg(reinterpret_cast<const float4*>(p) + 1);  // floats 4..7
-        const float4 y = __ldg(reinterpret_cast<const float4*>(p) + 2);  // floats 8..11
-        o[0] = x.y;
-        o[1] = x.z;
-        o[2] = x.w;
-        o[3] = y.x;
-        o[4] = y.y;
-      }
-    } else {
-#pragma unroll
-      for (int v = 0; v < 5; ++v) o[v] = p[5 * a + v];
+      for (int v = 0; v < 5; ++v) o[v] = w[v];
+    } else {  // floats 5..7 of the record and the pair
+      const float4 x = __ldg(reinterpret_cast<const float4*>(p) + 1);  // floats 4..7
+      const float2 z = __ldg(reinterpret_cast<const float2*>(B.Fz) + c);
+      o[0] = x.y;
+      o[1] = x.z;
+      o[2] = x.w;
+      o[3] = z.x;
+      o[4] = z.y;
     }
   }
   __device__ __forceinline__ void G_rec(int32_t c, T* o) const { ld_rec<T, kRecG>((const T*)B.G + (size_t)c * kRecG, o); }
@@ -1106,7 +1110,7 @@ size_t split_metric_record_bytes(int precision, int64_t N) {
 static void split_counts(int precision, int& nP, int& nF, int& nG) {
   const bool rec = precision == FJ_PREC_F32FLUX;
   nP = rec ? 2 * kRecP : kRecP64;  // FP32: the stage input's primitives and the next stage's
-  nF = rec ? kRecF : 15;
+  nF = rec ? kRecFA + kRecFB : 15;
   nG = 9;  // records: kRecG per cell in G, then one per cell in Gz
 }
 
@@ -1134,7 +1138,13 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
     // records are multiples of 16 bytes; FP32: [input | next] primitive records
     blocks[b].prim = prim + (precision == FJ_PREC_F32FLUX ? kRecP : nP) * off * t;
     blocks[b].prim_next = precision == FJ_PREC_F32FLUX ? prim + (kRecP * total + kRecP * off) * t : blocks[b].prim;
-    blocks[b].F = F + nF * off * t;
+    if (precision == FJ_PREC_F32FLUX) {
+      blocks[b].F = F + kRecFA * off * t;
+      blocks[b].Fz = F + (kRecFA * total + kRecFB * off) * t;
+    } else {
+      blocks[b].F = F + nF * off * t;
+      blocks[b].Fz = nullptr;
+    }
     if (precision == FJ_PREC_F32FLUX) {
       blocks[b].G = G + kRecG * off * t;
       blocks[b].Gz = G + (kRecG * total + off) * t;
