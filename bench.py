@@ -69,9 +69,9 @@ STEP_BYTES = {"f64": 560.0, "f32": 452.0}
 # DRAM bytes per padded cell of one stage-2 launch group (dram__bytes_read +
 # dram__bytes_write summed over the primitive, flux and assembly kernels),
 # measured by ncu on `bench.py --stage-only --n 96` (4 blocks of 100^3 padded
-# cells, 4.0 M) and scaled per cell: FP32 59 + 169 + 309 B, FP64 74 + 301 +
+# cells, 4.0 M) and scaled per cell: FP32 59 + 147 + 283 B, FP64 74 + 301 +
 # 401 B
-STAGE_TRAFFIC = {"f32": 538.0, "f64": 777.0}
+STAGE_TRAFFIC = {"f32": 489.0, "f64": 777.0}
 
 
 def _peaks():
