@@ -161,20 +161,20 @@ __device__ __forceinline__ void add_cell(T* __restrict__ lamP, int N, int c, con
 // (faces at the ends of a k row are invalid and contribute zero, so a warp that
 // spans two rows combines correctly); along i and j each face adds its four
 // cells' adjoints atomically.
-template <typename T, int NT, int MB>
-__global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, const double* __restrict__ kxyz,
-                                                      const double* __restrict__ lv, T* __restrict__ lamP, ADims d,
-                                                      Phys ph) {
+// (a, bx) = the face axis and the block of faces this CTA takes.
+template <typename T>
+__device__ __forceinline__ void adj_faces_body(const T* __restrict__ P, const double* __restrict__ kxyz,
+                                               const double* __restrict__ lv, T* __restrict__ lamP,
+                                               const ADims& d, const Phys& ph, int a, int bx) {
   const int N = d.ni * d.nj * d.nk;
-  if (blockIdx.x * blockDim.x >= (unsigned)N) return;  // whole block past the end (uniform)
-  const int a = blockIdx.y;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bx * (int)blockDim.x >= N) return;  // whole block past the end (uniform)
+  const int c = bx * blockDim.x + threadIdx.x;
   const int n_a = a == 0 ? d.ni : (a == 1 ? d.nj : d.nk);
   const int sa = a == 0 ? d.nj * d.nk : (a == 1 ? d.nk : 1);
   if (threadIdx.x == 0) {
     // L2 fills of the ranges this CTA reaches first: lam/vol and the metric
     // row one cell ahead along a, the primitives two ahead
-    const int c0 = blockIdx.x * blockDim.x, n = min((int)blockDim.x, N - c0);
+    const int c0 = bx * blockDim.x, n = min((int)blockDim.x, N - c0);
     const int a1 = c0 + sa, m1 = min(n, N - a1), a2 = c0 + 2 * sa, m2 = min(n, N - a2);
     if (m1 > 0) {
       for (int v = 0; v < 5; ++v) l2_prefetch(lv + (size_t)v * N + a1, m1 * 8);
@@ -227,6 +227,13 @@ __global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, c
   if (lane == 0) add_cell<T>(lamP, N, c - 1, lc[0]);  // nonzero only for a valid face, so c >= 1
   if (lane == 31) add_cell<T>(lamP, N, c + 1, lc[2]);
   if (lane >= 30) add_cell<T>(lamP, N, c + 2, lc[3]);
+}
+
+template <typename T, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB) k_adj_faces(const T* __restrict__ P, const double* __restrict__ kxyz,
+                                                      const double* __restrict__ lv, T* __restrict__ lamP, ADims d,
+                                                      Phys ph) {
+  adj_faces_body<T>(P, kxyz, lv, lamP, d, ph, blockIdx.y, blockIdx.x);
 }
 
 // lamD: 12 x N (s-major: u, v, w, T; l = 0..2), lamL: 4 x N (local u, v, w, T).
@@ -349,16 +356,17 @@ __device__ __forceinline__ double adj_visc_cell(const T* __restrict__ P, const d
   return dot;
 }
 
-template <typename T, int MB = 1>
-__global__ void __launch_bounds__(kAT, MB) k_adj_visc(const T* __restrict__ P, const double* __restrict__ kxyz,
-                                                     const double* __restrict__ lam, T* __restrict__ lamD,
-                                                     T* __restrict__ lamL, ADims d, Phys ph,
-                                                     double* __restrict__ dmu, double mu_scale) {
+// bx = the block of cells this CTA takes (blockDim.x a multiple of 32)
+template <typename T>
+__device__ __forceinline__ void adj_visc_body(const T* __restrict__ P, const double* __restrict__ kxyz,
+                                              const double* __restrict__ lam, T* __restrict__ lamD,
+                                              T* __restrict__ lamL, const ADims& d, const Phys& ph,
+                                              double* __restrict__ dmu, double mu_scale, int bx) {
   const int N = d.ni * d.nj * d.nk;
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = bx * blockDim.x + threadIdx.x;
   if (threadIdx.x == 0) {
     // L2 fills one i-plane ahead (nearer neighbours were fetched by earlier CTAs)
-    const int a1 = blockIdx.x * blockDim.x + d.nj * d.nk, m1 = min((int)blockDim.x, N - a1);
+    const int a1 = bx * blockDim.x + d.nj * d.nk, m1 = min((int)blockDim.x, N - a1);
     if (m1 > 0) {
       for (int v = 1; v < 5; ++v) l2_prefetch(lam + (size_t)v * N + a1, m1 * 8);
       for (int lm = 0; lm < 9; ++lm) l2_prefetch(kxyz + (size_t)lm * N + a1, m1 * 8);
@@ -377,6 +385,33 @@ __global__ void __launch_bounds__(kAT, MB) k_adj_visc(const T* __restrict__ P, c
     for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
     if ((threadIdx.x & 31) == 0 && dot != 0.0) atomicAdd(dmu, mu_scale * dot);
   }
+}
+
+template <typename T, int MB = 1>
+__global__ void __launch_bounds__(kAT, MB) k_adj_visc(const T* __restrict__ P, const double* __restrict__ kxyz,
+                                                     const double* __restrict__ lam, T* __restrict__ lamD,
+                                                     T* __restrict__ lamL, ADims d, Phys ph,
+                                                     double* __restrict__ dmu, double mu_scale) {
+  adj_visc_body<T>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale, blockIdx.x);
+}
+
+// The face VJPs of the three axes and the viscous VJP in one launch of kAT-
+// thread CTAs: CTA b takes task b % 4 (face axis 0, 1, 2, or the viscous VJP)
+// over block b / 4 of cells, so every residency wave mixes the issue-bound
+// face work with the load-bound viscous work on the same SMs and reads the
+// same primitive, metric and adjoint ranges for all four tasks.  The tasks
+// write disjoint arrays (lamP by atomics; lamD, lamL), so their order does not
+// matter.
+template <typename T, int MB>
+__global__ void __launch_bounds__(kAT, MB)
+    k_adj_faces_visc(const T* __restrict__ P, const double* __restrict__ kxyz, const double* __restrict__ lv,
+                     T* __restrict__ lamP, const double* __restrict__ lam, T* __restrict__ lamD,
+                     T* __restrict__ lamL, ADims d, Phys ph, double* __restrict__ dmu, double mu_scale) {
+  const int task = blockIdx.x & 3, bx = blockIdx.x >> 2;
+  if (task < 3)
+    adj_faces_body<T>(P, kxyz, lv, lamP, d, ph, task, bx);
+  else
+    adj_visc_body<T>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale, bx);
 }
 
 template <typename T>
@@ -517,7 +552,17 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
   const bool inv = (flags & kRhsInvscd) != 0;
   k_adj_prims<T><<<grid, kAT, 0, st>>>(q, P, N, ph.gm1, ph.R, lam, vol, inv ? lv : nullptr, inv ? lamP : nullptr);
   ctx->launches += 1;
-  if (flags & kRhsInvscd) {
+  int rest = flags;  // the parts still to launch
+  if constexpr (sizeof(T) == 4) {
+    if (ctx->adj_variant == 0 && (flags & kRhsInvscd) && (flags & kRhsViscous)) {
+      // FP32 default: both VJPs in one launch (80 registers, 3 CTAs of 256 per SM)
+      k_adj_faces_visc<T, 3><<<4 * (unsigned)grid, kAT, 0, st>>>(P, kxyz, lv, lamP, lam, lamD, lamL, d, ph, dmu,
+                                                                mu_scale);
+      ctx->launches += 1;
+      rest &= ~(kRhsInvscd | kRhsViscous);
+    }
+  }
+  if (rest & kRhsInvscd) {
     // register caps (threads per CTA, minimum CTAs per SM): the FP64 face VJP
     // needs ~180 registers uncapped.  Variant 0 is the fastest measured on
     // B200 (TGV 96^3 adjoint sweep): FP64 128 x 4 (128 registers), FP32
@@ -539,7 +584,7 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
     }
     ctx->launches += 1;
   }
-  if (flags & kRhsViscous) {
+  if (rest & kRhsViscous) {
     // variants 0 and 2 cap the viscous VJP at 64 registers (4 CTAs per SM)
     if (ctx->adj_variant == 0 || ctx->adj_variant == 2)
       k_adj_visc<T, 4><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale);

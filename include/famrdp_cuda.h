@@ -141,7 +141,8 @@ int fj_ctx_set_pipeline(fj_ctx* ctx, int pipeline, int seg, int tile);
 /* Launch shape of the RHS adjoint's face and viscous kernels (a tuning knob;
  * results agree to the rounding of atomic accumulation order): 0 = the
  * fastest measured (default; face kernel register-capped per precision,
- * viscous kernel capped at 64 registers), 1 = face kernel uncapped, 2 = the
+ * viscous kernel capped at 64 registers; with FP32 fluxes both VJPs in one
+ * launch of interleaved CTAs), 1 = face kernel uncapped, 2 = the
  * other face cap, 3 = 0 and 4 = 2 with the viscous kernel uncapped.  The
  * reference has no counterpart. */
 #define FJ_NUM_ADJ_VARIANTS 5
