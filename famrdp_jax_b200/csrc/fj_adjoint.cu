@@ -395,15 +395,15 @@ __global__ void __launch_bounds__(kAT, MB) k_adj_visc(const T* __restrict__ P, c
   adj_visc_body<T>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale, blockIdx.x);
 }
 
-// The face VJPs of the three axes and the viscous VJP in one launch of kAT-
+// The face VJPs of the three axes and the viscous VJP in one launch of NT-
 // thread CTAs: CTA b takes task b % 4 (face axis 0, 1, 2, or the viscous VJP)
 // over block b / 4 of cells, so every residency wave mixes the issue-bound
 // face work with the load-bound viscous work on the same SMs and reads the
 // same primitive, metric and adjoint ranges for all four tasks.  The tasks
 // write disjoint arrays (lamP by atomics; lamD, lamL), so their order does not
 // matter.
-template <typename T, int MB>
-__global__ void __launch_bounds__(kAT, MB)
+template <typename T, int NT, int MB>
+__global__ void __launch_bounds__(NT, MB)
     k_adj_faces_visc(const T* __restrict__ P, const double* __restrict__ kxyz, const double* __restrict__ lv,
                      T* __restrict__ lamP, const double* __restrict__ lam, T* __restrict__ lamD,
                      T* __restrict__ lamL, ADims d, Phys ph, double* __restrict__ dmu, double mu_scale) {
@@ -555,9 +555,12 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
   int rest = flags;  // the parts still to launch
   if constexpr (sizeof(T) == 4) {
     if (ctx->adj_variant == 0 && (flags & kRhsInvscd) && (flags & kRhsViscous)) {
-      // FP32 default: both VJPs in one launch (80 registers, 3 CTAs of 256 per SM)
-      k_adj_faces_visc<T, 3><<<4 * (unsigned)grid, kAT, 0, st>>>(P, kxyz, lv, lamP, lam, lamD, lamL, d, ph, dmu,
-                                                                mu_scale);
+      // FP32 default: both VJPs in one launch (80 registers, 3 CTAs of 256 per
+      // SM).  FP64 keeps two launches: its face VJP is bound by the FP64 pipe at
+      // the 128-register cap, and the fused form (128 x 4) measured 4 % slower
+      // on the reverse sweep
+      k_adj_faces_visc<T, kAT, 3><<<4 * (unsigned)grid, kAT, 0, st>>>(P, kxyz, lv, lamP, lam, lamD, lamL, d, ph,
+                                                                     dmu, mu_scale);
       ctx->launches += 1;
       rest &= ~(kRhsInvscd | kRhsViscous);
     }
