@@ -433,9 +433,9 @@ __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ 
       if (m1 > 0)
         for (int f = 0; f < 12; ++f) l2_prefetch(lamD + (size_t)f * N + a1, m1 * (int)sizeof(T));
     }
-    const double* ep[4] = {e.x1, e.y1, e.x2, e.y2};
-    for (int t = 0; t < 4; ++t)
-      if ((t < 2 ? e.o1 : e.o2) && ep[t])
+    const double* ep[5] = {e.x1, e.y1, e.z1, e.x2, e.y2};
+    for (int t = 0; t < 5; ++t)
+      if ((t < 3 ? e.o1 : e.o2) && ep[t])
         for (int f = 0; f < 5; ++f) l2_prefetch(ep[t] + (size_t)f * N + c0, n * 8);
   }
   double lr = 0, lu = 0, lv = 0, lw = 0, lp = 0, lT = 0;
@@ -492,6 +492,7 @@ __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ 
     const int t = f * N + x;
     o1[f] = e.a1 * e.x1[t] + e.e1 * V[f];
     if (e.y1) o1[f] += e.b1 * e.y1[t];
+    if (e.z1) o1[f] += e.c1 * e.z1[t];
     if (e.o2) {
       o2[f] = e.a2 * e.x2[t];
       if (e.y2) o2[f] += e.b2 * e.y2[t];

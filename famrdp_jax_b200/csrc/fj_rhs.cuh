@@ -42,7 +42,7 @@ size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, i
 // ---- adjoint (fj_adjoint.cu, fj_halo.cu) ----
 // Elementwise epilogue of an RHS VJP V = (dL/dq)^T lam, applied in the kernel
 // that produces V instead of writing V:
-//   o1 = a1 x1 + b1 y1 + e1 V        (y1 may be NULL)
+//   o1 = a1 x1 + b1 y1 + c1 z1 + e1 V   (y1, z1 may be NULL)
 //   o2 = a2 x2 + b2 y2               (o2 may be NULL; y2 may be NULL)
 // Every input is read at a cell before any output is written there, so an
 // output may alias an input.
@@ -52,6 +52,8 @@ struct VjpEpilogue {
   double a1 = 0.0;
   const double* y1 = nullptr;
   double b1 = 0.0;
+  const double* z1 = nullptr;
+  double c1 = 0.0;
   double e1 = 1.0;
   double* o2 = nullptr;
   const double* x2 = nullptr;

@@ -42,6 +42,27 @@ def test_rhs_vjp_matches_autograd(cuda_device, limiter, visc_law):
     assert rel_l2(got, ref.numpy()) <= 1e-10
 
 
+@pytest.mark.parametrize("limiter", ["minmod", "vanleer"])
+@pytest.mark.parametrize("visc_law", ["sutherland", "constant"])
+@pytest.mark.parametrize("shape", [(9, 8, 10), (13, 19, 41)])
+def test_f32_rhs_vjp_close_to_autograd(cuda_device, limiter, visc_law, shape):
+    """The FP32-flux RHS VJP (face and viscous VJPs in one launch of
+    interleaved CTAs, FP32 face arithmetic, FP64 lam/vol and final
+    accumulation) against torch.autograd of the FP64 twin, on a block whose k
+    rows do not align with warps.  Bound: relative L2 <= 2e-6 (measured
+    1.4e-7 with minmod, 5.7e-7 with van Leer)."""
+    q, kxyz, vol = random_block(shape, 5)
+    cfg = _cfg(limiter=limiter, visc_law=visc_law, precision="f32")
+    lam = np.random.default_rng(6).standard_normal(q.shape)
+    qt = torch.tensor(q, requires_grad=True)
+    L = TORCH.rhs_block(qt, torch.tensor(kxyz), torch.tensor(vol), cfg)
+    (ref,) = torch.autograd.grad(L, qt, grad_outputs=torch.tensor(lam))
+    m = Metrics(jac=dev(vol), kxyz=dev(kxyz), vol=dev(vol))
+    got = host(adjoint.rhs_vjp(dev(q), m, cfg, dev(lam)))
+    err = rel_l2(got, ref.numpy())
+    assert err <= 2e-6
+
+
 def _mirror_case():
     """One block with farfield, symmetry and adiabatic-wall faces and one
     self-periodic pair."""
@@ -271,6 +292,27 @@ def test_mu_gradient_matches_autograd(cuda_device):
     dmu = torch.zeros(1, dtype=torch.float64, device="cuda")
     adjoint.step_vjp([dev(q) for q in qs], metrics, cfg, dt, [dev(l) for l in lam], dmu=dmu)
     assert abs(float(dmu) - ref) <= 1e-7 * abs(ref), (float(dmu), ref)
+
+
+def test_f32_mu_gradient_close_to_f64(cuda_device):
+    """dJ/dmu0 of one step accumulated by the FP32-flux viscous VJP (inside
+    the combined face + viscous launch) against the FP64 path's, and the
+    step's input adjoint likewise.  Bounds: 1e-6 relative (measured 5.7e-8
+    and 1.7e-8)."""
+    import dataclasses
+    qs, mets, cfg = _periodic_case()
+    dt = 0.5 * NP.cfl_dt(qs, mets, cfg.gas.gamma, 0.5, 2)
+    lam = [np.random.default_rng(5).standard_normal(q.shape) for q in qs]
+    metrics = tuple(Metrics(jac=dev(v), kxyz=dev(k), vol=dev(v)) for k, v in mets)
+    vals, grads = {}, {}
+    for prec in ("f64", "f32"):
+        c2 = dataclasses.replace(cfg, precision=prec)
+        dmu = torch.zeros(1, dtype=torch.float64, device="cuda")
+        grads[prec] = host(adjoint.step_vjp([dev(q) for q in qs], metrics, c2, dt, [dev(l) for l in lam],
+                                            dmu=dmu)[0])
+        vals[prec] = float(dmu)
+    assert abs(vals["f32"] - vals["f64"]) <= 1e-6 * abs(vals["f64"])
+    assert rel_l2(grads["f32"], grads["f64"]) <= 1e-6
 
 
 def test_mach_gradient_matches_finite_differences(cuda_device):
