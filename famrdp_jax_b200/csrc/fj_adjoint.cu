@@ -88,6 +88,17 @@ __device__ __forceinline__ void store_prims(T* __restrict__ P, int N, int c, con
   }
 }
 
+// q -> (rho, u, v, w, p, T) of cell c, in the primitive buffer's layout
+template <typename T>
+__device__ __forceinline__ void write_prims(const double* __restrict__ q, T* __restrict__ P, int N, int c,
+                                            double gm1, double R) {
+  const double r = q[c], ir = 1.0 / r;
+  const double u = q[N + c] * ir, v = q[2 * N + c] * ir, w = q[3 * N + c] * ir;
+  const double p = gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
+  const T x[6] = {(T)r, (T)u, (T)v, (T)w, (T)p, (T)(r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300)};
+  store_prims<T>(P, N, c, x);
+}
+
 // With lv, also lv = lam / (vol + 1e-300) per cell, in FP64: the face adjoint
 // -lam(c)/vol(c) + lam(c+e_a)/vol(c+e_a) of every axis then costs one FP64
 // subtraction per face instead of two divisions.
@@ -105,11 +116,7 @@ __global__ void k_adj_prims(const double* __restrict__ q, T* __restrict__ P, int
 #pragma unroll
     for (int v = 0; v < 5; ++v) lv[v * N + c] = lam[v * N + c] * iv;
   }
-  const double r = q[c], ir = 1.0 / r;
-  const double u = q[N + c] * ir, v = q[2 * N + c] * ir, w = q[3 * N + c] * ir;
-  const double p = gm1 * (q[4 * N + c] - r * (0.5 * (u * u + v * v + w * w)));
-  const T x[6] = {(T)r, (T)u, (T)v, (T)w, (T)p, (T)(r * R > 1e-300 ? p * ir * (1.0 / R) : p * 1e300)};
-  store_prims<T>(P, N, c, x);
+  write_prims<T>(q, P, N, c, gm1, R);
 }
 
 __device__ __forceinline__ void atomic_add(float* a, float v) { atomicAdd(a, v); }
@@ -415,9 +422,9 @@ __global__ void __launch_bounds__(NT, MB)
 }
 
 template <typename T>
-__global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ lamP,
-                            const T* __restrict__ lamD, const T* __restrict__ lamL,
-                            double* __restrict__ out, ADims d, Phys ph, int flags, VjpEpilogue e) {
+__global__ void k_adj_final(const double* __restrict__ q, T* lamP, const T* __restrict__ lamD,
+                            const T* __restrict__ lamL, double* __restrict__ out, T* __restrict__ P,
+                            double* __restrict__ lam_vol, ADims d, Phys ph, int flags, VjpEpilogue e) {
   const int N = d.ni * d.nj * d.nk;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= N) return;
@@ -433,10 +440,11 @@ __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ 
       if (m1 > 0)
         for (int f = 0; f < 12; ++f) l2_prefetch(lamD + (size_t)f * N + a1, m1 * (int)sizeof(T));
     }
-    const double* ep[5] = {e.x1, e.y1, e.z1, e.x2, e.y2};
-    for (int t = 0; t < 5; ++t)
-      if ((t < 3 ? e.o1 : e.o2) && ep[t])
+    const double* ep[6] = {e.x1, e.y1, e.z1, e.x2, e.y2, e.next_q};
+    for (int t = 0; t < 6; ++t)
+      if ((t < 3 || t == 5 ? e.o1 : e.o2) && ep[t])
         for (int f = 0; f < 5; ++f) l2_prefetch(ep[t] + (size_t)f * N + c0, n * 8);
+    if (e.o1 && e.next_q && (flags & kRhsInvscd)) l2_prefetch(e.next_vol + c0, n * 8);
   }
   double lr = 0, lu = 0, lv = 0, lw = 0, lp = 0, lT = 0;
   if (flags & kRhsInvscd) {
@@ -503,6 +511,19 @@ __global__ void k_adj_final(const double* __restrict__ q, const T* __restrict__ 
     e.o1[f * N + x] = o1[f];
     if (e.o2) e.o2[f * N + x] = o2[f];
   }
+  if (e.next_q) {
+    // what the next RHS VJP of this block reads first (its k_adj_prims
+    // launch is skipped); this cell's lamP was read above, by this thread only
+    write_prims<T>(e.next_q, P, N, x, ph.gm1, ph.R);
+    if (flags & kRhsInvscd) {
+      const double iv = 1.0 / (e.next_vol[x] + 1e-300);
+#pragma unroll
+      for (int f = 0; f < 5; ++f) {
+        lam_vol[f * N + x] = o1[f] * iv;
+        lamP[f * N + x] = T(0);
+      }
+    }
+  }
 }
 
 // dJ/dq of J = sum_interior vol * 0.5 |m|^2 / rho
@@ -551,8 +572,10 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
   const ADims d{ni, nj, nk};
   const int grid = grid_for(N, kAT);
   const bool inv = (flags & kRhsInvscd) != 0;
-  k_adj_prims<T><<<grid, kAT, 0, st>>>(q, P, N, ph.gm1, ph.R, lam, vol, inv ? lv : nullptr, inv ? lamP : nullptr);
-  ctx->launches += 1;
+  if (!(epi && epi->ws_ready)) {
+    k_adj_prims<T><<<grid, kAT, 0, st>>>(q, P, N, ph.gm1, ph.R, lam, vol, inv ? lv : nullptr, inv ? lamP : nullptr);
+    ctx->launches += 1;
+  }
   int rest = flags;  // the parts still to launch
   if constexpr (sizeof(T) == 4) {
     if (ctx->adj_variant == 0 && (flags & kRhsInvscd) && (flags & kRhsViscous)) {
@@ -596,7 +619,7 @@ int rhs_vjp_impl(fj_ctx* ctx, const double* q, const double* kxyz, const double*
       k_adj_visc<T><<<grid, kAT, 0, st>>>(P, kxyz, lam, lamD, lamL, d, ph, dmu, mu_scale);
     ctx->launches += 1;
   }
-  k_adj_final<T><<<grid, kAT, 0, st>>>(q, lamP, lamD, lamL, out, d, ph, flags, epi ? *epi : VjpEpilogue{});
+  k_adj_final<T><<<grid, kAT, 0, st>>>(q, lamP, lamD, lamL, out, P, lv, d, ph, flags, epi ? *epi : VjpEpilogue{});
   ctx->launches += 1;
   return launch_status(ctx, "rhs vjp launch");
 }

@@ -980,12 +980,14 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
     //   LB = 2/3 lam + 2/3 dt V3   (q0 receives 1/3 lam, added at stage 1)
     VjpEpilogue e3;
     e3.o1 = LB, e3.x1 = lam_in[b], e3.a1 = 2.0 / 3.0, e3.e1 = 2.0 / 3.0 * dt;
+    e3.next_q = Q1, e3.next_vol = B.vol;  // leaves the stage-2 VJP's inputs in wk
     s = rhs_vjp(ctx, Q2, B.kxyz, B.vol, lam_in[b], nullptr, B.ni, B.nj, B.nk, pp, flags, wk, st, dmu_b,
                 2.0 / 3.0 * dt * inv_mu, &e3);
     // stage 2: q2 = 3/4 q0 + 1/4 (q1 + dt L(q1)):
     //   LA = 1/4 LB + dt/4 V2      (q0 receives 3/4 LB, added at stage 1)
     VjpEpilogue e2;
     e2.o1 = LA, e2.x1 = LB, e2.a1 = 0.25, e2.e1 = 0.25 * dt;
+    e2.next_q = B.q, e2.next_vol = B.vol, e2.ws_ready = true;
     if (s == FJ_OK)
       s = rhs_vjp(ctx, Q1, B.kxyz, B.vol, LB, nullptr, B.ni, B.nj, B.nk, pp, flags, wk, st, dmu_b,
                   0.25 * dt * inv_mu, &e2);
@@ -993,7 +995,7 @@ static int step_vjp_impl(fj_ctx* ctx, const fj_block* blocks, const double* cons
     // (L0 is read by no stage, so each of its cells is written once)
     VjpEpilogue e1;
     e1.o1 = L0, e1.x1 = lam_in[b], e1.a1 = 1.0 / 3.0, e1.y1 = LB, e1.b1 = 0.75, e1.z1 = LA, e1.c1 = 1.0;
-    e1.e1 = dt;
+    e1.e1 = dt, e1.ws_ready = true;
     if (s == FJ_OK)
       s = rhs_vjp(ctx, B.q, B.kxyz, B.vol, LA, nullptr, B.ni, B.nj, B.nk, pp, flags, wk, st, dmu_b, dt * inv_mu,
                   &e1);

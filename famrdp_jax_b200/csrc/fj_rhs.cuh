@@ -45,7 +45,11 @@ size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, i
 //   o1 = a1 x1 + b1 y1 + c1 z1 + e1 V   (y1, z1 may be NULL)
 //   o2 = a2 x2 + b2 y2               (o2 may be NULL; y2 may be NULL)
 // Every input is read at a cell before any output is written there, so an
-// output may alias an input.
+// output may alias an input.  With next_q set, the kernel also leaves in the
+// workspace what the next RHS VJP of the same block (state next_q, adjoint
+// o1, cell volumes next_vol, same flags) reads first: the primitives, lam/vol
+// and the cleared face sums; that call is then made with ws_ready and skips
+// its primitive launch.
 struct VjpEpilogue {
   double* o1 = nullptr;
   const double* x1 = nullptr;
@@ -60,6 +64,9 @@ struct VjpEpilogue {
   double a2 = 0.0;
   const double* y2 = nullptr;
   double b2 = 0.0;
+  const double* next_q = nullptr;
+  const double* next_vol = nullptr;
+  bool ws_ready = false;
 };
 // out = (dL/dq)^T lam for one block (L = the RHS parts selected by flags), or
 // with epi the epilogue's outputs instead (out unused); with dmu set, also
