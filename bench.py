@@ -189,10 +189,14 @@ def workload_desc(case, args):
             "tree24": "uneven blocks U[16,160]^3 on a random spanning tree, farfield/periodic faces, M 0.8, Re 5e4",
             "ensemble64": "64 independent self-periodic 64^3 Taylor-Green instances, M U[0.1,0.9], Re log-U[1e2,1e4], "
                           "0.5% noise, per-instance mu0 and dt, all instances per launch"}
+    # per padded cell a step reads at least q, kxyz and vol and writes q: 160 B
+    mb = 160.0 * case.padded_cells / 1e6
+    l2 = (f"inputs larger than L2 (state + metrics {mb:.0f} MB per step >> 126 MB)" if mb > 2 * 126 else
+          f"inputs of {mb:.0f} MB per step, not flushed from L2 between steps (a launch-bound case)")
     return {"workload": f"{case.name}: {len(case.qs)} blocks, {desc[args.workload]}",
             "blocks": len(case.qs), "cells_interior": case.interior_cells, "cells_padded": case.padded_cells,
             "precision": args.precision, "ghost": case.cfg.ghost, "seed": args.seed,
-            "l2": "inputs larger than L2 (state + metrics per step >> 126 MB)",
+            "l2": l2,
             "cuda_graph": "each timed step is one replay of a captured step graph (halo, BCs, 3 stages)"}
 
 
