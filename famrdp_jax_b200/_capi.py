@@ -199,8 +199,10 @@ def pipeline_setting(device=None):
 
 
 def set_adjoint_variant(variant: int = 0, device=None) -> None:
-    """Launch shape of the adjoint's face kernel (0 = register-capped default,
-    1 = uncapped, 2 = the other cap)."""
+    """Launch shape of the adjoint's face and viscous kernels: 0 = the
+    default (register caps per precision; with FP32 fluxes both in one
+    launch), 1 = face kernel uncapped, 2 = the other face cap, 3 / 4 = 0 / 2
+    with the viscous kernel uncapped."""
     c = ctx(device)
     check(lib().fj_ctx_set_adjoint_variant(c, int(variant)), "fj_ctx_set_adjoint_variant", c)
 

@@ -63,6 +63,29 @@ def test_f32_rhs_vjp_close_to_autograd(cuda_device, limiter, visc_law, shape):
     assert err <= 2e-6
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_rhs_vjp_every_launch_variant(cuda_device, variant, precision):
+    """Every launch shape of the face and viscous VJPs (fj_ctx_set_adjoint_variant;
+    variant 0 runs FP32 as one combined launch, the others as two) against
+    torch.autograd of the FP64 twin: FP64 <= 1e-10, FP32 <= 2e-6 relative L2."""
+    from famrdp_jax_b200 import _capi
+    q, kxyz, vol = random_block((13, 19, 41), 7)
+    cfg = _cfg(limiter="vanleer", precision=precision)
+    lam = np.random.default_rng(8).standard_normal(q.shape)
+    qt = torch.tensor(q, requires_grad=True)
+    L = TORCH.rhs_block(qt, torch.tensor(kxyz), torch.tensor(vol), cfg)
+    (ref,) = torch.autograd.grad(L, qt, grad_outputs=torch.tensor(lam))
+    m = Metrics(jac=dev(vol), kxyz=dev(kxyz), vol=dev(vol))
+    qd = dev(q)
+    _capi.set_adjoint_variant(variant, qd.device)
+    try:
+        got = host(adjoint.rhs_vjp(qd, m, cfg, dev(lam)))
+    finally:
+        _capi.set_adjoint_variant(0, qd.device)
+    assert rel_l2(got, ref.numpy()) <= (1e-10 if precision == "f64" else 2e-6)
+
+
 def _mirror_case():
     """One block with farfield, symmetry and adiabatic-wall faces and one
     self-periodic pair."""
