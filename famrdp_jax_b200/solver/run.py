@@ -8,8 +8,9 @@ here.
 
 After every ``check_every`` steps (when cfg.nan_check) the state is checked
 for non-finite values and non-positive density or pressure; on failure the
-last good state and the failing one are saved under ``dump_dir`` (when given)
-and FloatingPointError names the step.
+state before the failing step (the last good one when check_every is 1) and
+the failing one are saved under ``dump_dir`` (when given) and
+FloatingPointError names the step.
 """
 from __future__ import annotations
 
