@@ -32,9 +32,14 @@ Printed on rank 0 as ONE JSON line:
   cpu_baseline the NumPy FP64 oracle (1 core) on one block for one step;
   fp32_error_table  FP32-flux against FP64 per conserved variable, full and
                interior, at steps 1, 10, 100 (and 200 for tree24);
-  adjoint      adjoint/forward time of the checkpointed trajectory adjoint on
-               the 96^3 Taylor-Green case (50 steps, a checkpoint every 10),
-               FP64 and FP32-flux, with dJ/dmu0 and dJ/dM0.
+  workloads    (default workload only) the same record -- value, step time,
+               stage-group roofline, end to end -- for the uneven 24-block
+               tree, the 64-instance ensemble and the 32^3 Taylor-Green block,
+               in both precisions;
+  adjoint      adjoint/forward and gradient/forward time of the checkpointed
+               trajectory adjoint on the 96^3 Taylor-Green case (50 steps, a
+               checkpoint every 10), FP64 and FP32-flux, with dJ/dmu0, dJ/dM0
+               and the FP64 gradient's central-difference check.
 
 ``--impl reference`` times the reference algorithm on the host cores (the
 PyTorch-CPU FP64 port of the reference, all threads; the reference itself is
@@ -262,13 +267,16 @@ def run_reference(args):
     return 0
 
 
-def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32")):
+def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"), fd=True):
     """Adjoint/forward time on the 96^3 Taylor-Green configuration (M0 0.3,
     Re 800, constant viscosity, 1 % noise, kinetic-energy objective after 50
     steps, a checkpoint every 10 steps), FP64 and FP32-flux, with the FP32-flux
     gradient's relative L2 distance from the FP64 gradient.  Device time by
     CUDA events on the stream the kernels run on; "adjoint_over_forward" is the
-    reverse sweep (segment recompute + step adjoints) over the plain forward."""
+    reverse sweep (segment recompute + step adjoints) over the plain forward,
+    "gradient_over_forward" the whole gradient (checkpointed forward + reverse
+    sweep) over the plain forward.  With fd, the FP64 gradient is also checked
+    against central differences of the forward (eps 1e-6, 16 directions)."""
     import dataclasses as dc
 
     import torch
@@ -326,10 +334,26 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"))
         dJ_dM0 = float(torch.sum(g[0] * torch.as_tensor(dq_dM0, device=device))) + dmu * 1.0 / c.meta["Re"]
         out[prec] = {"forward_ms_per_step": t_fwd / nsteps, "checkpointed_forward_ms_per_step": t_ckpt / nsteps,
                      "reverse_sweep_ms_per_step": t_rev / nsteps, "adjoint_over_forward": t_rev / t_fwd,
+                     "gradient_over_forward": (t_ckpt + t_rev) / t_fwd,
                      "J": J, "dJ_dmu0": dmu, "dJ_dM0": dJ_dM0}
+        del plan, run, final, checkpoints, lams, g, qa, qb
+        torch.cuda.empty_cache()
+    out["ratios_note"] = ("adjoint_over_forward = reverse sweep (segment recompute + step adjoints) / plain "
+                          "forward; gradient_over_forward = (checkpointed forward + reverse sweep) / plain forward")
     if len(grads) == 2:
         out["f32_vs_f64_grad_rel_l2"] = float(torch.linalg.vector_norm(grads["f32"] - grads["f64"]) /
                                               torch.linalg.vector_norm(grads["f64"]))
+    if fd:
+        from famrdp_jax_b200.solver.gradcheck import fd_check_kinetic_energy
+        st = cases.to_state(c, device)
+        dt = diagnostics.cfl_dt(st, c.cfg, c.cfl)
+        r = fd_check_kinetic_energy(st, dc.replace(c.cfg, precision="f64"), dt, nsteps, checkpoint_every=every,
+                                    eps=1e-6, ndirs=16, seed=0)
+        out["fd_check_f64"] = {k: v for k, v in r.items() if k != "per_direction"} | {
+            "rel_direction": [row["rel_direction"] for row in r["per_direction"]],
+            "rel_gradnorm": [row["rel_gradnorm"] for row in r["per_direction"]],
+            "note": "central differences of the GPU forward, eps 1e-6, 16 seeded unit-L2 directions; "
+                    "rel_direction = |fd-ad|/|ad|, rel_gradnorm = |fd-ad|/|grad J|"}
     return out
 
 
@@ -391,103 +415,11 @@ def _max_over_ranks(x: float, ws: int, device) -> float:
     return float(t.item())
 
 
-def run_ours(args):
+def _stage_roofline(plan, q0s, dt, prec, padded_cells):
+    """The dominant kernel group, one stage-2 evaluation of all blocks, timed
+    live (10 launches of the group after 3 warm-ups, CUDA events on the
+    launching stream)."""
     import torch
-    import torch.distributed as dist
-
-    from famrdp_jax_b200 import _capi, cases
-    from famrdp_jax_b200.core.types import Block, State
-    from famrdp_jax_b200.mesh.metric import compute_metrics
-    from famrdp_jax_b200.solver import diagnostics
-    from famrdp_jax_b200.solver.step import StepPlan, step
-
-    ws, rank, local = _dist()
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
-    if ws > 1:
-        import datetime
-        dist.init_process_group("nccl", device_id=device, timeout=datetime.timedelta(seconds=300))
-
-    def metrics_fn(xyz):
-        m = compute_metrics(torch.as_tensor(xyz, dtype=torch.float64, device=device), ghost=2)
-        return m.jac.cpu().numpy(), m.kxyz.cpu().numpy(), m.vol.cpu().numpy()
-
-    case = build_case(args, metrics_fn)
-    warm = max(args.warmup, 3)
-    cells = case.interior_cells
-    st0 = cases.to_state(case, device)
-    dt = diagnostics.cfl_dt(st0, case.cfg, case.cfl)
-    if args.stage_only:
-        # four standalone stage-2 evaluations of all blocks (the launch group
-        # the roofline line times), for a profiler to capture: nothing else
-        cfg = dataclasses.replace(case.cfg, precision=args.precision)
-        plan = StepPlan(st0, cfg)
-        if args.precision == "f32":
-            plan.set_variant(args.shape)
-        q0s = [b.q for b in st0.blocks]
-        qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state
-        outs = [torch.empty_like(q) for q in q0s]
-        for _ in range(4):
-            plan.stage(qin, q0s, outs, dt, 2)
-        torch.cuda.synchronize()
-        if rank == 0:
-            print(json.dumps({"stage_only": True, "precision": args.precision, "shape": args.shape,
-                              "padded_cells": case.padded_cells}), flush=True)
-        return 0
-    ens = None
-    if "mu0" in case.meta and isinstance(case.meta["mu0"], list):  # independent instances
-        ens = (case.meta["mu0"], [diagnostics.cfl_dt(State(blocks=(b,), metrics=(m,)), case.cfg, case.cfl)
-                                  for b, m in zip(st0.blocks, st0.metrics)])
-
-    def barrier():
-        if ws > 1:
-            dist.barrier()
-
-    order = [args.precision] + [p for p in ("f32", "f64") if p != args.precision]
-    results, finals, plans = {}, {}, {}
-    clk_summary = None
-    for prec in order:
-        cfg = dataclasses.replace(case.cfg, precision=prec)
-        state = cases.to_state(case, device)
-        plan = StepPlan(state, cfg)
-        if ens:
-            plan.set_ensemble(*ens)
-        plans[prec] = (plan, cfg, state)
-        qa = [b.q for b in state.blocks]
-        qb = [torch.empty_like(q) for q in qa]
-        tuned = plan.autotune(qa, qb, dt, reps=3)  # launch shape of the FP32 kernels (qb is scratch here)
-        for _ in range(warm):  # also captures the two ping-pong step graphs
-            plan.run(qa, qb, dt, graph=True)
-            qa, qb = qb, qa
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
-        s = torch.cuda.current_stream()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        n0 = _capi.launch_count(device)
-        with ClockSampler(_gpu_index(local)) as clk:
-            e0.record(s)
-            for _ in range(args.steps):
-                plan.run(qa, qb, dt, graph=True)
-                qa, qb = qb, qa
-            e1.record(s)
-            torch.cuda.synchronize()
-        launches = _capi.launch_count(device) - n0
-        barrier()
-        ms = _max_over_ranks(e0.elapsed_time(e1), ws, device)
-        results[prec] = {"ms_per_step": ms / args.steps, "value": _throughput(cells, args.steps, ms, ws),
-                         "launches": launches, "autotune": {"chosen": tuned[0], "ms_per_step": tuned[1]},
-                         "step_hbm_gbs": STEP_BYTES[prec] * case.padded_cells * ws / (ms / args.steps / 1e3) / 1e9}
-        if prec == args.precision:
-            clk_summary = clk.summary()
-        finals[prec] = qa
-    num = sum(float(torch.sum((finals["f32"][b] - finals["f64"][b]) ** 2)) for b in range(len(case.qs)))
-    den = sum(float(torch.sum(finals["f64"][b] ** 2)) for b in range(len(case.qs)))
-    err_f32 = (num / den) ** 0.5
-
-    # ---- dominant kernel group: one RK stage of all blocks ------------------
-    plan, cfg, state = plans[args.precision]
-    q0s = finals[args.precision]
     qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state q0
     outs = [torch.empty_like(q) for q in q0s]
     for _ in range(3):
@@ -502,25 +434,36 @@ def run_ours(args):
     a1.record(s)
     torch.cuda.synchronize()
     stage_ms = a0.elapsed_time(a1) / reps
-    alg = STAGE_BYTES[args.precision] * case.padded_cells
+    alg = STAGE_BYTES[prec] * padded_cells
     peak, peak_kind = _peaks()
     achieved = alg / (stage_ms / 1e3) / 1e9
-    traffic = STAGE_TRAFFIC.get(args.precision)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic * case.padded_cells if traffic else None,
-                "kernel": "one TVD-RK3 stage of all blocks (split pipeline: prims, fluxes, assembly; 3 launches)",
-                "alg_bytes_per_launch": alg, "launch_ms": stage_ms, "peak_kind": peak_kind}
+    traffic = STAGE_TRAFFIC.get(prec)
+    del qin, outs
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic * padded_cells if traffic else None,
+            "traffic_note": f"{traffic:.0f} B per padded cell (ncu dram__bytes_read+write of the stage-2 group on "
+                            f"4 x 100^3 padded cells) x the cells of one launch" if traffic else None,
+            "kernel": "one TVD-RK3 stage of all blocks (split pipeline: prims, fluxes, assembly; 3 launches)",
+            "alg_bytes_per_cell": STAGE_BYTES[prec], "alg_bytes_per_launch": alg, "launch_ms": stage_ms,
+            "peak_kind": peak_kind}
 
-    # ---- end to end with host buffers ----------------------------------------
-    # every step copies its input state from pinned host memory and its result
-    # back.  Two public paths: step() per call (copy in, step, copy out, one
-    # stream) and HostStepper, which overlaps step n's copy-in, step n-1 and the
-    # copy-out of step n-2 on three streams; the line reports the faster.
+
+def _end_to_end(plan, cfg, state, q0s, dt, cells, steps, ws, device, barrier):
+    """The metric through the public API with host buffers: every step copies
+    its input state from pinned host memory and its result back.  Two public
+    paths: step() per call (copy in, step, copy out, one stream) and
+    HostStepper, which overlaps step n's copy-in, step n-1 and the copy-out of
+    step n-2 on three streams; the faster is reported."""
+    import torch
+
+    from famrdp_jax_b200.core.types import Block, State
+    from famrdp_jax_b200.solver.step import step
     from famrdp_jax_b200.solver.stream import HostStepper
+    s = torch.cuda.current_stream()
     host_in = [q.detach().cpu().pin_memory() for q in q0s]
     host_out = [torch.empty_like(h).pin_memory() for h in host_in]
     dev_in = [torch.empty_like(q) for q in q0s]
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = max(3, min(steps, 10))
 
     def e2e_step():
         for d, h in zip(dev_in, host_in):
@@ -547,16 +490,160 @@ def run_ours(args):
     piped_ms = timed_e2e(lambda: stepper.run([host_in] * e2e_steps, [host_out] * e2e_steps, dt))
     bytes_io = sum(h.numel() * 8 for h in host_in)
     e2e_ms = min(serial_ms, piped_ms)
-    e2e = {"value": _throughput(cells, e2e_steps, e2e_ms, ws), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
-           "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps,
-           "path": "HostStepper (pipelined)" if piped_ms <= serial_ms else "step() per call",
-           "serial_step_value": _throughput(cells, e2e_steps, serial_ms, ws),
-           "pipelined_value": _throughput(cells, e2e_steps, piped_ms, ws)}
+    del stepper, host_in, host_out, dev_in
+    return {"value": _throughput(cells, e2e_steps, e2e_ms, ws), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+            "d2h_bytes_per_step": bytes_io, "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps,
+            "path": "HostStepper (pipelined)" if piped_ms <= serial_ms else "step() per call",
+            "serial_step_value": _throughput(cells, e2e_steps, serial_ms, ws),
+            "pipelined_value": _throughput(cells, e2e_steps, piped_ms, ws)}
+
+
+def measure_case(case, prec, steps, warm, device, ws, local, barrier, ens=None, sample_clocks=False):
+    """Graph-replayed steps of one workload in one precision: throughput,
+    launches, the autotuner's choice, the stage-group roofline and the
+    end-to-end figure.  Returns (record, final state, clock summary)."""
+    import torch
+
+    from famrdp_jax_b200 import _capi, cases
+    from famrdp_jax_b200.solver import diagnostics
+    from famrdp_jax_b200.solver.step import StepPlan
+    cells = case.interior_cells
+    cfg = dataclasses.replace(case.cfg, precision=prec)
+    state = cases.to_state(case, device)
+    dt = diagnostics.cfl_dt(state, cfg, case.cfl)
+    plan = StepPlan(state, cfg)
+    if ens:
+        plan.set_ensemble(*ens)
+    qa = [b.q for b in state.blocks]
+    qb = [torch.empty_like(q) for q in qa]
+    tuned = plan.autotune(qa, qb, dt, reps=3)  # launch shape of the FP32 kernels (qb is scratch here)
+    for _ in range(warm):  # also captures the two ping-pong step graphs
+        plan.run(qa, qb, dt, graph=True)
+        qa, qb = qb, qa
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = _capi.launch_count(device)
+    clk = ClockSampler(_gpu_index(local)) if sample_clocks else None
+    if clk:
+        clk.__enter__()
+    e0.record(s)
+    for _ in range(steps):
+        plan.run(qa, qb, dt, graph=True)
+        qa, qb = qb, qa
+    e1.record(s)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    launches = _capi.launch_count(device) - n0
+    barrier()
+    ms = _max_over_ranks(e0.elapsed_time(e1), ws, device)
+    rec = {"ms_per_step": ms / steps, "value": _throughput(cells, steps, ms, ws), "launches": launches,
+           "launches_per_step": launches / steps,
+           "autotune": {"chosen": tuned[0], "ms_per_step": tuned[1]},
+           "step_hbm_gbs": STEP_BYTES[prec] * case.padded_cells * ws / (ms / steps / 1e3) / 1e9}
+    rec["roofline"] = _stage_roofline(plan, qa, dt, prec, case.padded_cells)
+    rec["e2e"] = _end_to_end(plan, cfg, state, qa, dt, cells, steps, ws, device, barrier)
+    final = [q.clone() for q in qa]
+    del plan, qa, qb, state
+    torch.cuda.empty_cache()
+    return rec, final, (clk.summary() if clk else None)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from famrdp_jax_b200 import cases
+    from famrdp_jax_b200.core.types import State
+    from famrdp_jax_b200.mesh.metric import compute_metrics
+    from famrdp_jax_b200.solver import diagnostics
+    from famrdp_jax_b200.solver.step import StepPlan
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", device_id=device, timeout=datetime.timedelta(seconds=300))
+
+    def metrics_fn(xyz):
+        m = compute_metrics(torch.as_tensor(xyz, dtype=torch.float64, device=device), ghost=2)
+        return m.jac.cpu().numpy(), m.kxyz.cpu().numpy(), m.vol.cpu().numpy()
+
+    case = build_case(args, metrics_fn)
+    warm = max(args.warmup, 3)
+    st0 = cases.to_state(case, device)
+    dt = diagnostics.cfl_dt(st0, case.cfg, case.cfl)
+    if args.stage_only:
+        # four standalone stage-2 evaluations of all blocks (the launch group
+        # the roofline line times), for a profiler to capture: nothing else
+        cfg = dataclasses.replace(case.cfg, precision=args.precision)
+        plan = StepPlan(st0, cfg)
+        if args.precision == "f32":
+            plan.set_variant(args.shape)
+        q0s = [b.q for b in st0.blocks]
+        qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state
+        outs = [torch.empty_like(q) for q in q0s]
+        for _ in range(4):
+            plan.stage(qin, q0s, outs, dt, 2)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"stage_only": True, "precision": args.precision, "shape": args.shape,
+                              "padded_cells": case.padded_cells}), flush=True)
+        return 0
+
+    def ensemble_of(c, st):
+        if "mu0" in c.meta and isinstance(c.meta["mu0"], list):  # independent instances
+            return (c.meta["mu0"], [diagnostics.cfl_dt(State(blocks=(b,), metrics=(m,)), c.cfg, c.cfl)
+                                    for b, m in zip(st.blocks, st.metrics)])
+        return None
+
+    ens = ensemble_of(case, st0)
+    del st0
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    order = [args.precision] + [p for p in ("f32", "f64") if p != args.precision]
+    results, finals = {}, {}
+    clk_summary = None
+    for prec in order:
+        rec, finals[prec], clk = measure_case(case, prec, args.steps, warm, device, ws, local, barrier, ens,
+                                              sample_clocks=(prec == args.precision))
+        results[prec] = rec
+        if clk is not None:
+            clk_summary = clk
+    num = sum(float(torch.sum((finals["f32"][b] - finals["f64"][b]) ** 2)) for b in range(len(case.qs)))
+    den = sum(float(torch.sum(finals["f64"][b] ** 2)) for b in range(len(case.qs)))
+    err_f32 = (num / den) ** 0.5
+    del finals
+
+    # ---- the other configurations, each in both precisions -----------------
+    others = {}
+    if args.workload == "wavy4" and not args.no_workloads:
+        for wl in ("tree24", "ensemble64", "tgv32"):
+            sub = argparse.Namespace(**{**vars(args), "workload": wl})
+            c2 = build_case(sub)
+            st2 = cases.to_state(c2, device)
+            ens2 = ensemble_of(c2, st2)
+            del st2
+            entry = {"config": workload_desc(c2, sub)}
+            for prec in ("f32", "f64"):
+                rec, _, _ = measure_case(c2, prec, args.steps, warm, device, ws, local, barrier, ens2)
+                entry[prec] = rec
+            entry["f32_over_f64"] = entry["f64"]["ms_per_step"] / entry["f32"]["ms_per_step"]
+            others[wl] = entry
+            del c2
+            torch.cuda.empty_cache()
 
     cpu = cpu_oracle_sample(case, dt) if (rank == 0 and not args.no_cpu) else None
     marks = (1, 10, 100, 200) if args.workload == "tree24" else (1, 10, 100)
     errs = error_table(case, dt, device, marks, ens) if (rank == 0 and not args.no_error_table) else None
-    adj = (adjoint_timing(device, args.adjoint_n, args.adjoint_steps, args.adjoint_every)
+    adj = (adjoint_timing(device, args.adjoint_n, args.adjoint_steps, args.adjoint_every, fd=not args.no_fd)
            if (rank == 0 and not args.no_adjoint) else None)
     if rank == 0:
         r = results[args.precision]
@@ -564,11 +651,13 @@ def run_ours(args):
                 "warmup": warm, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.precision == "f64" else "f32-flux/f64-state",
                 "data": "synthetic", "config": workload_desc(case, args) | {"parallelism": f"replicas x{ws}"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["launches"],
+                "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": clk_summary,
                 "variants": {p: results[p] for p in order} | {
+                    "f32_over_f64": results["f64"]["ms_per_step"] / results["f32"]["ms_per_step"],
                     "f32_vs_f64_rel_l2": err_f32,
                     "f32_vs_f64_note": f"whole state after {warm + args.steps} steps from the same start"},
+                "workloads": others or None,
                 "adjoint": adj, "fp32_error_table": errs,
                 "dt": dt if not ens else {"per_instance": True, "min": min(ens[1]), "max": max(ens[1])}}
         print(json.dumps(line), flush=True)
@@ -594,6 +683,9 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
     ap.add_argument("--no-error-table", action="store_true", help="skip the FP32-vs-FP64 error table")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the sub-records of the other configurations (tree24, ensemble64, tgv32)")
+    ap.add_argument("--no-fd", action="store_true", help="skip the adjoint's central-difference check")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="print only the adjoint/forward timing (one JSON line)")
     ap.add_argument("--adjoint-n", type=int, default=96)
@@ -609,7 +701,7 @@ def main(argv=None):
         _capi.set_adjoint_variant(args.adjoint_variant, torch.device("cuda:0"))
         precs = ("f64", "f32") if args.adjoint_precision == "both" else (args.adjoint_precision,)
         print(json.dumps(adjoint_timing(torch.device("cuda:0"), args.adjoint_n, args.adjoint_steps,
-                                        args.adjoint_every, precs)), flush=True)
+                                        args.adjoint_every, precs, fd=not args.no_fd)), flush=True)
         return 0
     if args.impl == "reference":
         return run_reference(args)

@@ -523,6 +523,17 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
   // pipeline, field-major FP32 for the fused kernel (the FP64 kernels read
   // the caller's kxyz)
   const bool split = pl->pipeline == FJ_PIPELINE_SPLIT;
+  // the plan's own stream: set-up kernels and later graph captures run on it,
+  // never on the legacy stream.  The caller's pending writes of the states
+  // and metrics (on any stream) complete first: creation synchronises the
+  // device once.
+  e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pl->capture_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    pl->capture_stream = nullptr;
+    fj_plan_destroy(pl);
+    return cuda_status(ctx, e, "plan stream creation");
+  }
   if (p->precision == FJ_PREC_F32FLUX &&
       (pl->pipeline == FJ_PIPELINE_SPLIT || pl->pipeline == FJ_PIPELINE_FUSED)) {
     pl->kmet.assign(nblocks, nullptr);
@@ -536,22 +547,26 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
         return set_err(ctx, FJ_ERR_NO_MEMORY, "plan metric copy allocation failed");
       }
       s = split ? split_metric_records(blocks[b].kxyz, pl->kmet[b], blocks[b].ni, blocks[b].nj, blocks[b].nk,
-                                       p->precision, nullptr)
-                : convert_f64_f32(blocks[b].kxyz, (float*)pl->kmet[b], 9 * N, nullptr);
+                                       p->precision, pl->capture_stream)
+                : convert_f64_f32(blocks[b].kxyz, (float*)pl->kmet[b], 9 * N, pl->capture_stream);
       if (s != FJ_OK) {
         fj_plan_destroy(pl);
         return set_err(ctx, s, "plan metric conversion failed");
       }
     }
-    e = cudaStreamSynchronize(nullptr);
+    e = cudaStreamSynchronize(pl->capture_stream);
     if (e != cudaSuccess) {
       fj_plan_destroy(pl);
       return cuda_status(ctx, e, "plan metric conversion");
     }
     // the FP32-flux split path offsets the momentum fluxes' pressure by the
-    // mean pressure of the state the plan is created with
+    // mean pressure of the state the plan is created with (partial sums in
+    // the plan's scratch, which no step has used yet)
     if (split) {
-      s = mean_pressure(blocks, nblocks, p->gamma - 1.0, &pl->p_ref);
+      if (mean_pressure_scratch_bytes(nblocks) <= total)
+        s = mean_pressure(blocks, nblocks, p->gamma - 1.0, (double*)pl->scratch, pl->capture_stream, &pl->p_ref);
+      else
+        s = FJ_ERR_NO_MEMORY;
       if (s != FJ_OK || !std::isfinite(pl->p_ref)) pl->p_ref = 0.0;
     }
   }

@@ -15,7 +15,13 @@
 // context scratch.  Host code must not pass the array's name to a kernel: on
 // the host that name denotes a host-side placeholder, not device memory.  The
 // device address is looked up once per device with cudaGetSymbolAddress (with
-// that device current) and cached.
+// that device current) and cached for the life of the process: a
+// cudaDeviceReset while the library is in use (which would recreate the
+// context and could move the array) is not supported.
+//
+// Error attribution: a call finds the runtime's last-error state clear or
+// returns FJ_ERR_CUDA at once, leaving that earlier error for its owner to
+// read; a failure reported after the launches is then this call's own.
 #include <mutex>
 
 #include "fj_common.cuh"
@@ -23,9 +29,11 @@
 
 namespace {
 
-// Capacity of the shared scratch: FJ_NOALLOC_SCRATCH_BYTES (64 MiB).  Every
-// device on which the entry point runs holds this array until the process
-// exits.
+// Capacity of the shared scratch: FJ_NOALLOC_SCRATCH_BYTES (64 MiB).  The
+// array is reserved on a device when this file's module is loaded there: at
+// its first use under lazy module loading (the CUDA default), or at context
+// creation on every device under CUDA_MODULE_LOADING=EAGER, whether or not
+// the entry point runs there.  It is held until the process exits.
 static __device__ __align__(256) unsigned char g_rhs_scratch[FJ_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
@@ -47,6 +55,8 @@ extern "C" int fj_rhs_noalloc_f64(const double* q, const double* kxyz, const dou
   const size_t need = p->precision == FJ_PREC_F32FLUX ? staged_ws_bytes<float>(ni, nj, nk)
                                                       : staged_ws_bytes<double>(ni, nj, nk);
   if (need > (size_t)FJ_NOALLOC_SCRATCH_BYTES) return FJ_ERR_SCRATCH_LIMIT;
+  // an error left by an earlier, unrelated call stays for its owner to read
+  if (cudaPeekAtLastError() != cudaSuccess) return FJ_ERR_CUDA;
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {

@@ -10,7 +10,7 @@
 //                                                                  viscous.py:86-117
 //
 // It is the straightforward decomposition, kept as the cross-check of the
-// fused sweep kernels (fj_rhs_fused.cu) and as the general fallback for
+// fused stage kernel (fj_stage_fused.cu) and as the general fallback for
 // blocks the fused kernels do not tile.
 #include "fj_common.cuh"
 #include "fj_physics.cuh"

@@ -43,8 +43,10 @@ struct SplitBlock {
 // field-major FP64 kxyz (3, 3, ni, nj, nk): the nine kxyz[l][m] and, in FP32
 // records, the three face-normal difference sums the pressure offset uses.
 int split_metric_records(const double* kxyz, void* out, int ni, int nj, int nk, int precision, cudaStream_t st);
-// Mean pressure over all padded cells of the blocks (synchronous).
-int mean_pressure(const fj_block* blocks, int nblocks, double gm1, double* out);
+// Mean pressure over all padded cells of the blocks, on stream st with
+// mean_pressure_scratch_bytes(nblocks) bytes of device scratch; waits for st.
+size_t mean_pressure_scratch_bytes(int nblocks);
+int mean_pressure(const fj_block* blocks, int nblocks, double gm1, double* scratch, cudaStream_t st, double* out);
 // Bytes of one block's metric records.
 size_t split_metric_record_bytes(int precision, int64_t N);
 // Scratch bytes of the intermediates of `cells` padded cells in total.

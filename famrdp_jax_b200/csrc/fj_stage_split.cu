@@ -1078,23 +1078,21 @@ int split_metric_records(const double* kxyz, void* out, int ni, int nj, int nk, 
   return cudaGetLastError() == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
 }
 
-int mean_pressure(const fj_block* blocks, int nblocks, double gm1, double* out) {
-  double* part = nullptr;
+size_t mean_pressure_scratch_bytes(int nblocks) { return ((size_t)kPsumCtas * nblocks + 1) * sizeof(double); }
+
+int mean_pressure(const fj_block* blocks, int nblocks, double gm1, double* scratch, cudaStream_t st, double* out) {
+  double* part = scratch;
   const size_t n = (size_t)kPsumCtas * nblocks;
-  if (cudaMalloc(&part, (n + 1) * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return FJ_ERR_NO_MEMORY;
-  }
   int64_t cells = 0;
   for (int b = 0; b < nblocks; ++b) {
     const int64_t N = (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
     cells += N;
-    k_pressure_partial<<<kPsumCtas, kPsumThreads, 0, nullptr>>>(blocks[b].q, N, gm1, part + (size_t)b * kPsumCtas);
+    k_pressure_partial<<<kPsumCtas, kPsumThreads, 0, st>>>(blocks[b].q, N, gm1, part + (size_t)b * kPsumCtas);
   }
-  k_fold_sum<<<1, 1024, 0, nullptr>>>(part, (int)n, part + n);
+  k_fold_sum<<<1, 1024, 0, st>>>(part, (int)n, part + n);
   double h = 0.0;
-  const cudaError_t e = cudaMemcpy(&h, part + n, sizeof(double), cudaMemcpyDeviceToHost);
-  cudaFree(part);
+  cudaError_t e = cudaMemcpyAsync(&h, part + n, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return FJ_ERR_CUDA;
   *out = cells > 0 ? h / (double)cells : 0.0;
   return FJ_OK;

@@ -184,8 +184,11 @@ int fj_rhs_f64(fj_ctx* ctx, const double* q, const double* kxyz, const double* v
 /* The same result as fj_rhs_f64 for callers that cannot allocate device
  * memory.  No counterpart in the reference.  It takes no context and never
  * calls cudaMalloc/cudaFree: its intermediates live in one fixed device array
- * of FJ_NOALLOC_SCRATCH_BYTES inside the library, which each device that runs
- * it keeps until the process exits.  Meant for callers whose device memory is
+ * of FJ_NOALLOC_SCRATCH_BYTES inside the library.  The array is reserved on a
+ * device when its module loads there -- at first use under lazy module
+ * loading (the CUDA default), at context creation on every device that uses
+ * the library under CUDA_MODULE_LOADING=EAGER -- and kept until the process
+ * exits.  Meant for callers whose device memory is
  * owned by a framework (e.g. an XLA custom call under JAX, whose allocator has
  * reserved most of the GPU) or by a fixed start-up budget.
  *   - Limit: the intermediates need about 232 bytes per padded cell in FP64
@@ -197,7 +200,11 @@ int fj_rhs_f64(fj_ctx* ctx, const double* q, const double* kxyz, const double* v
  *   - All calls share the one array: calls that can run at the same time on
  *     one device (different streams, or different host threads) race on it
  *     and must be ordered by the caller.  The array keeps the last call's
- *     contents; no call depends on them. */
+ *     contents; no call depends on them.
+ *   - A call that finds a CUDA error pending on the calling thread returns
+ *     FJ_ERR_CUDA without launching and leaves that error in place.
+ *   - The array's device address is cached per device for the process's
+ *     life: cudaDeviceReset while the library is in use is not supported. */
 int fj_rhs_noalloc_f64(const double* q, const double* kxyz, const double* vol, double* rhs,
                        int ni, int nj, int nk, const fj_params* p, void* stream);
 

@@ -600,13 +600,18 @@ class Ref:
         return q
 
     # -- solver/step.py:18-56 ----------------------------------------------
-    def step(self, qs, metrics, cfg, dt):
+    def step(self, qs, metrics, cfg, dt, rhs_map=None):
         """solver/step.py:18-56: halo + BC once per STEP, then three RK stages
-        over all padded cells.  ``metrics`` is a sequence of (kxyz, vol)."""
+        over all padded cells.  ``metrics`` is a sequence of (kxyz, vol).
+        ``rhs_map(qs) -> [rhs_block of each q]`` may evaluate the blocks'
+        right-hand sides elsewhere (e.g. a process pool); the default
+        evaluates them here, one after another."""
         qs = self.halo_exchange(list(qs), cfg.topology, cfg.ghost)
         qs = [self.apply_bc(q, t, cfg) for q, t in zip(qs, cfg.topology)]
 
         def L(qt):
+            if rhs_map is not None:
+                return rhs_map(qt)
             return [self.rhs_block(q, m[0], m[1], cfg) for q, m in zip(qt, metrics)]
 
         L0 = L(qs)

@@ -8,7 +8,10 @@ float64 data in Fortran order).  Both blocks are 51 x 51 x 11 nodes.  The
 reference's own check (tests/validation/test_m11_metric_match.py:23-36)
 compares compute_metrics(xyz).jac against this Jacobian with atol 1e-13.
 
-    python tests/golden/make_test3_metric.py [REFERENCE_ROOT]
+    python tests/golden/make_test3_metric.py REFERENCE_ROOT
+
+REFERENCE_ROOT is the root of a famrdp_jax checkout (or set
+FAMRDP_JAX_REFERENCE).
 """
 from __future__ import annotations
 
@@ -32,7 +35,11 @@ def _read_xyz(path: Path) -> np.ndarray:
     return np.stack(comps, axis=0)
 
 
-def main(ref_root: str = "/root/reference") -> Path:
+def main(ref_root: str | None = None) -> Path:
+    import os
+    ref_root = ref_root or os.environ.get("FAMRDP_JAX_REFERENCE")
+    if not ref_root:
+        raise SystemExit("usage: make_test3_metric.py REFERENCE_ROOT (or set FAMRDP_JAX_REFERENCE)")
     base = Path(ref_root) / "validation" / "references" / "test3"
     out = {}
     for b in (1, 2):

@@ -43,3 +43,49 @@ def random_block(shape, seed, M=0.3, noise=0.05, metric_noise=0.1, gamma=1.4):
     kxyz = np.eye(3)[:, :, None, None, None] * 4.0 + metric_noise * 4.0 * rng.standard_normal((3, 3) + shape)
     vol = (1.0 / 64.0) * (1.0 + 0.1 * rng.random(shape))
     return q, kxyz, vol
+
+
+# ---- the oracle's block right-hand sides on a pool of host processes ----------
+_POOL_STATE = {}
+
+
+def _pool_init(metrics, cfg):
+    _POOL_STATE["metrics"] = metrics
+    _POOL_STATE["cfg"] = cfg
+
+
+def _pool_rhs(args):
+    from oracle.ref import NP
+    b, q = args
+    kxyz, vol = _POOL_STATE["metrics"][b]
+    return NP.rhs_block(q, kxyz, vol, _POOL_STATE["cfg"])
+
+
+class OraclePool:
+    """Evaluates the NumPy oracle's per-block RHS (the blocks are independent
+    within a stage) on spawned worker processes, one block per task, so that
+    multi-block trajectories of a few hundred steps finish in seconds.  Use as
+    ``NP.step(qs, metrics, cfg, dt, rhs_map=pool.rhs_map)``.  Workers are
+    started with ``spawn`` (never forked from a process that holds a CUDA
+    context)."""
+
+    def __init__(self, metrics, cfg, workers=None):
+        import concurrent.futures
+        import multiprocessing
+        import os
+        n = workers or max(1, min(len(metrics), len(os.sched_getaffinity(0))))
+        self.ex = concurrent.futures.ProcessPoolExecutor(
+            max_workers=n, mp_context=multiprocessing.get_context("spawn"), initializer=_pool_init,
+            initargs=(list(metrics), cfg))
+
+    def rhs_map(self, qs):
+        return list(self.ex.map(_pool_rhs, list(enumerate(qs))))
+
+    def close(self):
+        self.ex.shutdown(wait=True, cancel_futures=True)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

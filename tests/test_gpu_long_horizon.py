@@ -1,0 +1,106 @@
+"""Parity over the full step counts of the multi-block configurations.
+
+The 4-block curvilinear configuration runs 100 steps and the uneven 24-block
+tree 200 steps.  Block sizes are reduced so that the oracle finishes on the
+host cores within a minute or two; the geometry, topology, flow parameters,
+noise and step counts are the configurations' own.  The oracle is the NumPy
+FP64 restatement, its per-block right-hand sides evaluated on a pool of
+spawned host processes (the blocks are independent within a stage).
+
+Per step n, with q_n the oracle's state after n steps:
+  * one-step error (FP64): the GPU step applied to q_n against q_{n+1}, per
+    conserved variable, relative L2 over the full padded blocks and over the
+    interiors: <= 1e-12 (the drop-in bar);
+  * trajectory error: the GPU state after n free-running steps against q_n.
+    FP64: <= 1e-11 per variable at every step (the per-step rounding
+    differences of <= 1e-12 accumulate at most linearly over these horizons);
+    FP32-flux / FP64-state: <= 1e-5 per variable after the last step (the
+    precision variant's stated bound), with the table at steps 1, 10, 100
+    (and 200) printed.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from famrdp_jax_b200 import cases
+from famrdp_jax_b200.solver.step import step
+from oracle.ref import NP
+from parity_util import OraclePool, host, state_from_case
+
+pytestmark = pytest.mark.gpu
+
+FP64_ONE_STEP = 1e-12
+FP64_TRAJECTORY = 1e-11
+FP32_FINAL = 1e-5
+NAMES = ("rho", "rhou", "rhov", "rhow", "rhoE")
+
+
+def _per_variable(got, ref, g=2):
+    """Relative L2 per conserved variable, full padded blocks and interiors
+    (all blocks together); got and ref are lists of (5, ni, nj, nk) arrays."""
+    out = {}
+    for part in ("full", "interior"):
+        for v in range(5):
+            num = den = 0.0
+            for a, b in zip(got, ref):
+                x, y = a[v], b[v]
+                if part == "interior":
+                    x, y = x[g:-g, g:-g, g:-g], y[g:-g, g:-g, g:-g]
+                num += float(np.sum((x - y) ** 2))
+                den += float(np.sum(y ** 2))
+            out[f"{part}_{NAMES[v]}"] = (num / den) ** 0.5 if den > 0 else num ** 0.5
+    return out
+
+
+def _with_blocks(st, qs):
+    from famrdp_jax_b200.core.types import Block, State
+    blocks = tuple(Block(q=torch.as_tensor(q, device="cuda"), xyz=b.xyz) for q, b in zip(qs, st.blocks))
+    return State(blocks=blocks, metrics=st.metrics, t=st.t, step=st.step)
+
+
+def _long_run(case, nsteps, marks):
+    mets_np = [(m[1], m[2]) for m in case.metrics]
+    dt = NP.cfl_dt(case.qs, mets_np, case.cfg.gas.gamma, case.cfl, case.cfg.ghost)
+    cfg64 = dataclasses.replace(case.cfg, precision="f64")
+    cfg32 = dataclasses.replace(case.cfg, precision="f32")
+    st0 = state_from_case(case)
+    free64, free32 = st0, state_from_case(case)
+    ref_np = [q.copy() for q in case.qs]
+    worst_one, worst_traj64 = 0.0, 0.0
+    table32 = {}
+    with OraclePool(mets_np, cfg64) as pool:
+        for n in range(1, nsteps + 1):
+            one = step(_with_blocks(st0, ref_np), cfg64, dt)
+            ref_np = NP.step(ref_np, mets_np, cfg64, dt, rhs_map=pool.rhs_map)
+            e1 = _per_variable([host(b.q) for b in one.blocks], ref_np)
+            worst_one = max(worst_one, max(e1.values()))
+            assert max(e1.values()) <= FP64_ONE_STEP, (n, e1)
+            free64 = step(free64, cfg64, dt)
+            free32 = step(free32, cfg32, dt)
+            e64 = _per_variable([host(b.q) for b in free64.blocks], ref_np)
+            worst_traj64 = max(worst_traj64, max(e64.values()))
+            assert max(e64.values()) <= FP64_TRAJECTORY, (n, e64)
+            if n in marks or n == nsteps:
+                table32[n] = _per_variable([host(b.q) for b in free32.blocks], ref_np)
+    print(f"{case.name}: {nsteps} steps, worst FP64 one-step {worst_one:.2e}, "
+          f"worst FP64 trajectory {worst_traj64:.2e}")
+    for n, row in table32.items():
+        print(f"  FP32-flux after {n:3d} steps: " + ", ".join(f"{k} {v:.2e}" for k, v in row.items()))
+    assert max(table32[nsteps].values()) <= FP32_FINAL, table32[nsteps]
+    return table32
+
+
+def test_wavy4_hundred_steps(cuda_device):
+    """4 curvilinear blocks (2 x 2 in i-j, periodic), 24^3 cells each, Mach
+    0.5, Re 1e4, 1 % noise, 100 steps."""
+    c = cases.wavy4(n=24, metrics_fn=lambda x: NP.compute_metrics(x, ghost=2))
+    _long_run(c, 100, (1, 10, 100))
+
+
+def test_tree24_two_hundred_steps(cuda_device):
+    """24 uneven blocks (per-axis sizes U[8, 16]) on a seeded spanning tree
+    with farfield and periodic faces, Mach 0.8, Re 5e4, 1 % noise, 200 steps."""
+    c = cases.tree24(nblocks=24, lo=8, hi=16, seed=0)
+    _long_run(c, 200, (1, 10, 100, 200))

@@ -2,7 +2,9 @@
 mesh/build_state.py), after tests/mesh/test_io_grd.py, test_io_top.py and
 test_build_state.py.  The fixtures under tests/golden are written by
 tests/golden/make_mesh_fixtures.py; when the reference tree is present its own
-fixtures are parsed too."""
+fixtures are parsed too (set FAMRDP_JAX_REFERENCE to the root of a
+famrdp_jax checkout)."""
+import os
 from pathlib import Path
 
 import numpy as np
@@ -17,7 +19,10 @@ from famrdp_jax_b200.mesh.io_grd import read_grd, write_grd
 from famrdp_jax_b200.mesh.io_top import _face, parse_topology
 
 GOLD = Path(__file__).parent / "golden"
-REF_FIX = Path("/root/reference/tests/fixtures")
+# the reference project's own fixtures, when a checkout is named by
+# FAMRDP_JAX_REFERENCE (its root directory); skipped otherwise
+_REF_ROOT = os.environ.get("FAMRDP_JAX_REFERENCE")
+REF_FIX = Path(_REF_ROOT) / "tests" / "fixtures" if _REF_ROOT else Path("/nonexistent")
 
 
 def test_read_grd_shapes_and_values():

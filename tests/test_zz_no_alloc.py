@@ -6,8 +6,10 @@ in one fixed array inside the library instead of cudaMalloc'd scratch.
 
 Checked here through the C ABI: two calls in a row on different blocks
 agree with fj_rhs_f64 (the context-scratch entry point) within the RHS
-tolerance of the parity tests, and a block too large for the fixed array is
-refused before any device work.  This file is collected last on purpose.
+tolerance of the parity tests; a call allocates no device memory (the
+device's free memory is the same before and after it); and a block too large
+for the fixed array is refused before any device work.  This file is
+collected last on purpose.
 """
 import ctypes
 
@@ -66,3 +68,26 @@ def test_noalloc_rejects_blocks_beyond_capacity(cuda_device):
     status, _ = _rhs_no_alloc(q, kxyz, vol, p)
     assert status == _capi.FJ_ERR_SCRATCH_LIMIT
     assert b"fixed scratch" in _capi.lib().fj_status_string(status)
+
+
+def test_noalloc_call_allocates_no_device_memory(cuda_device):
+    """After a first call (which loads the library's module and looks up the
+    array's address), a call on a larger block leaves the device's free
+    memory unchanged: no allocation by the library, the driver or torch."""
+    p = _capi.params(GAS, limiter="minmod", ghost=2, precision="f64")
+    q, kxyz, vol = random_block((10, 9, 8), 40)
+    status, _ = _rhs_no_alloc(dev(q), dev(kxyz), dev(vol), p)
+    assert status == _capi.FJ_OK
+    q, kxyz, vol = random_block((60, 58, 62), 41)
+    qd, kd, vd = dev(q), dev(kxyz), dev(vol)
+    out = torch.empty_like(qd)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(cuda_device)
+    ni, nj, nk = qd.shape[1:]
+    status = _capi.lib().fj_rhs_noalloc_f64(qd.data_ptr(), kd.data_ptr(), vd.data_ptr(), out.data_ptr(),
+                                            ni, nj, nk, ctypes.byref(p), _capi.stream(qd.device))
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info(cuda_device)
+    assert status == _capi.FJ_OK
+    assert free_after == free_before, (free_before, free_after)
+    assert torch.isfinite(out).all()
