@@ -77,6 +77,10 @@ SIGNATURES = {
     "fj_plan_set_ensemble": (_I, [_P, _P, _P]),
     "fj_plan_set_variant": (_I, [_P, _I]),
     "fj_plan_set_streams": (_I, [_P, _I]),
+    "fj_plan_set_kernel": (_I, [_P, _I]),
+    "fj_plan_get_kernel": (_I, [_P, ctypes.POINTER(_I)]),
+    "fj_plan_set_wait_limit": (_I, [_P, _I]),
+    "fj_plan_check": (_I, [_P, ctypes.POINTER(_I), _P]),
     "fj_plan_autotune": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _I, ctypes.POINTER(_I), _P, _P]),
     "fj_plan_step_graph": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_step_save": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
@@ -166,6 +170,7 @@ PIPELINES = {"fused": 0, "staged": 1, "split": 2}
 
 
 NUM_SPLIT_VARIANTS = 6  # FJ_NUM_SPLIT_VARIANTS
+KERNELS = {"split": 0, "tile": 1}  # FJ_KERNEL_SPLIT, FJ_KERNEL_TILE
 TILES = {"8x32": 0, "4x32": 1, "6x32": 2, "8x16": 3, "16x32": 4, "8x64": 5, "16x16": 6}
 
 

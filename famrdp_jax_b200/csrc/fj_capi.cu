@@ -10,6 +10,7 @@
 #include "fj_common.cuh"
 #include "fj_rhs.cuh"
 #include "fj_split.cuh"
+#include "fj_tile.cuh"
 #include "fj_stage.cuh"
 
 namespace fj {
@@ -154,7 +155,7 @@ int check_step_args(fj_ctx* ctx, const fj_block* blocks, double* const* q_out, i
 // intermediates; the other pipelines run block by block and size everything
 // for the largest block.  The halo slabs reuse the tail (the halo runs first).
 size_t step_layout(const fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
-                   int nlinks, const fj_params* p, size_t* stage_b, size_t* tail_b) {
+                   int nlinks, const fj_params* p, size_t* stage_b, size_t* tail_b, bool with_tile = false) {
   size_t maxN = 0, sumStage = 0, rhs_b = 0;
   int64_t cells = 0;
   for (int b = 0; b < nblocks; ++b) {
@@ -166,7 +167,10 @@ size_t step_layout(const fj_ctx* ctx, const fj_block* blocks, int nblocks, const
   }
   const bool split = ctx->pipeline == FJ_PIPELINE_SPLIT;
   *stage_b = split ? sumStage : align256(5 * maxN * sizeof(double));
-  const size_t work = split ? split_scratch_bytes(p->precision, cells) : rhs_b;
+  size_t work = split ? split_scratch_bytes(p->precision, cells) : rhs_b;
+  // FP32-flux split plans may run the tile kernel, whose padded primitive
+  // buffers share the tail with the split intermediates
+  if (split && with_tile && p->precision == FJ_PREC_F32FLUX) work = std::max(work, tile_scratch_bytes(blocks, nblocks));
   *tail_b = align256(std::max(std::max(work, halo_ws_bytes(blocks, links, nlinks, p->ghost)), (size_t)256));
   return 2 * *stage_b + *tail_b;
 }
@@ -191,7 +195,43 @@ struct StepOpts {
   // the second group half a stage later was slower)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // FP32-flux split plans: run the stages with the fused TMA-tile kernel
+  const TileMaps* tile = nullptr;
+  int wait_limit = -1;
 };
+
+// The three stages of all blocks with the tile kernel: the primitives of the
+// halo-filled start state into padded buffer 0, then stage 1 (buffer 0 ->
+// stage result q1 + its primitives in buffer 1), stage 2 (1 -> 0), stage 3.
+int tile_step(fj_ctx* ctx, const std::vector<fj_block>& out, double* const* q1s, double* const* q2s,
+              double* const* q_out, const fj_params* p, double dt, void* const* kmet, cudaStream_t st,
+              const StepOpts& o) {
+  const int nb = (int)out.size();
+  std::vector<const double*> q0v(nb);
+  for (int b = 0; b < nb; ++b) q0v[b] = out[b].q;
+  int s = tile_prims(ctx, *o.tile, 0, q0v.data(), out.data(), nb, p->gamma - 1.0, p->R, o.p_ref, st);
+  Phys ph = make_phys(p);
+  ph.p_ref = o.p_ref;
+  std::vector<TileBlock> tb(nb);
+  for (int stage = 1; stage <= 3 && s == FJ_OK; ++stage) {
+    for (int b = 0; b < nb; ++b) {
+      TileBlock& B = tb[b];
+      B = TileBlock{};
+      B.q = stage == 1 ? out[b].q : (stage == 2 ? q1s[b] : q2s[b]);
+      B.q0 = out[b].q;
+      B.out = stage == 1 ? q1s[b] : (stage == 2 ? q2s[b] : q_out[b]);
+      B.kaos = (const float*)kmet[b];
+      B.vol = out[b].vol;
+      B.mu0 = o.mu0_b ? o.mu0_b[b] : p->mu0;
+      B.dt = o.dt_b ? o.dt_b[b] : dt;
+      B.ni = out[b].ni;
+      B.nj = out[b].nj;
+      B.nk = out[b].nk;
+    }
+    s = tile_stage(ctx, *o.tile, stage == 2 ? 1 : 0, tb.data(), nb, ph, stage, st, o.wait_limit);
+  }
+  return s;
+}
 
 int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* const* q1s,
               double* const* q2s, double* const* q_out, int nblocks, const fj_link* links, int nlinks,
@@ -216,6 +256,8 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
   s = apply_bc(ctx, out.data(), nblocks, bcs, nbcs, p, st);
   if (s != FJ_OK) return s;
   const int flags = kRhsInvscd | kRhsViscous;
+  if (ctx->pipeline == FJ_PIPELINE_SPLIT && o.tile && p->precision == FJ_PREC_F32FLUX && kmet)
+    return tile_step(ctx, out, q1s, q2s, q_out, p, dt, kmet, st, o);
   if (ctx->pipeline == FJ_PIPELINE_SPLIT) {
     // all blocks per launch; the tail holds the intermediates of every block
     std::vector<SplitBlock> sb(nblocks);
@@ -512,7 +554,8 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
   pl->p = *p;
   // the plan keeps the context's pipeline choice of its creation time
   pl->pipeline = ctx->pipeline;
-  const size_t total = step_layout(ctx, blocks, nblocks, links, nlinks, p, &pl->stage_bytes, &pl->halo_bytes);
+  const size_t total =
+      step_layout(ctx, blocks, nblocks, links, nlinks, p, &pl->stage_bytes, &pl->halo_bytes, true);
   cudaError_t e = cudaMalloc(&pl->scratch, total);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -569,6 +612,19 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
         s = FJ_ERR_NO_MEMORY;
       if (s != FJ_OK || !std::isfinite(pl->p_ref)) pl->p_ref = 0.0;
     }
+    // the fused TMA-tile kernel: padded primitive buffers in the tail and
+    // their tensor maps (absent when the driver's encoder is unavailable)
+    if (split) {
+      TileMaps* tm = new (std::nothrow) TileMaps();
+      if (tm && tile_setup(blocks, nblocks, (char*)pl->scratch + 2 * pl->stage_bytes, *tm) &&
+          tile_clear_error(*tm, pl->capture_stream) == FJ_OK &&
+          cudaStreamSynchronize(pl->capture_stream) == cudaSuccess) {
+        pl->tile = tm;
+      } else {
+        delete tm;
+        cudaGetLastError();
+      }
+    }
   }
   *out = pl;
   return FJ_OK;
@@ -600,6 +656,10 @@ static int plan_step_impl(fj_plan* pl, double* const* q_in, double* const* q_out
   opts.dt_b = pl->dt_b.empty() ? nullptr : pl->dt_b.data();
   opts.p_ref = pl->p_ref;
   opts.variant = pl->variant;
+  if (pl->kernel == FJ_KERNEL_TILE && pl->tile) {
+    opts.tile = (const TileMaps*)pl->tile;
+    opts.wait_limit = pl->wait_limit;
+  }
   if (pl->streams == 2) {
     opts.side = pl->side_stream;
     opts.fork = pl->ev_fork;
@@ -664,6 +724,51 @@ int fj_plan_set_streams(fj_plan* pl, int n) {
   return FJ_OK;
 }
 
+int fj_plan_set_kernel(fj_plan* pl, int kernel) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  if (kernel != FJ_KERNEL_SPLIT && kernel != FJ_KERNEL_TILE)
+    return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "unknown stage kernel");
+  if (kernel == FJ_KERNEL_TILE && !pl->tile)
+    return set_err(pl->ctx, FJ_ERR_NOT_IMPLEMENTED,
+                   "the tile kernel needs an FP32-flux split plan and the driver's tensor-map encoder");
+  if (kernel != pl->kernel) drop_graphs(pl);
+  pl->kernel = kernel;
+  return FJ_OK;
+}
+
+int fj_plan_get_kernel(const fj_plan* pl, int* kernel) {
+  if (!pl || !kernel) return FJ_ERR_INVALID_ARGUMENT;
+  *kernel = pl->kernel;
+  return FJ_OK;
+}
+
+int fj_plan_set_wait_limit(fj_plan* pl, int limit) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  if (limit < -1) return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "limit must be >= -1");
+  if (limit != pl->wait_limit) drop_graphs(pl);
+  pl->wait_limit = limit;
+  return FJ_OK;
+}
+
+int fj_plan_check(fj_plan* pl, int* word, void* stream) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  int w = 0;
+  if (pl->tile) {
+    const TileMaps& tm = *(const TileMaps*)pl->tile;
+    int s = tile_read_error(tm, &w, S(stream));
+    if (s == FJ_OK && w != 0) s = tile_clear_error(tm, S(stream));
+    if (s == FJ_OK) s = cuda_status(pl->ctx, cudaStreamSynchronize(S(stream)), "plan check");
+    if (s != FJ_OK) return s;
+  } else {
+    int s = cuda_status(pl->ctx, cudaStreamSynchronize(S(stream)), "plan check");
+    if (s != FJ_OK) return s;
+  }
+  if (word) *word = w;
+  return w == 0 ? FJ_OK
+                : set_err(pl->ctx, FJ_ERR_CUDA, "a bounded wait of the tile kernel gave up (error word " +
+                                                    std::to_string(w) + ")");
+}
+
 int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, int reps, int* chosen,
                      double* ms_out, void* stream) {
   if (!pl || !chosen || reps < 1) return FJ_ERR_INVALID_ARGUMENT;
@@ -672,34 +777,55 @@ int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, dou
   const bool tunable = split && pl->p.precision == FJ_PREC_F32FLUX;
   const int nv = tunable ? FJ_NUM_SPLIT_VARIANTS : 1;
   const int ns = split && pl->blocks.size() >= 2 ? 2 : 1;
+  const bool with_tile = tunable && pl->tile != nullptr;
   if (ms_out)
-    for (int i = 0; i < 2 * FJ_NUM_SPLIT_VARIANTS; ++i) ms_out[i] = 0.0;
+    for (int i = 0; i < 2 * FJ_NUM_SPLIT_VARIANTS + 1; ++i) ms_out[i] = 0.0;
   cudaStream_t st = S(stream);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int s = cuda_status(ctx, cudaEventCreate(&e0), "event");
   if (s == FJ_OK) s = cuda_status(ctx, cudaEventCreate(&e1), "event");
-  const int keep_v = pl->variant, keep_s = pl->streams;
-  int best_v = keep_v, best_s = keep_s;
+  const int keep_v = pl->variant, keep_s = pl->streams, keep_k = pl->kernel;
+  int best_v = keep_v, best_s = keep_s, best_k = keep_k;
   float best_ms = -1.0f;
+  // mean step time of the plan's current settings over `reps` steps
+  auto time_steps = [&](float& ms) -> int {
+    int t = plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);  // untimed
+    if (t == FJ_OK) t = cuda_status(ctx, cudaEventRecord(e0, st), "event record");
+    for (int r = 0; r < reps && t == FJ_OK; ++r) t = plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);
+    if (t == FJ_OK) t = cuda_status(ctx, cudaEventRecord(e1, st), "event record");
+    if (t == FJ_OK) t = cuda_status(ctx, cudaEventSynchronize(e1), "event sync");
+    if (t == FJ_OK) t = cuda_status(ctx, cudaEventElapsedTime(&ms, e0, e1), "event time");
+    return t;
+  };
+  if (s == FJ_OK) s = fj_plan_set_kernel(pl, FJ_KERNEL_SPLIT);
   for (int sn = 1; sn <= ns && s == FJ_OK; ++sn) {
     for (int v = 0; v < nv && s == FJ_OK; ++v) {
       s = fj_plan_set_variant(pl, tunable ? v : keep_v);
       if (s == FJ_OK) s = fj_plan_set_streams(pl, sn);
-      if (s == FJ_OK) s = plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);  // untimed
-      if (s == FJ_OK) s = cuda_status(ctx, cudaEventRecord(e0, st), "event record");
-      for (int r = 0; r < reps && s == FJ_OK; ++r)
-        s = plan_step_impl(pl, q_in, q_out, nullptr, nullptr, nullptr, dt, stream);
-      if (s == FJ_OK) s = cuda_status(ctx, cudaEventRecord(e1, st), "event record");
-      if (s == FJ_OK) s = cuda_status(ctx, cudaEventSynchronize(e1), "event sync");
       float ms = 0.0f;
-      if (s == FJ_OK) s = cuda_status(ctx, cudaEventElapsedTime(&ms, e0, e1), "event time");
+      if (s == FJ_OK) s = time_steps(ms);
       if (s == FJ_OK) {
         if (ms_out) ms_out[(sn - 1) * FJ_NUM_SPLIT_VARIANTS + v] = ms / reps;
         if (best_ms < 0.0f || ms < best_ms) {
           best_ms = ms;
           best_v = tunable ? v : keep_v;
           best_s = sn;
+          best_k = FJ_KERNEL_SPLIT;
         }
+      }
+    }
+  }
+  if (with_tile && s == FJ_OK) {
+    s = fj_plan_set_streams(pl, 1);
+    if (s == FJ_OK) s = fj_plan_set_kernel(pl, FJ_KERNEL_TILE);
+    float ms = 0.0f;
+    if (s == FJ_OK) s = time_steps(ms);
+    if (s == FJ_OK) {
+      if (ms_out) ms_out[2 * FJ_NUM_SPLIT_VARIANTS] = ms / reps;
+      if (best_ms < 0.0f || ms < best_ms) {
+        best_ms = ms;
+        best_s = 1;
+        best_k = FJ_KERNEL_TILE;
       }
     }
   }
@@ -707,8 +833,10 @@ int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, dou
   if (e1) cudaEventDestroy(e1);
   int r = fj_plan_set_variant(pl, s == FJ_OK ? best_v : keep_v);
   if (r == FJ_OK) r = fj_plan_set_streams(pl, s == FJ_OK ? best_s : keep_s);
+  if (r == FJ_OK) r = fj_plan_set_kernel(pl, s == FJ_OK ? best_k : keep_k);
   if (s == FJ_OK) s = r;
-  *chosen = pl->variant + FJ_NUM_SPLIT_VARIANTS * (pl->streams - 1);
+  *chosen = pl->kernel == FJ_KERNEL_TILE ? 2 * FJ_NUM_SPLIT_VARIANTS
+                                         : pl->variant + FJ_NUM_SPLIT_VARIANTS * (pl->streams - 1);
   return s;
 }
 
@@ -790,7 +918,33 @@ int fj_plan_stage(fj_plan* pl, double* const* q, double* const* q0, double* cons
   const int saved = ctx->pipeline;
   ctx->pipeline = pl->pipeline;
   int s = FJ_OK;
-  if (pl->pipeline == FJ_PIPELINE_SPLIT) {
+  if (pl->pipeline == FJ_PIPELINE_SPLIT && pl->kernel == FJ_KERNEL_TILE && pl->tile && !pl->kmet.empty()) {
+    // the tile kernel: the primitives of q into padded buffer 0, then the stage
+    // (which, for stages 1 and 2, also writes its result's primitives)
+    const TileMaps& tm = *(const TileMaps*)pl->tile;
+    std::vector<fj_block> in(pl->blocks);
+    for (int b = 0; b < nb; ++b) in[b].q = q[b];
+    std::vector<const double*> qv(q, q + nb);
+    s = tile_prims(ctx, tm, 0, qv.data(), in.data(), nb, pl->p.gamma - 1.0, pl->p.R, pl->p_ref, S(stream));
+    Phys ph = make_phys(&pl->p);
+    ph.p_ref = pl->p_ref;
+    std::vector<TileBlock> tb(nb);
+    for (int b = 0; b < nb; ++b) {
+      const fj_block& B = pl->blocks[b];
+      tb[b] = TileBlock{};
+      tb[b].q = q[b];
+      tb[b].q0 = stage > 1 ? q0[b] : q[b];
+      tb[b].out = out[b];
+      tb[b].kaos = (const float*)pl->kmet[b];
+      tb[b].vol = B.vol;
+      tb[b].mu0 = pl->mu0_b.empty() ? pl->p.mu0 : pl->mu0_b[b];
+      tb[b].dt = pl->dt_b.empty() ? dt : pl->dt_b[b];
+      tb[b].ni = B.ni;
+      tb[b].nj = B.nj;
+      tb[b].nk = B.nk;
+    }
+    if (s == FJ_OK) s = tile_stage(ctx, tm, 0, tb.data(), nb, ph, stage, S(stream), pl->wait_limit);
+  } else if (pl->pipeline == FJ_PIPELINE_SPLIT) {
     std::vector<SplitBlock> sb(nb);
     for (int b = 0; b < nb; ++b) {
       const fj_block& B = pl->blocks[b];
@@ -1041,6 +1195,7 @@ int fj_plan_destroy(fj_plan* pl) {
   for (void* k : pl->kmet)
     if (k) cudaFree(k);
   if (pl->scratch) cudaFree(pl->scratch);
+  delete (TileMaps*)pl->tile;
   delete pl;
   return FJ_OK;
 }

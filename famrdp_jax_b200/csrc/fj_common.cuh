@@ -55,6 +55,13 @@ struct fj_plan {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t capture_stream = nullptr;  // private stream for graph capture
   std::vector<fj_graph_entry> graphs;     // most recently used last
+  // FP32-flux split plans: which stage kernels run (FJ_KERNEL_SPLIT: the three
+  // split kernels; FJ_KERNEL_TILE: the fused TMA-tile kernel), the tile
+  // kernel's plan data (fj::TileMaps, owned; nullptr when unavailable) and its
+  // bounded-wait limit (-1: the default)
+  int kernel = FJ_KERNEL_SPLIT;
+  void* tile = nullptr;
+  int wait_limit = -1;
 };
 
 namespace fj {

@@ -14,6 +14,11 @@ and two errors are reported per direction:
     derivative's bound for a unit direction.
 The gradient direction itself (d = g / |g|, where fd should equal |g|) and
 dJ/dmu0 (central differences in mu0 with step eps_mu * mu0) are checked too.
+eps_mu defaults to 1e-3: J moves by about 2 eps_mu mu0 |dJ/dmu0| between the
+two evaluations, and at 1e-6 that is within a few thousand FP64 roundings of
+J on a 96^3 block over 50 steps (measured: a 2.3e-5 relative error that is
+rounding, not the adjoint); J depends smoothly on mu0 (the viscous RHS is
+linear in it), so the larger step costs no measurable truncation error.
 J is only piecewise smooth (minmod switches where two slopes have equal
 magnitude or a slope changes sign): a +-eps perturbation that crosses one of
 those points biases fd, so single directions can disagree at any eps.
@@ -42,7 +47,7 @@ def _objective(plan: StepPlan, state: State, q0s, nsteps: int, dt: float, ghost:
 
 
 def fd_check_kinetic_energy(state: State, cfg, dt: float, nsteps: int, *, checkpoint_every: int = 10,
-                            eps: float = 1e-6, ndirs: int = 16, seed: int = 0, eps_mu: float = 1e-6) -> dict:
+                            eps: float = 1e-6, ndirs: int = 16, seed: int = 0, eps_mu: float = 1e-3) -> dict:
     """Adjoint gradient of J = interior kinetic energy after nsteps steps
     against central differences; returns the per-direction errors and their
     maxima (see the module docstring)."""

@@ -112,10 +112,12 @@ class StepPlan:
 
     def autotune(self, qs, outs, dt: float, reps: int = 3):
         """Times every launch shape of the FP32-flux split kernels and both
-        stream counts over `reps` steps qs -> outs (outs is overwritten) and
-        keeps the fastest; returns (chosen, mean step ms per candidate), the
-        candidate index being shape + NUM_SPLIT_VARIANTS * (streams - 1)."""
-        n = 2 * _capi.NUM_SPLIT_VARIANTS
+        stream counts, and the fused tile kernel, over `reps` steps qs -> outs
+        (outs is overwritten) and keeps the fastest; returns (chosen, mean step
+        ms per candidate), the candidate index being shape +
+        NUM_SPLIT_VARIANTS * (streams - 1), or 2 * NUM_SPLIT_VARIANTS for the
+        tile kernel."""
+        n = 2 * _capi.NUM_SPLIT_VARIANTS + 1
         ms = (ctypes.c_double * n)()
         ch = ctypes.c_int()
         c = _capi.ctx(self.device)
@@ -127,6 +129,37 @@ class StepPlan:
     def set_streams(self, n: int) -> None:
         c = _capi.ctx(self.device)
         _capi.check(self._lib.fj_plan_set_streams(self._handle, int(n)), "fj_plan_set_streams", c)
+
+    def set_kernel(self, kernel: str) -> None:
+        """Stage kernels of an FP32-flux plan: "split" (three kernels per stage
+        through scratch) or "tile" (one persistent fused kernel per stage over a
+        (tile, i-plane) work-list, primitive planes staged by TMA)."""
+        if kernel not in _capi.KERNELS:
+            raise KeyError(kernel)
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_set_kernel(self._handle, _capi.KERNELS[kernel]), "fj_plan_set_kernel", c)
+
+    @property
+    def kernel(self) -> str:
+        k = ctypes.c_int()
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_get_kernel(self._handle, ctypes.byref(k)), "fj_plan_get_kernel", c)
+        return {v: n for n, v in _capi.KERNELS.items()}[k.value]
+
+    def set_wait_limit(self, limit: int) -> None:
+        """Tries of each bounded wait in the tile kernel (-1: the default)."""
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_set_wait_limit(self._handle, int(limit)), "fj_plan_set_wait_limit", c)
+
+    def check(self) -> int:
+        """Waits for the plan's work on the current stream and returns the tile
+        kernel's error word (0: no bounded wait gave up), clearing it; raises
+        RuntimeError when it was nonzero."""
+        w = ctypes.c_int()
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_check(self._handle, ctypes.byref(w), _capi.stream(self.device)),
+                    "fj_plan_check", c)
+        return w.value
 
     def set_variant(self, variant: int) -> None:
         c = _capi.ctx(self.device)

@@ -276,6 +276,30 @@ int fj_plan_set_ensemble(fj_plan* plan, const double* mu0, const double* dt);
  * Results do not depend on it. */
 #define FJ_NUM_SPLIT_VARIANTS 6
 int fj_plan_set_variant(fj_plan* plan, int variant);
+/* Stage kernels of an FP32-flux split plan (no counterpart in the reference,
+ * whose rhs/step are one XLA program): FJ_KERNEL_SPLIT runs each stage as the
+ * three split kernels through scratch; FJ_KERNEL_TILE runs it as ONE
+ * persistent launch over a work-list of (8 x 30 (j, k) tile, i-plane) units
+ * of all blocks, each CTA streaming along i with its primitive planes staged
+ * by TMA (cp.async.bulk.tensor) from a padded FP32 copy that holds the
+ * periodic images, every intermediate in shared memory or registers.  The
+ * results agree to FP32 rounding (the face arithmetic is the same; the
+ * temperature is formed in FP32).  FJ_KERNEL_TILE returns
+ * FJ_ERR_NOT_IMPLEMENTED for FP64 or non-split plans and when the driver's
+ * tensor-map encoder is unavailable.  Changing it drops captured graphs. */
+#define FJ_KERNEL_SPLIT 0
+#define FJ_KERNEL_TILE 1
+int fj_plan_set_kernel(fj_plan* plan, int kernel);
+int fj_plan_get_kernel(const fj_plan* plan, int* kernel);
+/* Diagnostics of the tile kernel's bounded waits: every wait for a TMA copy
+ * gives up after `limit` tries (-1 restores the default, about a second);
+ * a CTA whose wait gave up records it in the plan's error word, stops and
+ * exits after its copies in flight have landed (never a trap or a hang).
+ * fj_plan_check waits for `stream`, stores the word (0 = no wait gave up) in
+ * *word, clears it, and returns FJ_ERR_CUDA when it was nonzero.  limit = 0
+ * makes every wait give up at once (used by the tests). */
+int fj_plan_set_wait_limit(fj_plan* plan, int limit);
+int fj_plan_check(fj_plan* plan, int* word, void* stream);
 /* Split-pipeline plans of two or more blocks: n = 2 splits the blocks into two
  * groups of about equal cells whose three stages run on two streams (forked
  * from and joined back into the step's stream), so one group's flux kernels
@@ -285,10 +309,12 @@ int fj_plan_set_streams(fj_plan* plan, int n);
 /* The autotuner: times `reps` steps q_in -> q_out (after one untimed step) for
  * every launch shape (FP32-flux split plans) and stream count (split plans of
  * two or more blocks) with CUDA events on `stream`, keeps the fastest in the
- * plan and reports it as shape + FJ_NUM_SPLIT_VARIANTS * (streams - 1) (and,
- * if ms_out is non-NULL, the 2 * FJ_NUM_SPLIT_VARIANTS mean step times at that
- * index; 0 where not timed).  q_out is overwritten; q_in is not changed.
- * Synchronises the stream. */
+ * plan and reports it as shape + FJ_NUM_SPLIT_VARIANTS * (streams - 1), or
+ * 2 * FJ_NUM_SPLIT_VARIANTS for the tile kernel (FP32-flux plans whose tile
+ * kernel is available: one more candidate) (and, if ms_out is non-NULL, the
+ * 2 * FJ_NUM_SPLIT_VARIANTS + 1 mean step times at those indices; 0 where not
+ * timed).  q_out is overwritten; q_in is not changed.  Synchronises the
+ * stream. */
 int fj_plan_autotune(fj_plan* plan, double* const* q_in, double* const* q_out, double dt, int reps,
                      int* chosen, double* ms_out, void* stream);
 int fj_plan_step_graph(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,

@@ -7,7 +7,8 @@ Bounds (see famrdp_jax_b200/solver/gradcheck.py for the two error measures):
   * every direction: |fd - ad| <= 1e-6 |grad J|;
   * the gradient direction: |fd - |g|| <= 1e-6 |g| (a per-direction relative
     bound where the directional derivative is large enough to resolve);
-  * dJ/dmu0: relative error <= 1e-6.
+  * dJ/dmu0: relative error <= 1e-6 (central difference in mu0 with step
+    1e-3 mu0; see gradcheck.py for why not 1e-6).
 The per-direction relative errors of the random directions are printed, not
 bounded: their derivatives are about |grad J| / sqrt(5e6) and FP64 rounding
 of J divided by eps is of that order.
