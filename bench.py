@@ -76,7 +76,7 @@ STEP_BYTES = {"f64": 560.0, "f32": 452.0}
 # measured by ncu on `bench.py --stage-only --n 96` (4 blocks of 100^3 padded
 # cells, 4.0 M) and scaled per cell: FP32 59 + 147 + 283 B, FP64 74 + 301 +
 # 401 B
-STAGE_TRAFFIC = {"f32": 489.0, "f64": 777.0}
+STAGE_TRAFFIC = {("f32", "split"): 489.0, ("f64", "split"): 777.0}
 
 
 def _peaks():
@@ -437,13 +437,17 @@ def _stage_roofline(plan, q0s, dt, prec, padded_cells):
     alg = STAGE_BYTES[prec] * padded_cells
     peak, peak_kind = _peaks()
     achieved = alg / (stage_ms / 1e3) / 1e9
-    traffic = STAGE_TRAFFIC.get(prec)
+    kern = plan.kernel
+    traffic = STAGE_TRAFFIC.get((prec, kern))
     del qin, outs
+    what = ("one TVD-RK3 stage of all blocks (fused TMA-tile kernel: one persistent launch, plus the launch "
+            "that fills the padded primitive planes)" if kern == "tile" else
+            "one TVD-RK3 stage of all blocks (split pipeline: prims, fluxes, assembly; 3 launches)")
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic * padded_cells if traffic else None,
             "traffic_note": f"{traffic:.0f} B per padded cell (ncu dram__bytes_read+write of the stage-2 group on "
                             f"4 x 100^3 padded cells) x the cells of one launch" if traffic else None,
-            "kernel": "one TVD-RK3 stage of all blocks (split pipeline: prims, fluxes, assembly; 3 launches)",
+            "kernel": what, "stage_kernel": kern,
             "alg_bytes_per_cell": STAGE_BYTES[prec], "alg_bytes_per_launch": alg, "launch_ms": stage_ms,
             "peak_kind": peak_kind}
 
@@ -498,7 +502,7 @@ def _end_to_end(plan, cfg, state, q0s, dt, cells, steps, ws, device, barrier):
             "pipelined_value": _throughput(cells, e2e_steps, piped_ms, ws)}
 
 
-def measure_case(case, prec, steps, warm, device, ws, local, barrier, ens=None, sample_clocks=False):
+def measure_case(case, prec, steps, warm, device, ws, local, barrier, ens=None, sample_clocks=False, kernel="auto"):
     """Graph-replayed steps of one workload in one precision: throughput,
     launches, the autotuner's choice, the stage-group roofline and the
     end-to-end figure.  Returns (record, final state, clock summary)."""
@@ -517,6 +521,8 @@ def measure_case(case, prec, steps, warm, device, ws, local, barrier, ens=None, 
     qa = [b.q for b in state.blocks]
     qb = [torch.empty_like(q) for q in qa]
     tuned = plan.autotune(qa, qb, dt, reps=3)  # launch shape of the FP32 kernels (qb is scratch here)
+    if prec == "f32" and kernel != "auto":
+        plan.set_kernel(kernel)
     for _ in range(warm):  # also captures the two ping-pong step graphs
         plan.run(qa, qb, dt, graph=True)
         qa, qb = qb, qa
@@ -584,6 +590,8 @@ def run_ours(args):
         plan = StepPlan(st0, cfg)
         if args.precision == "f32":
             plan.set_variant(args.shape)
+            if args.kernel != "auto":
+                plan.set_kernel(args.kernel)
         q0s = [b.q for b in st0.blocks]
         qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state
         outs = [torch.empty_like(q) for q in q0s]
@@ -592,6 +600,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"stage_only": True, "precision": args.precision, "shape": args.shape,
+                              "kernel": plan.kernel,
                               "padded_cells": case.padded_cells}), flush=True)
         return 0
 
@@ -613,7 +622,7 @@ def run_ours(args):
     clk_summary = None
     for prec in order:
         rec, finals[prec], clk = measure_case(case, prec, args.steps, warm, device, ws, local, barrier, ens,
-                                              sample_clocks=(prec == args.precision))
+                                              sample_clocks=(prec == args.precision), kernel=args.kernel)
         results[prec] = rec
         if clk is not None:
             clk_summary = clk
@@ -633,7 +642,8 @@ def run_ours(args):
             del st2
             entry = {"config": workload_desc(c2, sub)}
             for prec in ("f32", "f64"):
-                rec, _, _ = measure_case(c2, prec, args.steps, warm, device, ws, local, barrier, ens2)
+                rec, _, _ = measure_case(c2, prec, args.steps, warm, device, ws, local, barrier, ens2,
+                                         kernel=args.kernel)
                 entry[prec] = rec
             entry["f32_over_f64"] = entry["f64"]["ms_per_step"] / entry["f32"]["ms_per_step"]
             others[wl] = entry
@@ -679,6 +689,8 @@ def main(argv=None):
     ap.add_argument("--stage-only", action="store_true",
                     help="only run four standalone stage-2 evaluations (for a profiler)")
     ap.add_argument("--shape", type=int, default=1, help="FP32 launch shape for --stage-only")
+    ap.add_argument("--kernel", choices=["auto", "split", "tile"], default="auto",
+                    help="FP32 stage kernels: auto = the autotuner's choice (split shapes and the tile kernel)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")

@@ -219,7 +219,8 @@ __device__ __forceinline__ void invscd_face(const Prim<T> c[4], T kl0, T kl1, T 
 // ---------------------------------------------------------------------------
 template <typename T> struct FastMath;
 template <> struct FastMath<double> {
-  static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+  // __drcp_rn: the IEEE round-to-nearest reciprocal, the same value as 1.0 / x
+  static __device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
   static __device__ __forceinline__ double sqrt_pos(double x) { return sqrt(x); }
   static __device__ __forceinline__ double sqrt_nn(double x) { return sqrt(x); }
 };
@@ -278,27 +279,61 @@ __device__ __forceinline__ void roe_prim(const Prim<T>& L, const Prim<T>& R, T n
   const T Ec = POFF ? p_ref * inv_gm1 : T(0), Hc = POFF ? p_ref * (inv_gm1 + T(1)) : T(0);
   const T EL = POFF ? eL + Ec : eL;
   const T ER = POFF ? eR + Ec : eR;
-  const T HL = (POFF ? (eL + L.p) + Hc : EL + L.p) * M::rcp(rhoL);
-  const T HR = (POFF ? (eR + R.p) + Hc : ER + R.p) * M::rcp(rhoR);
-  const T sqL = M::sqrt_pos(rhoL), sqR = M::sqrt_pos(rhoR);
-  const T inv_ss = M::rcp(fj_max(sqL + sqR, Tiny<T>::ss()));
-  const T wl = sqL * inv_ss, wr = sqR * inv_ss;
+  const T irL = M::rcp(rhoL), irR = M::rcp(rhoR);
+  const T HL = (POFF ? (eL + L.p) + Hc : EL + L.p) * irL;
+  const T HR = (POFF ? (eR + R.p) + Hc : ER + R.p) * irR;
+  // Roe weights sqL / (sqL + sqR), sqR / (sqL + sqR) and rho_h = sqL sqR.  In
+  // FP64 from one square root, t = sqrt(rhoR / rhoL): wl = 1 / (1 + t),
+  // wr = t / (1 + t), rho_h = rhoL t (the same values; the reference's clamp
+  // of sqL + sqR at 1e-150 cannot bind once rho >= 1e-300).  FP32 keeps the
+  // two MUFU square roots.
+  T wl, wr, rho_h;
+  if constexpr (sizeof(T) == 8) {
+    const T t = sqrt(rhoR * irL);
+    wl = M::rcp(T(1) + t);
+    wr = t * wl;
+    rho_h = rhoL * t;
+  } else {
+    const T sqL = M::sqrt_pos(rhoL), sqR = M::sqrt_pos(rhoR);
+    const T inv_ss = M::rcp(fj_max(sqL + sqR, Tiny<T>::ss()));
+    wl = sqL * inv_ss;
+    wr = sqR * inv_ss;
+    rho_h = sqL * sqR;
+  }
   const T u_h = wl * L.u + wr * R.u;
   const T v_h = wl * L.v + wr * R.v;
   const T w_h = wl * L.w + wr * R.w;
   const T H_h = wl * HL + wr * HR;
   const T q2 = u_h * u_h + v_h * v_h + w_h * w_h;
   const T c2 = fj_max(gm1 * (H_h - T(0.5) * q2), Tiny<T>::c2());
-  const T c_h = M::sqrt_pos(c2);
-  const T inv_c2 = M::rcp(c2);
+  T c_h, inv_c2;
+  if constexpr (sizeof(T) == 8) {
+    // one reciprocal square root for c and 1/c^2 (c2 >= 1e-30 > 0)
+    const T ic = rsqrt(c2);
+    c_h = c2 * ic;
+    inv_c2 = ic * ic;
+  } else {
+    c_h = M::sqrt_pos(c2);
+    inv_c2 = M::rcp(c2);
+  }
   const T un_h = u_h * n0 + v_h * n1 + w_h * n2;
-  const T rho_h = sqL * sqR;
 
   const T eps = eps_entropy * (fj_abs(un_h) + c_h);
-  const T inv_eps = M::rcp(eps);
   const T lam1 = un_h - c_h, lam5 = un_h + c_h;
-  const T al1 = fj_abs(lam1) >= eps ? fj_abs(lam1) : T(0.5) * (lam1 * lam1 * inv_eps + eps);
-  const T al5 = fj_abs(lam5) >= eps ? fj_abs(lam5) : T(0.5) * (lam5 * lam5 * inv_eps + eps);
+  T al1 = fj_abs(lam1), al5 = fj_abs(lam5);
+  if constexpr (sizeof(T) == 8) {
+    // Harten's fix (flux/roe.py:45-52) only where |lambda| < eps: the FP64
+    // reciprocal of eps is taken only then
+    if (al1 < eps || al5 < eps) {
+      const T inv_eps = M::rcp(eps);
+      if (al1 < eps) al1 = T(0.5) * (lam1 * lam1 * inv_eps + eps);
+      if (al5 < eps) al5 = T(0.5) * (lam5 * lam5 * inv_eps + eps);
+    }
+  } else {
+    const T inv_eps = M::rcp(eps);
+    al1 = al1 >= eps ? al1 : T(0.5) * (lam1 * lam1 * inv_eps + eps);
+    al5 = al5 >= eps ? al5 : T(0.5) * (lam5 * lam5 * inv_eps + eps);
+  }
   const T al2 = fj_abs(un_h);
 
   const T d0 = R.rho - L.rho;

@@ -155,7 +155,8 @@ __device__ __forceinline__ void prefetch_assembly(const Dev& d, int cta, int fla
   if (FIELD) {
     if (flags & kRhsInvscd) {
       l2_prefetch(B.vol + c0, n * 8);
-      for (int v = 0; v < 15; ++v) l2_prefetch((const T*)B.F + v * N + c0, n * (int64_t)sizeof(T));
+      // the i and j faces (the assembly evaluates the k faces itself)
+      for (int v = 0; v < 10; ++v) l2_prefetch((const T*)B.F + v * N + c0, n * (int64_t)sizeof(T));
     }
     if (flags & kRhsViscous) {
       for (int lm = 0; lm < 9; ++lm) l2_prefetch(B.kxyz + lm * N + c0, n * 8);
@@ -798,27 +799,58 @@ __global__ void __launch_bounds__(kSplitThreads, 2) k_fm_fluxes(const Table tab,
 #pragma unroll
       for (int v = 0; v < 5; ++v) F[(5 + v) * N + c] = Fo[v];
     }
-    if (x.k >= 1 && x.k <= x.nk - 3) {
-      const Cell6<T> K2 = load_cell<T, false>(P, N, c + 2);
-      metric_row<T>(B, N, 2, c, kc);
-      metric_row<T>(B, N, 2, c + 1, kn);
-      face_from_cells<T>(Km, C0, Kp, K2, kc, kn, ph, Fo);
-#pragma unroll
-      for (int v = 0; v < 5; ++v) F[(10 + v) * N + c] = Fo[v];
-    }
+    // the k faces are evaluated in the assembly (this kernel is bound by the
+    // FP64 pipe, the assembly by memory latency)
   }
 }
 
+// The k face c-1 | c (rhs/invscd.py:62-100) of the FP64 path from the
+// primitive records of c-2 .. c+1 and the k rows of kxyz at c-1 and c.
 template <typename T>
-__global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table tab, const int flags,
+__device__ __forceinline__ void fm_k_face_left(const SplitBlock& B, int32_t N, int32_t c, const Phys& ph, T F[5]) {
+  const T* __restrict__ P = (const T*)B.prim;
+  const Cell6<T> a0 = load_cell<T, false>(P, N, c - 2), a1 = load_cell<T, false>(P, N, c - 1),
+                 a2 = load_cell<T, false>(P, N, c), a3 = load_cell<T, false>(P, N, c + 1);
+  T kl[3], kr[3];
+  metric_row<T>(B, N, 2, c - 1, kl);
+  metric_row<T>(B, N, 2, c, kr);
+  face_from_cells<T>(a0, a1, a2, a3, kl, kr, ph, F);
+}
+
+// Each warp assembles 31 consecutive cells; lane l evaluates the k face on the
+// left of its cell and takes the one on its right from lane l+1 by shuffle
+// (lane 31's cell is the next warp's first, for which it only supplies the
+// face), as in the FP32 assembly.
+template <typename T>
+__global__ void __launch_bounds__(kSplitThreads, 3) k_fm_assemble(const Table tab, const int flags,
                                                                  const int stage, const int next_prims,
                                                                  const double gm1, const double R,
-                                                                 const double iR) {
-  const int b = find_block(tab, blockIdx.x);
+                                                                 const double iR, const Phys ph) {
+  const int b = find_block_asm(tab, blockIdx.x);
+  const Dev& dv = tab.b[b];
+  const SplitBlock& B = dv.blk;
+  if (threadIdx.x == 0) prefetch_assembly<T, false, true>(dv, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Cell x;
-  if (threadIdx.x == 0) prefetch_assembly<T, false, true>(tab.b[b], blockIdx.x, flags, stage);
-  if (!decode(tab.b[b], blockIdx.x, x)) return;
-  const SplitBlock& B = tab.b[b].blk;
+  x.N = (int64_t)B.ni * B.nj * B.nk;
+  x.c = (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells + warp * 31 + lane;
+  const bool alive = x.c < x.N;
+  if (alive) {
+    const uint32_t t1 = dv.dk.div((uint32_t)x.c);
+    x.k = (int)((uint32_t)x.c - t1 * (uint32_t)B.nk);
+    x.i = (int)dv.dj.div(t1);
+    x.j = (int)(t1 - (uint32_t)x.i * (uint32_t)B.nj);
+    x.ni = B.ni;
+    x.nj = B.nj;
+    x.nk = B.nk;
+  }
+  T fl[5] = {T(0), T(0), T(0), T(0), T(0)}, fr[5];
+  // face c-1 | c exists for k-1 in [1, nk-3]
+  if ((flags & kRhsInvscd) && alive && x.k >= 2 && x.k <= x.nk - 2)
+    fm_k_face_left<T>(B, (int32_t)x.N, (int32_t)x.c, ph, fl);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) fr[v] = __shfl_down_sync(0xffffffffu, fl[v], 1);
+  if (lane == 31 || !alive) return;
   const int64_t N = x.N, c = x.c;
   const int64_t si = (int64_t)x.nj * x.nk, sj = x.nk;
   const int n[3] = {x.ni, x.nj, x.nk};
@@ -838,16 +870,24 @@ __global__ void __launch_bounds__(kSplitThreads, 4) k_fm_assemble(const Table ta
 #pragma unroll
         for (int a = 0; a < 3; ++a)
           if (on[a]) {
-            const T* Fa = F + (int64_t)(a * 5 + v) * N;
-            dsum += (double)(Fa[c] - Fa[c - st[a]]);
+            if (a == 2) {
+              dsum += (double)(fr[v] - fl[v]);
+            } else {
+              const T* Fa = F + (int64_t)(a * 5 + v) * N;
+              dsum += (double)(Fa[c] - Fa[c - st[a]]);
+            }
           }
       } else {
         T s = T(0);
 #pragma unroll
         for (int a = 0; a < 3; ++a)
           if (on[a]) {
-            const T* Fa = F + (int64_t)(a * 5 + v) * N;
-            s += Fa[c] - Fa[c - st[a]];
+            if (a == 2) {
+              s += fr[v] - fl[v];
+            } else {
+              const T* Fa = F + (int64_t)(a * 5 + v) * N;
+              s += Fa[c] - Fa[c - st[a]];
+            }
           }
         dsum = (double)s;
       }
@@ -1009,8 +1049,8 @@ int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int fla
     if (!prims_ready) fm::k_fm_prims<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, 1.0 / ph.R);
     fm::k_fm_fluxes<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
     if (after_fluxes) cudaEventRecord(after_fluxes, st);
-    fm::k_fm_assemble<double><<<ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
-                                                                1.0 / ph.R);
+    fm::k_fm_assemble<double><<<asm_ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
+                                                                    1.0 / ph.R, ph);
   } else {
     if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, 1.0 / ph.R,
                                                                        K_AOS ? ph.p_ref : 0.0);

@@ -5,11 +5,13 @@
 // no intermediate in global memory.
 //
 // Work-list.  A tile is TJ = 8 rows (j) x TK = 30 columns (k) of one block;
-// a work unit is one i-plane of one tile.  The units of all blocks form one
-// list (block by block, tile by tile, plane by plane) and each CTA of the
-// persistent grid takes an equal contiguous range of it, i.e. one or more
-// runs of consecutive planes ("segments") of one or two tiles.  A CTA streams
-// along i through each segment.
+// a work item is one segment of consecutive i-planes of one tile (segments
+// of 24..48 planes when that gives the grid several items per CTA, else the
+// whole i extent).  Items are ordered segment-slowest (segment, block, tile),
+// and the CTAs of the persistent grid (two per SM) take them in that order
+// from a work counter, so the CTAs busy at one time hold neighbouring tiles of
+// the same plane range and share their halo rows in L2.  A CTA streams along
+// i through each segment.
 //
 // Shared memory (one CTA, 8 warps; warp w owns row j0 + w, lane l column
 // k0 - 1 + l, so lanes 1..30 are the tile's columns and lanes 0 and 31 its
@@ -44,6 +46,11 @@
 // is muscl2.py:18-37 (limiter arguments in the reference's order); each slope
 // is evaluated once per cell and axis instead of once per face side.
 //
+// The global data a plane needs beyond the TMA box (stage input, start state,
+// volumes, metric records) is fetched into L2 three planes ahead by the lanes
+// of warp 0 (cp.async.bulk.prefetch.L2), so the assembly's loads do not wait
+// for DRAM.
+//
 // Bounded waits: every mbarrier wait gives up after a limit; a CTA whose wait
 // gave up sets the error word, stops issuing loads and computing, waits for
 // its copies in flight and exits.
@@ -75,7 +82,7 @@ constexpr int SSLOT = 5 * GR * GC;
 constexpr int FR = TJ + 1;
 constexpr int FSLOT = 5 * FR * GC;
 constexpr int kSmemFloats = RS * PSLOT_STRIDE + 4 * GSLOT + 2 * SSLOT + 2 * FSLOT;
-constexpr size_t kSmemBytes = (size_t)kSmemFloats * 4 + RS * 8 + 16 + 128;
+constexpr size_t kSmemBytes = (size_t)kSmemFloats * 4 + RS * 8 + 16 + 128;  // + mbarriers, flags, alignment
 constexpr int kDefaultWaitLimit = 1 << 22;
 constexpr int kDrainWaitLimit = 1 << 26;
 static_assert(PSLOT <= PSLOT_STRIDE, "slot pitch");
@@ -85,9 +92,12 @@ struct __align__(64) TileParams {
   CUtensorMap map[kTileMaxBlocks];
   TileBlock blk[kTileMaxBlocks];
   Phys ph;
-  int64_t units;
   int* err;
+  int* next;            // work counter (zeroed before the launch)
   int nb, stage, wait_limit;
+  int seg_len;          // planes per segment
+  int max_seg;          // segments of the block with the most planes
+  int items;            // work items: (segment, block, tile) with the segment slowest
 };
 static_assert(sizeof(TileParams) <= 32764, "kernel parameter space");
 
@@ -242,6 +252,35 @@ __device__ __forceinline__ void ld_row(const float* __restrict__ rec, int l, flo
   k[2] = __ldg(rec + 3 * l + 2);
 }
 
+__device__ __forceinline__ void l2_fetch(const void* p, int64_t n) { l2_prefetch(p, n); }
+
+// L2 fills of what plane x of the tile will read from global memory: the
+// stage input, the step's start state and the volumes of its rows, and the
+// metric records of its rows with their j / k ring (warp 0, one range per
+// lane at a time).
+__device__ __forceinline__ void prefetch_plane(const TileBlock& B, int x, int j0, int k0, int nrows, int ncols,
+                                               bool state, bool with_q0, int lane) {
+  const int nj = B.nj, nk = B.nk;
+  const int64_t N = (int64_t)B.ni * nj * nk;
+  const int nq = state ? nrows * (with_q0 ? 11 : 6) : 0;  // 5 q (+ 5 q0) + vol per row
+  const int nm = nrows + 2;                               // metric rows j0-1 .. j0+nrows
+  const int xm = x < 0 ? x + B.ni : (x >= B.ni ? x - B.ni : x);
+  for (int t = lane; t < nq + nm; t += 32) {
+    if (t < nq) {
+      const int row = t % nrows, a = t / nrows;  // a: 0..4 q, 5 vol, 6..10 q0
+      const int64_t c = ((int64_t)x * nj + (int64_t)(j0 + row)) * nk + k0;
+      if (a < 5) l2_fetch(B.q + a * N + c, (int64_t)ncols * 8);
+      else if (a == 5) l2_fetch(B.vol + c, (int64_t)ncols * 8);
+      else l2_fetch(B.q0 + (a - 6) * N + c, (int64_t)ncols * 8);
+    } else {
+      int rr = j0 - 1 + (t - nq);
+      rr = rr < 0 ? rr + nj : (rr >= nj ? rr - nj : rr);
+      const int ka = max(k0 - 1, 0), kb = min(k0 + ncols + 1, nk);
+      l2_fetch(B.kaos + (((int64_t)xm * nj + rr) * nk + ka) * 12, (int64_t)(kb - ka) * 48);
+    }
+  }
+}
+
 // The primitives (rho, u, v, w, p - p_ref) of cell (i, j, k) into the padded
 // array and its periodic images (physics/eos.py:12-17 in FP64, then FP32).
 __device__ __forceinline__ void write_prims(float* __restrict__ dst, const TileBlock& B, int i, int j, int k,
@@ -320,27 +359,40 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
   uint32_t used = 0;   // per slot (thread 0): a load was ever issued
   bool stop = false;
 
-  const int64_t U = P.units;
-  const int64_t u_end = U * (blockIdx.x + 1) / gridDim.x;
-  int64_t u = U * blockIdx.x / gridDim.x;
-  while (u < u_end && !stop) {
-    int b = 0;
+  int* const item_sh = fail + 1;
+  while (!stop) {
+    // ---- next work item (segment, block, tile), segment slowest, so that the
+    // CTAs busy at one time hold neighbouring tiles of the same plane range
+    // and their halo rows meet in L2
+    __syncthreads();  // the previous segment's readers of G / Fj and item_sh are done
+    if (tid == 0) *item_sh = atomicAdd(P.next, 1);
+    __syncthreads();
+    const int item = *item_sh;
+    if (item >= P.items) break;
+    // blocks hold contiguous item ranges per segment: unit_begin is the block's
+    // first item within a segment's range, ntj * ntk its tile count
+    int seg = 0, b = 0, tile = 0;
     {
-      int lo = 0, hi = P.nb - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (P.blk[mid].unit_begin <= u) lo = mid;
-        else hi = mid - 1;
+      int rem = item;
+      for (seg = 0; seg < P.max_seg; ++seg) {
+        int cnt = 0;
+        for (int t = 0; t < P.nb; ++t)
+          if (seg * P.seg_len < P.blk[t].ni) cnt += P.blk[t].ntj * P.blk[t].ntk;
+        if (rem < cnt) break;
+        rem -= cnt;
       }
-      b = lo;
+      for (b = 0; b < P.nb; ++b) {
+        if (seg * P.seg_len >= P.blk[b].ni) continue;
+        const int cnt = P.blk[b].ntj * P.blk[b].ntk;
+        if (rem < cnt) break;
+        rem -= cnt;
+      }
+      tile = rem;
     }
     const TileBlock& B = P.blk[b];
     const CUtensorMap* map = &P.map[b];
-    const int64_t loc = u - B.unit_begin;
-    const int tile = (int)(loc / B.ni);
-    const int ib = (int)(loc - (int64_t)tile * B.ni);
-    const int ie = (int)min((int64_t)B.ni, (int64_t)ib + (u_end - u));
-    u += ie - ib;
+    const int ib = seg * P.seg_len;
+    const int ie = min(B.ni, ib + P.seg_len);
     const int ni = B.ni, nj = B.nj, nk = B.nk;
     const int jt = tile / B.ntk, kt = tile - jt * B.ntk;
     const int j0 = jt * TJ, k0 = kt * TK;
@@ -356,8 +408,14 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
     const int64_t N = (int64_t)ni * nj * nk;
     const float mu0 = (float)B.mu0;
     const double dt = B.dt;
+    // metric record of (plane x, own row, column kc): krow + x * kplane
+    const int64_t kplane = (int64_t)nj * nk * 12;
+    const float* const krow = B.kaos + ((int64_t)min(r, nj - 1) * nk + kc) * 12;
 
-    __syncthreads();  // the previous segment's readers of G / Fj are done
+    if (w == 0) {
+      for (int x = ib - 1; x <= min(ib + 1, ie - 1); ++x)
+        prefetch_plane(B, x, j0, k0, nrows, ncols, x >= ib, stage >= 2, l);
+    }
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       for (int x = ib - 2; x <= min(ib + 1, ie + 1); ++x) {
@@ -392,12 +450,17 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
       const float* const Sjc = Sj + (p & 1) * SSLOT;          // j-slopes of plane p
       float* const Fjc = Fj + (p & 1) * FSLOT;                // j-faces of plane p
 
+      // own metric records of planes p and p+1 (rows 0, 1, 2: the face
+      // normals; p+1: also G(p+1))
+      float kp[12], kn[12];
+      if (row_ok) {
+        ld_rec12(krow + pw * kplane, kp);
+        ld_rec12(krow + pw1 * kplane, kn);
+      }
       // ---- A1: G(p+1) on the own row, every lane (lanes 0 / 31: k-halo) ----
       if (row_ok) {
-        float kk[12];
-        ld_rec12(B.kaos + (((int64_t)pw1 * nj + r) * nk + kc) * 12, kk);
         float Gv[9];
-        visc_flux(S0, S1, S2, by0, bx0, kk, mu0, C, Gv);
+        visc_flux(S0, S1, S2, by0, bx0, kn, mu0, C, Gv);
 #pragma unroll
         for (int c = 0; c < 9; ++c) Gn[(c * GR + w + 1) * GC + l] = Gv[c];
       }
@@ -405,8 +468,7 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
       if (full && row_ok) {
         const F5 c = ldP(S0, by0, bx0), m = ldP(S0, by0, bx0 - 1), pp = ldP(S0, by0, bx0 + 1);
         const F5 sk = slope(m, c, pp, C.limiter);
-        float kr[3], kl[3];
-        ld_row(B.kaos + (((int64_t)pw * nj + r) * nk + kc) * 12, 2, kr);
+        float kr[3] = {kp[6], kp[7], kp[8]}, kl[3];
         F5 skm;
 #pragma unroll
         for (int f = 0; f < NF; ++f) skm.v[f] = __shfl_up_sync(0xffffffffu, sk.v[f], 1);
@@ -431,9 +493,9 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
           sL.v[f] = Sjc[(f * GR + w + 1) * GC + l];
           sR.v[f] = Sjc[(f * GR + w + 2) * GC + l];
         }
-        float kl[3], kr[3];
-        ld_row(B.kaos + (((int64_t)pw * nj + r) * nk + k) * 12, 1, kl);
-        ld_row(B.kaos + (((int64_t)pw * nj + r + 1) * nk + k) * 12, 1, kr);
+        const float kl[3] = {kp[3], kp[4], kp[5]};
+        float kr[3];
+        ld_row(krow + pw * kplane + nk * 12, 1, kr);
         float F[5];
         face_flux(ldP(S0, by0, bx0), sL, ldP(S0, by0 + 1, bx0), sR, kl, kr, C, F);
 #pragma unroll
@@ -450,9 +512,7 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
         }
         // face (p | p+1) exists for p in [1, ni-3]
         if (pre1 && p >= 1 && p <= ni - 3) {
-          float kl[3], kr[3];
-          ld_row(B.kaos + (((int64_t)p * nj + r) * nk + k) * 12, 0, kl);
-          ld_row(B.kaos + (((int64_t)(p + 1) * nj + r) * nk + k) * 12, 0, kr);
+          const float kl[3] = {kp[0], kp[1], kp[2]}, kr[3] = {kn[0], kn[1], kn[2]};
           face_flux(a0, si, a1, sn, kl, kr, C, Fip);
         }
         si = sn;
@@ -513,6 +573,8 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
         ipar ^= 1u << s;
         used |= 1u << s;
       }
+      // ---- L2 fills for plane p+3 (read by A(p+2) and B(p+3)) --------------
+      if (w == 0 && p + 3 <= ie) prefetch_plane(B, p + 3, j0, k0, nrows, ncols, p + 3 < ie, stage >= 2, l);
 
       if (full) {
         // ---- B(p): assembly of plane p -------------------------------------
@@ -530,7 +592,7 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
           }
           const double vol = B.vol[c];
           float kk[12];
-          ld_rec12(B.kaos + c * 12, kk);
+          ld_rec12(krow + pw * kplane, kk);
           double rv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
           const bool on_i = p >= 2 && p <= ni - 3, on_j = r >= 2 && r <= nj - 3, on_k = k >= 2 && k <= nk - 3;
           if (on_i || on_j || on_k) {
@@ -644,7 +706,7 @@ bool tile_setup(const fj_block* blocks, int nblocks, void* scratch, TileMaps& tm
   }
   // the error word lives apart from the scratch, which the halo fill reuses
   if (!tm.err) {
-    if (cudaMalloc(&tm.err, sizeof(int)) != cudaSuccess) {
+    if (cudaMalloc(&tm.err, 2 * sizeof(int)) != cudaSuccess) {
       cudaGetLastError();
       tm.err = nullptr;
       return false;
@@ -702,7 +764,8 @@ int tile_stage(fj_ctx* ctx, const TileMaps& tm, int which, TileBlock* blocks, in
     TileParams* prm = new (std::nothrow) TileParams();
     if (!prm) return FJ_ERR_NO_MEMORY;
     prm->nb = std::min(kTileMaxBlocks, nblocks - base);
-    int64_t units = 0;
+    int64_t tiles = 0;
+    int max_ni = 0;
     for (int t = 0; t < prm->nb; ++t) {
       TileBlock& B = prm->blk[t];
       B = blocks[base + t];
@@ -710,22 +773,38 @@ int tile_stage(fj_ctx* ctx, const TileMaps& tm, int which, TileBlock* blocks, in
       B.nkp = tile_nkp(B.nk);
       B.ntj = (B.nj + TJ - 1) / TJ;
       B.ntk = (B.nk + TK - 1) / TK;
-      B.unit_begin = units;
       B.prim_next = stage < 3 ? tm.prim[1 - which][base + t] : nullptr;
-      units += (int64_t)B.ntj * B.ntk * B.ni;
+      tiles += (int64_t)B.ntj * B.ntk;
+      max_ni = std::max(max_ni, B.ni);
       std::memcpy(&prm->map[t], tm.map[which][base + t].data(), sizeof(CUtensorMap));
     }
+    // persistent grid of two CTAs per SM; segments of about 24..48 planes,
+    // fewer (longer) when that already gives every CTA several items
+    const int grid_max = 2 * num_sms();
+    int seg = max_ni;
+    while (seg > 24 && tiles * ((max_ni + seg - 1) / seg) < 4 * (int64_t)grid_max) seg = (seg + 1) / 2;
+    int64_t items = 0;
+    const int max_seg = (max_ni + seg - 1) / seg;
+    for (int t = 0; t < prm->nb; ++t)
+      items += (int64_t)prm->blk[t].ntj * prm->blk[t].ntk * ((prm->blk[t].ni + seg - 1) / seg);
     prm->ph = ph;
-    prm->units = units;
     prm->err = tm.err;
+    prm->next = tm.err + 1;
     prm->stage = stage;
     prm->wait_limit = wait_limit < 0 ? kDefaultWaitLimit : wait_limit;
-    // persistent grid: two CTAs per SM, at least ~16 planes per CTA
-    const int64_t g = std::min<int64_t>(2 * (int64_t)num_sms(), std::max<int64_t>(1, units / 16));
+    prm->seg_len = seg;
+    prm->max_seg = max_seg;
+    prm->items = (int)items;
+    const int64_t g = std::min<int64_t>(grid_max, std::max<int64_t>(1, items));
+    int s = cuda_status(ctx, cudaMemsetAsync(prm->next, 0, sizeof(int), st), "tile work counter");
+    if (s != FJ_OK) {
+      delete prm;
+      return s;
+    }
     k_tile_stage<<<(int)g, NT, kSmemBytes, st>>>(*prm);
     delete prm;
     ctx->launches += 1;
-    int s = launch_status(ctx, "tile stage launch");
+    s = launch_status(ctx, "tile stage launch");
     if (s != FJ_OK) return s;
   }
   return FJ_OK;

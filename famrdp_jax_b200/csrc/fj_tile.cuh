@@ -1,6 +1,6 @@
 // fj_tile.cuh -- the fused TMA-tile stage kernel (fj_stage_tile.cu): one
 // TVD-RK3 stage of all blocks (FP32 fluxes, FP64 state) in one persistent
-// launch over a work-list of (tile, i-plane) units.
+// launch over a work-list of (tile, i-plane segment) items.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -41,7 +41,6 @@ struct TileBlock {
   double mu0, dt;
   int ni, nj, nk, njp, nkp;
   int ntj, ntk;         // tiles along j and k
-  int64_t unit_begin;   // first work unit of this block (units: tile x plane)
 };
 
 // Host-side plan data of the tile path: one TMA descriptor per block and
