@@ -25,9 +25,8 @@ struct SplitBlock {
   const double* vol;     // (ni, nj, nk)
   void* prim;            // scratch: the primitives of the stage input (records in FP32)
   void* prim_next;       // where the assembly writes the next stage's primitives: a
-                         // second buffer in FP32 (the FP32 assembly also reads prim),
-                         // prim itself in FP64
-  void* F;               // scratch: FP64 15 x N (face c | c+e_a, axis-major); FP32 records of
+                         // second buffer (the assembly also reads prim: its k faces)
+  void* F;               // scratch: FP64 10 x N (face c | c+e_a for a = i, j, axis-major); FP32 records of
                          // the i face and the first three j-face components (8 per cell)
   void* Fz;              // FP32 only: the last two j-face components, two per cell
   void* G;               // scratch: viscous flux components (records: 8 per cell)

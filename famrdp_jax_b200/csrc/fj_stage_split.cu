@@ -646,7 +646,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
 
 // ---- field-major variant (the FP64 path) ----------------------------------
 // The FP64 path keeps its primitives as 48-byte records (three 16-byte loads
-// per neighbour) and its face and viscous fluxes field-major (15 + 9 arrays of
+// per neighbour) and its face and viscous fluxes field-major (10 + 9 arrays of
 // N): flux records would cost FP64 more registers (two doubles per vector
 // lane) and padding bytes than the index arithmetic they save.
 namespace fm {
@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(kSplitThreads, 3) k_fm_assemble(const Table ta
       T rec[kRecP64];
 #pragma unroll
       for (int v = 0; v < kRecP64; ++v) rec[v] = (T)pv[v];
-      st_rec<T, kRecP64>((T*)B.prim + c * kRecP64, rec);
+      st_rec<T, kRecP64>((T*)B.prim_next + c * kRecP64, rec);
     }
   }
 }
@@ -1028,7 +1028,7 @@ __global__ void k_fold_sum(const double* __restrict__ part, int n, double* __res
 struct SplitShape {
   int flux_occ, asm_occ;
 };
-constexpr SplitShape kSplitVariants[] = {{4, 4}, {3, 4}, {3, 6}, {3, 5}, {4, 6}, {3, 8}};
+constexpr SplitShape kSplitVariants[] = {{4, 4}, {3, 4}, {3, 6}, {3, 5}, {4, 3}, {2, 4}};
 static_assert(sizeof(kSplitVariants) / sizeof(kSplitVariants[0]) == FJ_NUM_SPLIT_VARIANTS, "variant table");
 
 template <typename T, bool K_AOS, int V>
@@ -1147,8 +1147,10 @@ size_t split_metric_record_bytes(int precision, int64_t N) {
 // arrays (FP64).
 static void split_counts(int precision, int& nP, int& nF, int& nG) {
   const bool rec = precision == FJ_PREC_F32FLUX;
-  nP = rec ? 2 * kRecP : kRecP64;  // FP32: the stage input's primitives and the next stage's
-  nF = rec ? kRecFA + kRecFB : 15;
+  // the stage input's primitives and the next stage's: the assembly reads the
+  // first (its k faces) while writing the second
+  nP = rec ? 2 * kRecP : 2 * kRecP64;
+  nF = rec ? kRecFA + kRecFB : 10;  // FP64: the i and j faces, field-major (the k faces stay in the assembly)
   nG = 9;  // records: kRecG per cell in G, then one per cell in Gz
 }
 
@@ -1173,9 +1175,10 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
   int64_t off = 0;
   for (int b = 0; b < nblocks; ++b) {
     const int64_t N = (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
-    // records are multiples of 16 bytes; FP32: [input | next] primitive records
-    blocks[b].prim = prim + (precision == FJ_PREC_F32FLUX ? kRecP : nP) * off * t;
-    blocks[b].prim_next = precision == FJ_PREC_F32FLUX ? prim + (kRecP * total + kRecP * off) * t : blocks[b].prim;
+    // records are multiples of 16 bytes: [input | next] primitive records
+    const int rp = precision == FJ_PREC_F32FLUX ? kRecP : kRecP64;
+    blocks[b].prim = prim + rp * off * t;
+    blocks[b].prim_next = prim + (rp * total + rp * off) * t;
     if (precision == FJ_PREC_F32FLUX) {
       blocks[b].F = F + kRecFA * off * t;
       blocks[b].Fz = F + (kRecFA * total + kRecFB * off) * t;

@@ -46,11 +46,6 @@
 // is muscl2.py:18-37 (limiter arguments in the reference's order); each slope
 // is evaluated once per cell and axis instead of once per face side.
 //
-// The global data a plane needs beyond the TMA box (stage input, start state,
-// volumes, metric records) is fetched into L2 three planes ahead by the lanes
-// of warp 0 (cp.async.bulk.prefetch.L2), so the assembly's loads do not wait
-// for DRAM.
-//
 // Bounded waits: every mbarrier wait gives up after a limit; a CTA whose wait
 // gave up sets the error word, stops issuing loads and computing, waits for
 // its copies in flight and exits.
@@ -252,35 +247,6 @@ __device__ __forceinline__ void ld_row(const float* __restrict__ rec, int l, flo
   k[2] = __ldg(rec + 3 * l + 2);
 }
 
-__device__ __forceinline__ void l2_fetch(const void* p, int64_t n) { l2_prefetch(p, n); }
-
-// L2 fills of what plane x of the tile will read from global memory: the
-// stage input, the step's start state and the volumes of its rows, and the
-// metric records of its rows with their j / k ring (warp 0, one range per
-// lane at a time).
-__device__ __forceinline__ void prefetch_plane(const TileBlock& B, int x, int j0, int k0, int nrows, int ncols,
-                                               bool state, bool with_q0, int lane) {
-  const int nj = B.nj, nk = B.nk;
-  const int64_t N = (int64_t)B.ni * nj * nk;
-  const int nq = state ? nrows * (with_q0 ? 11 : 6) : 0;  // 5 q (+ 5 q0) + vol per row
-  const int nm = nrows + 2;                               // metric rows j0-1 .. j0+nrows
-  const int xm = x < 0 ? x + B.ni : (x >= B.ni ? x - B.ni : x);
-  for (int t = lane; t < nq + nm; t += 32) {
-    if (t < nq) {
-      const int row = t % nrows, a = t / nrows;  // a: 0..4 q, 5 vol, 6..10 q0
-      const int64_t c = ((int64_t)x * nj + (int64_t)(j0 + row)) * nk + k0;
-      if (a < 5) l2_fetch(B.q + a * N + c, (int64_t)ncols * 8);
-      else if (a == 5) l2_fetch(B.vol + c, (int64_t)ncols * 8);
-      else l2_fetch(B.q0 + (a - 6) * N + c, (int64_t)ncols * 8);
-    } else {
-      int rr = j0 - 1 + (t - nq);
-      rr = rr < 0 ? rr + nj : (rr >= nj ? rr - nj : rr);
-      const int ka = max(k0 - 1, 0), kb = min(k0 + ncols + 1, nk);
-      l2_fetch(B.kaos + (((int64_t)xm * nj + rr) * nk + ka) * 12, (int64_t)(kb - ka) * 48);
-    }
-  }
-}
-
 // The primitives (rho, u, v, w, p - p_ref) of cell (i, j, k) into the padded
 // array and its periodic images (physics/eos.py:12-17 in FP64, then FP32).
 __device__ __forceinline__ void write_prims(float* __restrict__ dst, const TileBlock& B, int i, int j, int k,
@@ -412,10 +378,6 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
     const int64_t kplane = (int64_t)nj * nk * 12;
     const float* const krow = B.kaos + ((int64_t)min(r, nj - 1) * nk + kc) * 12;
 
-    if (w == 0) {
-      for (int x = ib - 1; x <= min(ib + 1, ie - 1); ++x)
-        prefetch_plane(B, x, j0, k0, nrows, ncols, x >= ib, stage >= 2, l);
-    }
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       for (int x = ib - 2; x <= min(ib + 1, ie + 1); ++x) {
@@ -573,8 +535,7 @@ __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ Ti
         ipar ^= 1u << s;
         used |= 1u << s;
       }
-      // ---- L2 fills for plane p+3 (read by A(p+2) and B(p+3)) --------------
-      if (w == 0 && p + 3 <= ie) prefetch_plane(B, p + 3, j0, k0, nrows, ncols, p + 3 < ie, stage >= 2, l);
+
 
       if (full) {
         // ---- B(p): assembly of plane p -------------------------------------

@@ -530,7 +530,9 @@ def test_autotune_launch_shapes_agree(cuda_device):
             assert torch.equal(a, b)
     chosen, ms = plan.autotune(qs, [torch.empty_like(q) for q in qs], dt, reps=2)
     n = _capi.NUM_SPLIT_VARIANTS
-    assert 0 <= chosen < 2 * n and len(ms) == 2 * n and min(ms) > 0
+    # candidates: every split shape at one and two streams, then the tile kernel
+    assert 0 <= chosen <= 2 * n and len(ms) == 2 * n + 1 and min(ms) > 0
+    assert plan.kernel == ("tile" if chosen == 2 * n else "split")
 
 
 def test_plan_argument_errors(cuda_device):
