@@ -7,6 +7,7 @@
 #include <stdio.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "famrdp_cuda.h"
@@ -177,6 +178,31 @@ inline Phys make_phys(const fj_params* p) {
   f.limiter = p->limiter;
   f.visc_law = p->visc_law;
   return f;
+}
+
+// Programmatic dependent launch.  A kernel launched with pdl_launch may be
+// scheduled while the previous kernel on its stream drains; it calls
+// grid_dep_wait() before its first load or store of data another kernel
+// writes (L2 prefetches may come first: L2 is coherent with the writes still
+// in flight), which blocks until the previous grid has completed and its
+// writes are visible.  Only the launch latency overlaps; without the launch
+// attribute the wait returns at once.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... Exp, typename... Act>
+inline cudaError_t pdl_launch(void (*k)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Act&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
 }
 
 // Starts an L2 fill of the bytes [p, p + n) of one contiguous range, clipped

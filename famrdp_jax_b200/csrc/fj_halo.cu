@@ -72,6 +72,7 @@ __device__ __forceinline__ int64_t cell_index(const int n[3], int i, int j, int 
 }
 
 __global__ void k_halo_gather(const HaloTable tab, double* __restrict__ scratch) {
+  grid_dep_wait();
   const HaloDesc& d = tab.d[blockIdx.y];
   const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
   const int64_t NS = (int64_t)d.sn[0] * d.sn[1] * d.sn[2];
@@ -87,6 +88,7 @@ __global__ void k_halo_gather(const HaloTable tab, double* __restrict__ scratch)
 }
 
 __global__ void k_halo_scatter(const HaloTable tab, const double* __restrict__ scratch) {
+  grid_dep_wait();
   const int L = blockIdx.y;
   const HaloDesc& d = tab.d[L];
   const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
@@ -128,6 +130,7 @@ __device__ __forceinline__ void bc_layers(int face, int n, int g, int o, int& ou
 }
 
 __global__ void k_bc(const BcTable tab, int g) {
+  grid_dep_wait();
   const BcDesc& d = tab.d[blockIdx.y];
   const int ax = d.face >> 1;
   const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;  // the two other axes
@@ -304,9 +307,9 @@ int halo_exchange(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_lin
       }
       dim3 grid((unsigned)std::min<int64_t>(grid_for(pass == 0 ? 5 * vmax : vmax), 4096), tab.n);
       if (pass == 0)
-        k_halo_gather<<<grid, kThreads, 0, st>>>(tab, scratch);
+        pdl_launch(k_halo_gather, grid, kThreads, 0, st, tab, scratch);
       else
-        k_halo_scatter<<<grid, kThreads, 0, st>>>(tab, scratch);
+        pdl_launch(k_halo_scatter, grid, kThreads, 0, st, tab, (const double*)scratch);
       ctx->launches += 1;
       s = launch_status(ctx, "halo launch");
       if (s != FJ_OK) return s;
@@ -355,7 +358,7 @@ int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs,
         vmax = std::max<int64_t>(vmax, area * p->ghost);
       }
       dim3 grid((unsigned)std::min<int64_t>(grid_for(vmax), 4096), tab.n);
-      k_bc<<<grid, kThreads, 0, st>>>(tab, p->ghost);
+      pdl_launch(k_bc, grid, kThreads, 0, st, tab, p->ghost);
       ctx->launches += 1;
       int s = launch_status(ctx, "bc launch");
       if (s != FJ_OK) return s;

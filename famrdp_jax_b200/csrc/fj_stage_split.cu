@@ -307,6 +307,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, 
                                                               const double p_ref) {
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
+  grid_dep_wait();
   const SplitBlock& B = tab.b[b].blk;
   const int32_t N = B.ni * B.nj * B.nk;
   const int32_t c = (blockIdx.x - B.cta_begin) * kSplitThreads + threadIdx.x;
@@ -338,6 +339,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
   using M = FastMath<T>;
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x);
+  grid_dep_wait();
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
@@ -614,6 +616,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
   const Dev& d = tab.b[b];
   const SplitBlock& B = d.blk;
   if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
+  grid_dep_wait();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
   const int64_t c = (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells + warp * 31 + lane;
@@ -656,6 +659,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_fm_prims(const Table tab, con
                                                               const double R, const double iR) {
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
+  grid_dep_wait();
   const SplitBlock& B = tab.b[b].blk;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
   const int64_t c = (int64_t)(blockIdx.x - B.cta_begin) * kSplitThreads + threadIdx.x;
@@ -715,6 +719,7 @@ __global__ void __launch_bounds__(kSplitThreads, 2) k_fm_fluxes(const Table tab,
   using M = FastMath<T>;
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_fluxes<T, false, true>(tab.b[b], blockIdx.x);
+  grid_dep_wait();
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
   const SplitBlock& B = tab.b[b].blk;
@@ -830,6 +835,7 @@ __global__ void __launch_bounds__(kSplitThreads, 3) k_fm_assemble(const Table ta
   const Dev& dv = tab.b[b];
   const SplitBlock& B = dv.blk;
   if (threadIdx.x == 0) prefetch_assembly<T, false, true>(dv, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
+  grid_dep_wait();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Cell x;
   x.N = (int64_t)B.ni * B.nj * B.nk;
@@ -1035,10 +1041,10 @@ template <typename T, bool K_AOS, int V>
 void launch_pair(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, int np,
                  cudaStream_t st, cudaEvent_t after_fluxes) {
   constexpr SplitShape sh = kSplitVariants[V];
-  k_split_fluxes<T, K_AOS, sh.flux_occ><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
+  pdl_launch(k_split_fluxes<T, K_AOS, sh.flux_occ>, ctas, kSplitThreads, 0, st, tab, ph, flags);
   if (after_fluxes) cudaEventRecord(after_fluxes, st);
-  k_split_assemble<T, K_AOS, sh.asm_occ><<<asm_ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1,
-                                                                              ph.R, 1.0 / ph.R, ph);
+  pdl_launch(k_split_assemble<T, K_AOS, sh.asm_occ>, asm_ctas, kSplitThreads, 0, st, tab, flags, stage, np, ph.gm1,
+             ph.R, 1.0 / ph.R, ph);
 }
 
 template <typename T, bool K_AOS>
@@ -1046,14 +1052,14 @@ int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int fla
                bool next_prims, int variant, cudaStream_t st, cudaEvent_t after_fluxes) {
   const int np = next_prims ? 1 : 0;
   if constexpr (sizeof(T) == 8) {
-    if (!prims_ready) fm::k_fm_prims<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, 1.0 / ph.R);
-    fm::k_fm_fluxes<double><<<ctas, kSplitThreads, 0, st>>>(tab, ph, flags);
+    if (!prims_ready) pdl_launch(fm::k_fm_prims<double>, ctas, kSplitThreads, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R);
+    pdl_launch(fm::k_fm_fluxes<double>, ctas, kSplitThreads, 0, st, tab, ph, flags);
     if (after_fluxes) cudaEventRecord(after_fluxes, st);
-    fm::k_fm_assemble<double><<<asm_ctas, kSplitThreads, 0, st>>>(tab, flags, stage, np, ph.gm1, ph.R,
-                                                                    1.0 / ph.R, ph);
+    pdl_launch(fm::k_fm_assemble<double>, asm_ctas, kSplitThreads, 0, st, tab, flags, stage, np, ph.gm1, ph.R,
+               1.0 / ph.R, ph);
   } else {
-    if (!prims_ready) k_split_prims<T><<<ctas, kSplitThreads, 0, st>>>(tab, ph.gm1, ph.R, 1.0 / ph.R,
-                                                                       K_AOS ? ph.p_ref : 0.0);
+    if (!prims_ready)
+      pdl_launch(k_split_prims<T>, ctas, kSplitThreads, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R, K_AOS ? ph.p_ref : 0.0);
     switch (K_AOS ? variant : 0) {
       case 1: launch_pair<T, K_AOS, 1>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
       case 2: launch_pair<T, K_AOS, 2>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;

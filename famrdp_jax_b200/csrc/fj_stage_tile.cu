@@ -274,6 +274,7 @@ __device__ __forceinline__ void write_prims(float* __restrict__ dst, const TileB
 
 __global__ void k_tile_prims(const TileBlock B, const double* __restrict__ q, float* __restrict__ dst, double gm1,
                              double p_ref) {
+  grid_dep_wait();
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= N) return;
@@ -286,6 +287,7 @@ __global__ void k_tile_prims(const TileBlock B, const double* __restrict__ q, fl
 
 __global__ void __launch_bounds__(NT, 2) k_tile_stage(const __grid_constant__ TileParams P) {
   extern __shared__ unsigned char smem_raw[];
+  grid_dep_wait();
   float* const base = (float*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
   float* const Pr = base;
   float* const Gs = Pr + RS * PSLOT_STRIDE;
@@ -713,7 +715,7 @@ int tile_prims(fj_ctx* ctx, const TileMaps& tm, int which, const double* const* 
     B.njp = tile_njp(B.nj);
     B.nkp = tile_nkp(B.nk);
     const int64_t N = (int64_t)B.ni * B.nj * B.nk;
-    k_tile_prims<<<grid_for(N), kThreads, 0, st>>>(B, q[b], tm.prim[which][b], gm1, p_ref);
+    pdl_launch(k_tile_prims, grid_for(N), kThreads, 0, st, B, q[b], tm.prim[which][b], gm1, p_ref);
     ctx->launches += 1;
   }
   return launch_status(ctx, "tile primitive launch");
@@ -762,7 +764,7 @@ int tile_stage(fj_ctx* ctx, const TileMaps& tm, int which, TileBlock* blocks, in
       delete prm;
       return s;
     }
-    k_tile_stage<<<(int)g, NT, kSmemBytes, st>>>(*prm);
+    pdl_launch(k_tile_stage, (int)g, NT, kSmemBytes, st, *prm);
     delete prm;
     ctx->launches += 1;
     s = launch_status(ctx, "tile stage launch");
