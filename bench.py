@@ -72,11 +72,12 @@ UNIT = "Mcell-stages/s"
 STAGE_BYTES = {"f64": 200.0, "f32": 164.0}
 STEP_BYTES = {"f64": 560.0, "f32": 452.0}
 # DRAM bytes per padded cell of one stage-2 launch group (dram__bytes_read +
-# dram__bytes_write summed over the primitive, flux and assembly kernels),
-# measured by ncu on `bench.py --stage-only --n 96` (4 blocks of 100^3 padded
-# cells, 4.0 M) and scaled per cell: FP32 59 + 147 + 283 B, FP64 74 + 301 +
-# 401 B
-STAGE_TRAFFIC = {("f32", "split"): 489.0, ("f64", "split"): 777.0}
+# dram__bytes_write summed over its kernels), measured by ncu on
+# `bench.py --stage-only --n 96` (4 blocks of 100^3 padded cells, 4.0 M) and
+# scaled per cell: split FP32 59 + 147 + 283 B (primitives, fluxes, assembly),
+# split FP64 74 + 301 + 401 B; the fused tile kernel 220 B (its primitive
+# launch not included)
+STAGE_TRAFFIC = {("f32", "split"): 489.0, ("f64", "split"): 777.0, ("f32", "tile"): 220.0}
 
 
 def _peaks():
@@ -308,13 +309,14 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"),
         dt = diagnostics.cfl_dt(st, cfg, c.cfl)
         qa = [st.blocks[0].q.clone()]
         qb = [torch.empty_like(qa[0])]
-        for _ in range(3):
-            plan.run(qa, qb, dt)
+        for _ in range(4):  # also captures the two ping-pong step graphs
+            plan.run(qa, qb, dt, graph=True)
+            qa, qb = qb, qa
 
-        def fwd():
+        def fwd():  # the plain forward, as graph replays (its fastest form)
             a, b = qa, qb
             for _ in range(nsteps):
-                plan.run(a, b, dt)
+                plan.run(a, b, dt, graph=True)
                 a, b = b, a
 
         _, t_fwd = timed(fwd)
@@ -323,6 +325,7 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"),
                            tables=adjoint._Tables(cfg), dmu=torch.zeros(1, dtype=torch.float64, device=device))
         run.buffers([st.blocks[0].q])  # the driver's reusable buffers, outside the timed region
         run.reverse_buffers([st.blocks[0].q])
+        adjoint._forward_with_checkpoints(run, [st.blocks[0].q])  # warm-up: captures the step graphs
         (final, checkpoints), t_ckpt = timed(lambda: adjoint._forward_with_checkpoints(run, [st.blocks[0].q]))
         lams = adjoint.kinetic_energy_grad(final, st.metrics, cfg.ghost)
         g, t_rev = timed(lambda: adjoint._reverse_sweep(run, checkpoints, lams))

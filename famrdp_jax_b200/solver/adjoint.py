@@ -187,7 +187,10 @@ def _forward_segment(run: _Run, qs, nsteps, keep: bool, pool=None):
             run.plan.run_save(cur, nxt, *pool[n], run.dt)
             states.append(pool[n])
         else:
-            run.plan.run(cur, nxt, run.dt)
+            # replayed from the plan's captured graphs: the steps between
+            # checkpoints only ever run ping -> pong, pong -> ping and the
+            # segment's first step, so a few graphs serve the whole sweep
+            run.plan.run(cur, nxt, run.dt, graph=True)
         cur = nxt
     return cur, states
 
