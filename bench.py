@@ -75,9 +75,9 @@ STEP_BYTES = {"f64": 560.0, "f32": 452.0}
 # dram__bytes_write summed over its kernels), measured by ncu on
 # `bench.py --stage-only --n 96` (4 blocks of 100^3 padded cells, 4.0 M) and
 # scaled per cell: split FP32 59 + 147 + 283 B (primitives, fluxes, assembly),
-# split FP64 74 + 301 + 401 B; the fused tile kernel 220 B (its primitive
+# split FP64 75 + 259 + 406 B; the fused tile kernel 220 B (its primitive
 # launch not included)
-STAGE_TRAFFIC = {("f32", "split"): 489.0, ("f64", "split"): 777.0, ("f32", "tile"): 220.0}
+STAGE_TRAFFIC = {("f32", "split"): 489.0, ("f64", "split"): 740.0, ("f32", "tile"): 220.0}
 
 
 def _peaks():
