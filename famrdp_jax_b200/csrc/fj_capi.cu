@@ -774,10 +774,11 @@ int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, dou
   if (!pl || !chosen || reps < 1) return FJ_ERR_INVALID_ARGUMENT;
   fj_ctx* ctx = pl->ctx;
   const bool split = pl->pipeline == FJ_PIPELINE_SPLIT;
-  const bool tunable = split && pl->p.precision == FJ_PREC_F32FLUX;
+  // the launch shapes of the split kernels, in both precisions
+  const bool tunable = split;
   const int nv = tunable ? FJ_NUM_SPLIT_VARIANTS : 1;
   const int ns = split && pl->blocks.size() >= 2 ? 2 : 1;
-  const bool with_tile = tunable && pl->tile != nullptr;
+  const bool with_tile = tunable && pl->p.precision == FJ_PREC_F32FLUX && pl->tile != nullptr;
   if (ms_out)
     for (int i = 0; i < 2 * FJ_NUM_SPLIT_VARIANTS + 1; ++i) ms_out[i] = 0.0;
   cudaStream_t st = S(stream);

@@ -713,9 +713,9 @@ __device__ __forceinline__ void metric_row(const SplitBlock& B, int32_t N, int r
   k[2] = (T)__ldg(K + 2 * N + c);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kSplitThreads, 2) k_fm_fluxes(const Table tab, const Phys ph,
-                                                               const int flags) {
+template <typename T, int OCC = 2>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_fm_fluxes(const Table tab, const Phys ph,
+                                                                 const int flags) {
   using M = FastMath<T>;
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_fluxes<T, false, true>(tab.b[b], blockIdx.x);
@@ -826,8 +826,8 @@ __device__ __forceinline__ void fm_k_face_left(const SplitBlock& B, int32_t N, i
 // left of its cell and takes the one on its right from lane l+1 by shuffle
 // (lane 31's cell is the next warp's first, for which it only supplies the
 // face), as in the FP32 assembly.
-template <typename T>
-__global__ void __launch_bounds__(kSplitThreads, 3) k_fm_assemble(const Table tab, const int flags,
+template <typename T, int OCC = 3>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_fm_assemble(const Table tab, const int flags,
                                                                  const int stage, const int next_prims,
                                                                  const double gm1, const double R,
                                                                  const double iR, const Phys ph) {
@@ -1028,14 +1028,30 @@ __global__ void k_fold_sum(const double* __restrict__ part, int n, double* __res
   if (threadIdx.x == 0) *out = s;
 }
 
-// Launch shapes of the FP32 record kernels, selected per plan by the
-// autotuner (index 0 is the default): the minimum resident CTAs per SM of the
-// flux and assembly kernels, i.e. their register caps.
+// Launch shapes of the split kernels, selected per plan by the autotuner
+// (index 0 is the default): the minimum resident CTAs per SM of the flux and
+// assembly kernels, i.e. their register caps.  These are the FP32 record
+// kernels' shapes; kSplitVariants64 below are the FP64 kernels'.
 struct SplitShape {
   int flux_occ, asm_occ;
 };
 constexpr SplitShape kSplitVariants[] = {{4, 4}, {3, 4}, {3, 6}, {3, 5}, {4, 3}, {2, 4}};
 static_assert(sizeof(kSplitVariants) / sizeof(kSplitVariants[0]) == FJ_NUM_SPLIT_VARIANTS, "variant table");
+
+// Launch shapes of the FP64 field-major kernels (the same variant index; FP64
+// face arithmetic needs more registers at the same occupancy).
+constexpr SplitShape kSplitVariants64[] = {{2, 3}, {2, 4}, {3, 3}, {2, 2}, {3, 4}, {3, 2}};
+static_assert(sizeof(kSplitVariants64) / sizeof(kSplitVariants64[0]) == FJ_NUM_SPLIT_VARIANTS, "variant table");
+
+template <int V>
+void launch_pair64(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, int np,
+                   cudaStream_t st, cudaEvent_t after_fluxes) {
+  constexpr SplitShape sh = kSplitVariants64[V];
+  pdl_launch(fm::k_fm_fluxes<double, sh.flux_occ>, ctas, kSplitThreads, 0, st, tab, ph, flags);
+  if (after_fluxes) cudaEventRecord(after_fluxes, st);
+  pdl_launch(fm::k_fm_assemble<double, sh.asm_occ>, asm_ctas, kSplitThreads, 0, st, tab, flags, stage, np, ph.gm1,
+             ph.R, 1.0 / ph.R, ph);
+}
 
 template <typename T, bool K_AOS, int V>
 void launch_pair(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, int np,
@@ -1053,10 +1069,14 @@ int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int fla
   const int np = next_prims ? 1 : 0;
   if constexpr (sizeof(T) == 8) {
     if (!prims_ready) pdl_launch(fm::k_fm_prims<double>, ctas, kSplitThreads, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R);
-    pdl_launch(fm::k_fm_fluxes<double>, ctas, kSplitThreads, 0, st, tab, ph, flags);
-    if (after_fluxes) cudaEventRecord(after_fluxes, st);
-    pdl_launch(fm::k_fm_assemble<double>, asm_ctas, kSplitThreads, 0, st, tab, flags, stage, np, ph.gm1, ph.R,
-               1.0 / ph.R, ph);
+    switch (variant) {
+      case 1: launch_pair64<1>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 2: launch_pair64<2>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 3: launch_pair64<3>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 4: launch_pair64<4>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      case 5: launch_pair64<5>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
+      default: launch_pair64<0>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes);
+    }
   } else {
     if (!prims_ready)
       pdl_launch(k_split_prims<T>, ctas, kSplitThreads, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R, K_AOS ? ph.p_ref : 0.0);

@@ -270,10 +270,11 @@ int fj_plan_set_ensemble(fj_plan* plan, const double* mu0, const double* dt);
  * the FJ_PLAN_MAX_GRAPHS most recently used graphs (a ping-pong loop uses
  * two). */
 #define FJ_PLAN_MAX_GRAPHS 4
-/* Launch shape of the plan's FP32-flux split kernels: the register caps
- * (minimum resident CTAs per SM) of the flux and assembly kernels, one of
- * FJ_NUM_SPLIT_VARIANTS; 0 is the default.  Changing it drops captured graphs.
- * Results do not depend on it. */
+/* Launch shape of the plan's split kernels (either precision; the shapes
+ * differ between FP32-flux and FP64): the register caps (minimum resident CTAs
+ * per SM) of the flux and assembly kernels, one of FJ_NUM_SPLIT_VARIANTS; 0 is
+ * the default.  Changing it drops captured graphs.  Results do not depend on
+ * it. */
 #define FJ_NUM_SPLIT_VARIANTS 6
 int fj_plan_set_variant(fj_plan* plan, int variant);
 /* Stage kernels of an FP32-flux split plan (no counterpart in the reference,
@@ -307,7 +308,7 @@ int fj_plan_check(fj_plan* plan, int* word, void* stream);
  * launch on one stream.  Results do not depend on it.  Drops captured graphs. */
 int fj_plan_set_streams(fj_plan* plan, int n);
 /* The autotuner: times `reps` steps q_in -> q_out (after one untimed step) for
- * every launch shape (FP32-flux split plans) and stream count (split plans of
+ * every launch shape (split plans, both precisions) and stream count (split plans of
  * two or more blocks) with CUDA events on `stream`, keeps the fastest in the
  * plan and reports it as shape + FJ_NUM_SPLIT_VARIANTS * (streams - 1), or
  * 2 * FJ_NUM_SPLIT_VARIANTS for the tile kernel (FP32-flux plans whose tile

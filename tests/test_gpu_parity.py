@@ -503,15 +503,17 @@ def test_residual_and_monitored_run(cuda_device, tmp_path):
     assert sorted(p.name for p in (tmp_path / "dumps").iterdir()) == ["step0000000_good.pt", "step0000001_bad.pt"]
 
 
-def test_autotune_launch_shapes_agree(cuda_device):
-    """Every launch shape of the FP32-flux split kernels and both stream counts
-    (block groups on two streams, also captured as a graph) give the same step
-    bit for bit; the autotuner keeps one of them."""
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_autotune_launch_shapes_agree(cuda_device, precision):
+    """Every launch shape of the split kernels and both stream counts (block
+    groups on two streams, also captured as a graph) give the same step bit for
+    bit, in both precisions; the autotuner keeps one of them (or, FP32-flux,
+    the tile kernel)."""
     import dataclasses
     from famrdp_jax_b200 import _capi
     from famrdp_jax_b200.solver.step import StepPlan
     c = cases.tree24(nblocks=4, lo=6, hi=12, seed=2)
-    cfg = dataclasses.replace(c.cfg, precision="f32")
+    cfg = dataclasses.replace(c.cfg, precision=precision)
     st = state_from_case(c)
     dt = NP.cfl_dt(c.qs, [(m[1], m[2]) for m in c.metrics], cfg.gas.gamma, c.cfl, 2)
     plan = StepPlan(st, cfg)
@@ -530,8 +532,10 @@ def test_autotune_launch_shapes_agree(cuda_device):
             assert torch.equal(a, b)
     chosen, ms = plan.autotune(qs, [torch.empty_like(q) for q in qs], dt, reps=2)
     n = _capi.NUM_SPLIT_VARIANTS
-    # candidates: every split shape at one and two streams, then the tile kernel
-    assert 0 <= chosen <= 2 * n and len(ms) == 2 * n + 1 and min(ms) > 0
+    # candidates: every split shape at one and two streams, then (FP32-flux) the
+    # tile kernel
+    timed = ms if precision == "f32" else ms[:2 * n]
+    assert 0 <= chosen <= 2 * n and len(ms) == 2 * n + 1 and min(timed) > 0
     assert plan.kernel == ("tile" if chosen == 2 * n else "split")
 
 
