@@ -423,31 +423,44 @@ def _stage_roofline(plan, q0s, dt, prec, padded_cells):
     live (10 launches of the group after 3 warm-ups, CUDA events on the
     launching stream)."""
     import torch
+    kern = plan.kernel
+    # the persistent step has no stage-sized launch: its one launch is the
+    # whole step (halo, boundary faces and three stages), timed as a graph
+    # replay and counted as three stages' algorithmic bytes
+    whole_step = kern == "persistent"
     qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state q0
     outs = [torch.empty_like(q) for q in q0s]
+
+    def launch():
+        if whole_step:
+            plan.run(qin, outs, dt, graph=True)
+        else:
+            plan.stage(qin, q0s, outs, dt, 2)
+
     for _ in range(3):
-        plan.stage(qin, q0s, outs, dt, 2)
+        launch()
     torch.cuda.synchronize()
     reps = 10
     s = torch.cuda.current_stream()
     a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a0.record(s)
     for _ in range(reps):
-        plan.stage(qin, q0s, outs, dt, 2)
+        launch()
     a1.record(s)
     torch.cuda.synchronize()
     stage_ms = a0.elapsed_time(a1) / reps
-    alg = STAGE_BYTES[prec] * padded_cells
+    alg = STAGE_BYTES[prec] * padded_cells * (3 if whole_step else 1)
     peak, peak_kind = _peaks()
     achieved = alg / (stage_ms / 1e3) / 1e9
-    kern = plan.kernel
     traffic = STAGE_TRAFFIC.get((prec, kern))
     del qin, outs
     what = ("one TVD-RK3 stage of all blocks (fused TMA-tile kernel: one persistent launch, plus the launch "
             "that fills the padded primitive planes)" if kern == "tile" else
-            "one TVD-RK3 stage of all blocks (split pipeline: prims, fluxes, assembly; 3 launches)")
+            "one whole TVD-RK3 step of all blocks (persistent kernel: halo, boundary faces, primitives and the "
+            "three stages in one launch after a counter reset; algorithmic bytes of three stages)" if whole_step
+            else "one TVD-RK3 stage of all blocks (split pipeline: prims, fluxes, assembly; 3 launches)")
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic * padded_cells if traffic else None,
+            "traffic": traffic * padded_cells * (3 if whole_step else 1) if traffic else None,
             "traffic_note": f"{traffic:.0f} B per padded cell (ncu dram__bytes_read+write of the stage-2 group on "
                             f"4 x 100^3 padded cells) x the cells of one launch" if traffic else None,
             "kernel": what, "stage_kernel": kern,
@@ -692,8 +705,9 @@ def main(argv=None):
     ap.add_argument("--stage-only", action="store_true",
                     help="only run four standalone stage-2 evaluations (for a profiler)")
     ap.add_argument("--shape", type=int, default=1, help="FP32 launch shape for --stage-only")
-    ap.add_argument("--kernel", choices=["auto", "split", "tile"], default="auto",
-                    help="FP32 stage kernels: auto = the autotuner's choice (split shapes and the tile kernel)")
+    ap.add_argument("--kernel", choices=["auto", "split", "tile", "persistent"], default="auto",
+                    help="FP32 stage kernels: auto = the autotuner's choice (split shapes, the tile kernel and the "
+                         "persistent step's shapes)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")

@@ -78,6 +78,7 @@ SIGNATURES = {
     "fj_plan_set_variant": (_I, [_P, _I]),
     "fj_plan_set_streams": (_I, [_P, _I]),
     "fj_plan_set_kernel": (_I, [_P, _I]),
+    "fj_plan_set_persist_shape": (_I, [_P, _I]),
     "fj_plan_get_kernel": (_I, [_P, ctypes.POINTER(_I)]),
     "fj_plan_set_wait_limit": (_I, [_P, _I]),
     "fj_plan_check": (_I, [_P, ctypes.POINTER(_I), _P]),
@@ -170,7 +171,9 @@ PIPELINES = {"fused": 0, "staged": 1, "split": 2}
 
 
 NUM_SPLIT_VARIANTS = 6  # FJ_NUM_SPLIT_VARIANTS
-KERNELS = {"split": 0, "tile": 1}  # FJ_KERNEL_SPLIT, FJ_KERNEL_TILE
+KERNELS = {"split": 0, "tile": 1, "persistent": 2}  # FJ_KERNEL_SPLIT, FJ_KERNEL_TILE, FJ_KERNEL_PERSIST
+NUM_PERSIST_SHAPES = 4  # FJ_NUM_PERSIST_SHAPES
+AUTOTUNE_CANDIDATES = 2 * NUM_SPLIT_VARIANTS + 1 + NUM_PERSIST_SHAPES  # FJ_AUTOTUNE_CANDIDATES
 TILES = {"8x32": 0, "4x32": 1, "6x32": 2, "8x16": 3, "16x32": 4, "8x64": 5, "16x16": 6}
 
 

@@ -10,6 +10,7 @@
 #include "fj_common.cuh"
 #include "fj_rhs.cuh"
 #include "fj_split.cuh"
+#include "fj_persist.cuh"
 #include "fj_tile.cuh"
 #include "fj_stage.cuh"
 
@@ -169,8 +170,11 @@ size_t step_layout(const fj_ctx* ctx, const fj_block* blocks, int nblocks, const
   *stage_b = split ? sumStage : align256(5 * maxN * sizeof(double));
   size_t work = split ? split_scratch_bytes(p->precision, cells) : rhs_b;
   // FP32-flux split plans may run the tile kernel, whose padded primitive
-  // buffers share the tail with the split intermediates
-  if (split && with_tile && p->precision == FJ_PREC_F32FLUX) work = std::max(work, tile_scratch_bytes(blocks, nblocks));
+  // buffers share the tail with the split intermediates, or the persistent
+  // step, whose halo slabs follow the intermediates
+  if (split && with_tile && p->precision == FJ_PREC_F32FLUX)
+    work = std::max({work, tile_scratch_bytes(blocks, nblocks),
+                     persist_tail_bytes(blocks, nblocks, links, nlinks, p->ghost)});
   *tail_b = align256(std::max(std::max(work, halo_ws_bytes(blocks, links, nlinks, p->ghost)), (size_t)256));
   return 2 * *stage_b + *tail_b;
 }
@@ -195,8 +199,10 @@ struct StepOpts {
   // the second group half a stage later was slower)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
-  // FP32-flux split plans: run the stages with the fused TMA-tile kernel
+  // FP32-flux split plans: run the stages with the fused TMA-tile kernel, or
+  // the whole step with the persistent kernel
   const TileMaps* tile = nullptr;
+  const PersistPlan* persist = nullptr;
   int wait_limit = -1;
 };
 
@@ -251,6 +257,10 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
       if (s != FJ_OK) return s;
     }
   }
+  // the persistent kernel: halo, BCs and the three stages in one launch
+  if (ctx->pipeline == FJ_PIPELINE_SPLIT && o.persist && p->precision == FJ_PREC_F32FLUX && kmet)
+    return persist_step(ctx, *o.persist, out.data(), nblocks, q1s, q2s, q_out, p, o.p_ref, mu0_b, dt_b, dt, kmet,
+                        tail, o.wait_limit, st);
   s = halo_exchange(ctx, out.data(), nblocks, links, nlinks, p->ghost, (double*)tail, tail_b, st);
   if (s != FJ_OK) return s;
   s = apply_bc(ctx, out.data(), nblocks, bcs, nbcs, p, st);
@@ -624,6 +634,16 @@ int fj_plan_create(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
         delete tm;
         cudaGetLastError();
       }
+      // the persistent step: its work-list and tables (absent when the plan
+      // does not qualify, e.g. more than 64 blocks)
+      PersistPlan* pp = new (std::nothrow) PersistPlan();
+      std::string why;
+      if (pp && persist_setup(ctx, blocks, nblocks, links, nlinks, bcs, nbcs, p, *pp, &why)) {
+        pl->persist = pp;
+      } else {
+        delete pp;
+        cudaGetLastError();
+      }
     }
   }
   *out = pl;
@@ -658,6 +678,10 @@ static int plan_step_impl(fj_plan* pl, double* const* q_in, double* const* q_out
   opts.variant = pl->variant;
   if (pl->kernel == FJ_KERNEL_TILE && pl->tile) {
     opts.tile = (const TileMaps*)pl->tile;
+    opts.wait_limit = pl->wait_limit;
+  }
+  if (pl->kernel == FJ_KERNEL_PERSIST && pl->persist) {
+    opts.persist = (const PersistPlan*)pl->persist;
     opts.wait_limit = pl->wait_limit;
   }
   if (pl->streams == 2) {
@@ -726,13 +750,35 @@ int fj_plan_set_streams(fj_plan* pl, int n) {
 
 int fj_plan_set_kernel(fj_plan* pl, int kernel) {
   if (!pl) return FJ_ERR_INVALID_ARGUMENT;
-  if (kernel != FJ_KERNEL_SPLIT && kernel != FJ_KERNEL_TILE)
+  if (kernel != FJ_KERNEL_SPLIT && kernel != FJ_KERNEL_TILE && kernel != FJ_KERNEL_PERSIST)
     return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "unknown stage kernel");
   if (kernel == FJ_KERNEL_TILE && !pl->tile)
     return set_err(pl->ctx, FJ_ERR_NOT_IMPLEMENTED,
                    "the tile kernel needs an FP32-flux split plan and the driver's tensor-map encoder");
+  if (kernel == FJ_KERNEL_PERSIST && !pl->persist)
+    return set_err(pl->ctx, FJ_ERR_NOT_IMPLEMENTED,
+                   "the persistent step needs an FP32-flux split plan of at most 64 blocks");
   if (kernel != pl->kernel) drop_graphs(pl);
   pl->kernel = kernel;
+  return FJ_OK;
+}
+
+int fj_plan_set_persist_shape(fj_plan* pl, int shape) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  if (shape < 0 || shape >= FJ_NUM_PERSIST_SHAPES) return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "unknown shape");
+  if (!pl->persist)
+    return set_err(pl->ctx, FJ_ERR_NOT_IMPLEMENTED,
+                   "the persistent step needs an FP32-flux split plan of at most 64 blocks");
+  if (shape == pl->persist_shape) return FJ_OK;
+  PersistPlan& pp = *(PersistPlan*)pl->persist;
+  // the work-list is re-laid out and uploaded: no step of this plan may be in flight
+  int s = cuda_status(pl->ctx, cudaDeviceSynchronize(), "persistent shape");
+  if (s != FJ_OK) return s;
+  if (!persist_reshape(pp, pl->blocks.data(), (int)pl->blocks.size(), kPersistShapes[shape].occ,
+                       kPersistShapes[shape].lag_scale))
+    return set_err(pl->ctx, FJ_ERR_CUDA, "persistent step work-list upload failed");
+  drop_graphs(pl);
+  pl->persist_shape = shape;
   return FJ_OK;
 }
 
@@ -752,21 +798,27 @@ int fj_plan_set_wait_limit(fj_plan* pl, int limit) {
 
 int fj_plan_check(fj_plan* pl, int* word, void* stream) {
   if (!pl) return FJ_ERR_INVALID_ARGUMENT;
-  int w = 0;
+  int w = 0, wp = 0;
+  int s = FJ_OK;
   if (pl->tile) {
     const TileMaps& tm = *(const TileMaps*)pl->tile;
-    int s = tile_read_error(tm, &w, S(stream));
+    s = tile_read_error(tm, &w, S(stream));
     if (s == FJ_OK && w != 0) s = tile_clear_error(tm, S(stream));
-    if (s == FJ_OK) s = cuda_status(pl->ctx, cudaStreamSynchronize(S(stream)), "plan check");
-    if (s != FJ_OK) return s;
-  } else {
-    int s = cuda_status(pl->ctx, cudaStreamSynchronize(S(stream)), "plan check");
-    if (s != FJ_OK) return s;
   }
-  if (word) *word = w;
-  return w == 0 ? FJ_OK
-                : set_err(pl->ctx, FJ_ERR_CUDA, "a bounded wait of the tile kernel gave up (error word " +
-                                                    std::to_string(w) + ")");
+  if (s == FJ_OK && pl->persist) {
+    const PersistPlan& pp = *(const PersistPlan*)pl->persist;
+    s = persist_read_error(pp, &wp, S(stream));
+    if (s == FJ_OK && wp != 0) s = persist_clear_error(pp, S(stream));
+  }
+  if (s == FJ_OK) s = cuda_status(pl->ctx, cudaStreamSynchronize(S(stream)), "plan check");
+  if (s != FJ_OK) return s;
+  // bit 0: the tile kernel's word; bit 1: the persistent step's
+  const int all = (w != 0 ? 1 : 0) | (wp != 0 ? 2 : 0);
+  if (word) *word = all;
+  if (all == 0) return FJ_OK;
+  return set_err(pl->ctx, FJ_ERR_CUDA,
+                 std::string("a bounded wait of the ") + (w != 0 ? "tile kernel" : "persistent step") +
+                     " gave up (error word " + std::to_string(w != 0 ? w : wp) + ")");
 }
 
 int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, double dt, int reps, int* chosen,
@@ -779,14 +831,15 @@ int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, dou
   const int nv = tunable ? FJ_NUM_SPLIT_VARIANTS : 1;
   const int ns = split && pl->blocks.size() >= 2 ? 2 : 1;
   const bool with_tile = tunable && pl->p.precision == FJ_PREC_F32FLUX && pl->tile != nullptr;
+  const bool with_persist = tunable && pl->p.precision == FJ_PREC_F32FLUX && pl->persist != nullptr;
   if (ms_out)
-    for (int i = 0; i < 2 * FJ_NUM_SPLIT_VARIANTS + 1; ++i) ms_out[i] = 0.0;
+    for (int i = 0; i < FJ_AUTOTUNE_CANDIDATES; ++i) ms_out[i] = 0.0;
   cudaStream_t st = S(stream);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int s = cuda_status(ctx, cudaEventCreate(&e0), "event");
   if (s == FJ_OK) s = cuda_status(ctx, cudaEventCreate(&e1), "event");
-  const int keep_v = pl->variant, keep_s = pl->streams, keep_k = pl->kernel;
-  int best_v = keep_v, best_s = keep_s, best_k = keep_k;
+  const int keep_v = pl->variant, keep_s = pl->streams, keep_k = pl->kernel, keep_p = pl->persist_shape;
+  int best_v = keep_v, best_s = keep_s, best_k = keep_k, best_p = keep_p;
   float best_ms = -1.0f;
   // mean step time of the plan's current settings over `reps` steps
   auto time_steps = [&](float& ms) -> int {
@@ -830,14 +883,32 @@ int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, dou
       }
     }
   }
+  for (int k = 0; with_persist && k < FJ_NUM_PERSIST_SHAPES && s == FJ_OK; ++k) {
+    s = fj_plan_set_streams(pl, 1);
+    if (s == FJ_OK) s = fj_plan_set_kernel(pl, FJ_KERNEL_PERSIST);
+    if (s == FJ_OK) s = fj_plan_set_persist_shape(pl, k);
+    float ms = 0.0f;
+    if (s == FJ_OK) s = time_steps(ms);
+    if (s == FJ_OK) {
+      if (ms_out) ms_out[2 * FJ_NUM_SPLIT_VARIANTS + 1 + k] = ms / reps;
+      if (best_ms < 0.0f || ms < best_ms) {
+        best_ms = ms;
+        best_s = 1;
+        best_k = FJ_KERNEL_PERSIST;
+        best_p = k;
+      }
+    }
+  }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   int r = fj_plan_set_variant(pl, s == FJ_OK ? best_v : keep_v);
   if (r == FJ_OK) r = fj_plan_set_streams(pl, s == FJ_OK ? best_s : keep_s);
   if (r == FJ_OK) r = fj_plan_set_kernel(pl, s == FJ_OK ? best_k : keep_k);
+  if (r == FJ_OK && pl->persist) r = fj_plan_set_persist_shape(pl, s == FJ_OK ? best_p : keep_p);
   if (s == FJ_OK) s = r;
-  *chosen = pl->kernel == FJ_KERNEL_TILE ? 2 * FJ_NUM_SPLIT_VARIANTS
-                                         : pl->variant + FJ_NUM_SPLIT_VARIANTS * (pl->streams - 1);
+  *chosen = pl->kernel == FJ_KERNEL_TILE      ? 2 * FJ_NUM_SPLIT_VARIANTS
+            : pl->kernel == FJ_KERNEL_PERSIST ? 2 * FJ_NUM_SPLIT_VARIANTS + 1 + pl->persist_shape
+                                              : pl->variant + FJ_NUM_SPLIT_VARIANTS * (pl->streams - 1);
   return s;
 }
 
@@ -1197,6 +1268,7 @@ int fj_plan_destroy(fj_plan* pl) {
     if (k) cudaFree(k);
   if (pl->scratch) cudaFree(pl->scratch);
   delete (TileMaps*)pl->tile;
+  delete (PersistPlan*)pl->persist;
   delete pl;
   return FJ_OK;
 }

@@ -62,6 +62,8 @@ struct fj_plan {
   // bounded-wait limit (-1: the default)
   int kernel = FJ_KERNEL_SPLIT;
   void* tile = nullptr;
+  void* persist = nullptr;  // FJ_KERNEL_PERSIST's plan data (fj::PersistPlan, owned; nullptr when unavailable)
+  int persist_shape = 0;    // its launch shape (FJ_NUM_PERSIST_SHAPES)
   int wait_limit = -1;
 };
 

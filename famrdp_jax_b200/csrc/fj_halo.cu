@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "fj_common.cuh"
+#include "fj_halo_dev.cuh"
 #include "fj_rhs.cuh"
 
 namespace fj {
@@ -37,28 +38,11 @@ namespace {
 constexpr int kMaxLinksPerLaunch = 192;
 constexpr int kMaxBcPerLaunch = 128;
 
-struct HaloDesc {
-  double* tgt;
-  const double* src;
-  long long off;      // slab offset in scratch (doubles)
-  long long s0;       // source cell index of the slab's first element
-  long long sstr[3];  // source index step per step along target slab axis 0, 1, 2
-  int tn[3], sn[3];
-  int tlo[3], ext[3];
-  int tgt_block;
-};
+using namespace hd;
 
 struct HaloTable {
   int n;
   HaloDesc d[kMaxLinksPerLaunch];
-};
-
-struct BcDesc {
-  double* q;
-  double qinf[5];
-  double T_wall;
-  int n[3];
-  int face, type, iso;
 };
 
 struct BcTable {
@@ -66,10 +50,6 @@ struct BcTable {
   double gamma, R;
   BcDesc d[kMaxBcPerLaunch];
 };
-
-__device__ __forceinline__ int64_t cell_index(const int n[3], int i, int j, int k) {
-  return ((int64_t)i * n[1] + j) * n[2] + k;
-}
 
 __global__ void k_halo_gather(const HaloTable tab, double* __restrict__ scratch) {
   grid_dep_wait();
@@ -79,10 +59,8 @@ __global__ void k_halo_gather(const HaloTable tab, double* __restrict__ scratch)
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 5 * V;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int v = (int)(t / V);
-    const int64_t r = t - v * V;
-    const int c = (int)(r % d.ext[2]);
-    const int b = (int)((r / d.ext[2]) % d.ext[1]);
-    const int a = (int)(r / ((int64_t)d.ext[2] * d.ext[1]));
+    int a, b, c;
+    slab_coords(d, t - v * V, a, b, c);
     scratch[d.off + t] = d.src[v * NS + d.s0 + a * d.sstr[0] + b * d.sstr[1] + c * d.sstr[2]];
   }
 }
@@ -95,37 +73,16 @@ __global__ void k_halo_scatter(const HaloTable tab, const double* __restrict__ s
   const int64_t NT = (int64_t)d.tn[0] * d.tn[1] * d.tn[2];
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < V;
        r += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(r % d.ext[2]);
-    const int b = (int)((r / d.ext[2]) % d.ext[1]);
-    const int a = (int)(r / ((int64_t)d.ext[2] * d.ext[1]));
+    int a, b, c;
+    slab_coords(d, r, a, b, c);
     const int ti = d.tlo[0] + a, tj = d.tlo[1] + b, tk = d.tlo[2] + c;
     bool later = false;
-    for (int L2 = L + 1; L2 < tab.n; ++L2) {
-      const HaloDesc& e = tab.d[L2];
-      if (e.tgt_block != d.tgt_block) continue;
-      if (ti >= e.tlo[0] && ti < e.tlo[0] + e.ext[0] && tj >= e.tlo[1] &&
-          tj < e.tlo[1] + e.ext[1] && tk >= e.tlo[2] && tk < e.tlo[2] + e.ext[2]) {
-        later = true;
-        break;
-      }
-    }
+    for (int L2 = L + 1; L2 < tab.n && !later; ++L2)
+      later = tab.d[L2].tgt_block == d.tgt_block && slab_covers(tab.d[L2], ti, tj, tk);
     if (later) continue;
     const int64_t tc = cell_index(d.tn, ti, tj, tk);
 #pragma unroll
     for (int v = 0; v < 5; ++v) d.tgt[v * NT + tc] = scratch[d.off + v * V + r];
-  }
-}
-
-// physics/bc/base.py:15-27 ghost_indices: outer layer o (0..g-1 counted from
-// the face) pairs with the mirrored inner layer.
-__device__ __forceinline__ void bc_layers(int face, int n, int g, int o, int& outer,
-                                          int& inner) {
-  if ((face & 1) == 0) {
-    outer = o;
-    inner = 2 * g - 1 - o;
-  } else {
-    outer = n - 1 - o;
-    inner = n - 2 * g + o;
   }
 }
 
@@ -134,49 +91,13 @@ __global__ void k_bc(const BcTable tab, int g) {
   const BcDesc& d = tab.d[blockIdx.y];
   const int ax = d.face >> 1;
   const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;  // the two other axes
-  const int64_t NT = (int64_t)d.n[0] * d.n[1] * d.n[2];
   const int64_t V = (int64_t)g * d.n[oa] * d.n[ob];
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < V;
        r += (int64_t)gridDim.x * blockDim.x) {
     const int y = (int)(r % d.n[ob]);
     const int x = (int)((r / d.n[ob]) % d.n[oa]);
     const int o = (int)(r / ((int64_t)d.n[ob] * d.n[oa]));
-    int outer, inner;
-    bc_layers(d.face, d.n[ax], g, o, outer, inner);
-    int io[3], ii[3];
-    io[ax] = outer; ii[ax] = inner;
-    io[oa] = x; ii[oa] = x;
-    io[ob] = y; ii[ob] = y;
-    const int64_t co = cell_index(d.n, io[0], io[1], io[2]);
-    const int64_t ci = cell_index(d.n, ii[0], ii[1], ii[2]);
-    if (d.type == FJ_BC_FARFIELD) {  // physics/bc/farfield.py:7-21
-#pragma unroll
-      for (int v = 0; v < 5; ++v) d.q[v * NT + co] = d.qinf[v];
-    } else if (d.type == FJ_BC_WALL && d.iso) {  // physics/bc/wall.py:32-55
-      const double r0 = d.q[ci], r1 = d.q[NT + ci], r2 = d.q[2 * NT + ci],
-                   r3 = d.q[3 * NT + ci], r4 = d.q[4 * NT + ci];
-      const double gm1 = tab.gamma - 1.0;
-      const double ke_i = 0.5 * (r1 * r1 + r2 * r2 + r3 * r3) / r0;
-      const double p_g = gm1 * (r4 - ke_i);
-      const double rho_g = p_g / (tab.R * d.T_wall);
-      const double scale = rho_g / r0;
-      const double u_g = -r1 * scale, v_g = -r2 * scale, w_g = -r3 * scale;
-      const double ke_g = 0.5 * (u_g * u_g + v_g * v_g + w_g * w_g) / rho_g;
-      d.q[co] = rho_g;
-      d.q[NT + co] = u_g;
-      d.q[2 * NT + co] = v_g;
-      d.q[3 * NT + co] = w_g;
-      d.q[4 * NT + co] = p_g / gm1 + ke_g;
-    } else {  // mirror: adiabatic wall (wall.py:27-29) or symmetry (symmetry.py:8-11)
-      double s[5] = {1.0, 1.0, 1.0, 1.0, 1.0};
-      if (d.type == FJ_BC_WALL) {
-        s[1] = s[2] = s[3] = -1.0;
-      } else {
-        s[1 + ax] = -1.0;
-      }
-#pragma unroll
-      for (int v = 0; v < 5; ++v) d.q[v * NT + co] = d.q[v * NT + ci] * s[v];
-    }
+    bc_cell(d, d.q, ax, oa, ob, o, x, y, g, tab.gamma, tab.R);
   }
 }
 
@@ -194,6 +115,10 @@ bool face_box(int face, const int n[3], int g, bool source, int lo[3], int ext[3
     lo[ax] = (face & 1) == 0 ? 0 : n[ax] - g;
   return true;
 }
+
+}  // namespace
+
+namespace hd {
 
 int build_links(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
                 int nlinks, int ghost, std::vector<HaloDesc>& out, size_t& scratch_doubles) {
@@ -262,6 +187,7 @@ int build_links(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link*
       }
     }
     d.tgt_block = l.tgt_block;
+    d.src_block = l.src_block;
     d.off = (long long)scratch_doubles;
     scratch_doubles += 5ull * d.ext[0] * d.ext[1] * d.ext[2];
     scratch_doubles = (scratch_doubles + 31) & ~31ull;  // 256-byte aligned slabs
@@ -270,7 +196,7 @@ int build_links(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link*
   return FJ_OK;
 }
 
-}  // namespace
+}  // namespace hd
 
 size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, int ghost) {
   size_t total = 0;
@@ -378,11 +304,7 @@ namespace {
 __device__ __forceinline__ bool later_link_covers(const HaloTable& tab, int L, int ti, int tj, int tk) {
   const HaloDesc& d = tab.d[L];
   for (int L2 = L + 1; L2 < tab.n; ++L2) {
-    const HaloDesc& e = tab.d[L2];
-    if (e.tgt_block != d.tgt_block) continue;
-    if (ti >= e.tlo[0] && ti < e.tlo[0] + e.ext[0] && tj >= e.tlo[1] && tj < e.tlo[1] + e.ext[1] &&
-        tk >= e.tlo[2] && tk < e.tlo[2] + e.ext[2])
-      return true;
+    if (tab.d[L2].tgt_block == d.tgt_block && slab_covers(tab.d[L2], ti, tj, tk)) return true;
   }
   return false;
 }

@@ -1,0 +1,591 @@
+// fj_step_persist.cu -- one TVD-RK3 step of all blocks (FP32 fluxes, FP64
+// state; solver/step.py:18-56) in ONE persistent launch.
+//
+// Work-list.  The host lays out, once per plan, the items of a step in an
+// order in which every item depends only on items ahead of it:
+//   1. halo gathers of every CUT1TO1 link into scratch (mesh/halo.py:89-90:
+//      all sources are read before any target is written);
+//   2. halo scatters, in link order (the later link wins where slabs overlap);
+//   3. boundary-condition faces in Face order (physics/bc/dispatch.py:15),
+//      each after every scatter into its block and its block's earlier faces;
+//   4. the primitives of each block's halo-filled state;
+//   5. per stage, per block, a wavefront of flux chunks (256 cells: the
+//      viscous components and the i and j faces, k_split_fluxes) and
+//      assembly chunks (248 cells: the k faces, the flux differences, the
+//      viscous divergence and the RK3 combine, k_split_assemble), each
+//      assembly chunk trailing the last flux chunk it reads by `lag` chunks,
+//      so that flux work (issue-bound) and assembly work (bound by loads)
+//      share the SMs and the intermediates are read back while still in L2.
+// A grid of resident CTAs takes items from an atomic counter.  An item first
+// waits (thread 0, bounded) for the completion counters of what it reads:
+//   scatter   all gathers;
+//   BC face   all scatters into its block, its block's BC items of earlier faces;
+//   primitive all scatters into and BC items of its block;
+//   flux s    stage 1: all primitive chunks of its block; stages 2, 3: all
+//             assembly chunks of the previous stage of its block (the
+//             periodic i wrap of the viscous stencil makes plane 0 depend on
+//             plane ni-1, so a stage cannot start on a block before the
+//             previous stage is done with all of it);
+//   assembly  the flux chunks of the i-planes next to its own (p-1 .. p+1,
+//             and the far end plane for the wrap at planes 0 and ni-1);
+// then does its work and bumps its counter (release).  Because every wait
+// is for an item taken earlier, by a CTA that is running, no item waits for
+// an item that cannot start: the launch needs no co-residency guarantee.
+// The arithmetic is the split kernels' (fj_split_dev.cuh) with plain loads
+// in place of the read-only path (the intermediates are written within the
+// launch), so a step is bit-identical to the three-kernel pipeline's.
+// Bounded waits: a wait that runs out sets the sticky error word and an abort
+// flag; every CTA then stops taking items and exits.  No trap, no hang.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "fj_halo_dev.cuh"
+#include "fj_persist.cuh"
+#include "fj_split_dev.cuh"
+
+namespace fj {
+
+namespace {
+
+using namespace sd;
+using hd::BcDesc;
+using hd::HaloDesc;
+
+// Control block (ints).  [0] the sticky error word; from kCtlReset on,
+// zeroed before every launch: the work counter, the abort flag and the
+// completion counters.
+constexpr int kCtlErr = 0;
+constexpr int kCtlReset = 32;
+constexpr int kCtlNext = 32, kCtlAbort = 33, kCtlGather = 34;
+constexpr int kCtlScatter = 64;   // + block
+constexpr int kCtlBc = 128;       // + block
+constexpr int kCtlPrims = 192;    // + block
+constexpr int kCtlAsm = 256;      // + 64 (stage - 1) + block
+constexpr int kCtlFlux = 448;     // + (stage - 1) total_planes + plane_base[block] + plane
+static_assert(kCtlAsm + 3 * kPersistMaxBlocks <= kCtlFlux, "control block layout");
+static_assert(kPersistMaxBlocks <= kMaxSplitBlocks, "block table");
+
+// Item codes: type | stage << 4 | face << 8 | index << 12 (block, link or BC
+// entry); the second word is the chunk.
+enum : uint32_t { kItGather = 0, kItScatter = 1, kItBc = 2, kItPrims = 3, kItFlux = 4, kItAsm = 5 };
+constexpr int kHaloChunk = 2048;  // slab elements per halo / BC item
+constexpr int kFluxCells = kSplitThreads;
+constexpr int kFlags = kRhsInvscd | kRhsViscous;
+// Waits give up after this many polls (64-256 ns apart: about a second)
+// unless the plan sets a limit.
+constexpr long long kDefaultWaitPolls = 1ll << 22;
+
+inline uint32_t item_code(uint32_t type, int stage, int face, int idx) {
+  return type | (uint32_t)stage << 4 | (uint32_t)face << 8 | (uint32_t)idx << 12;
+}
+
+struct PersistParams {
+  Table tab;  // q = q0 = the step's start state; prim: buffer 0, prim_next: buffer 1
+  double* qs[kPersistMaxBlocks][3];  // stage results q1, q2, q_out
+  Phys ph;
+  double gamma, gm1, R, iR;
+  const uint2* items;
+  const HaloDesc* links;
+  const BcDesc* bcs;
+  double* halo;
+  int* ctl;
+  int n_items, nlinks, ghost, wait_limit, n_gather, total_planes;
+  int scatter_total[kPersistMaxBlocks];
+  int bc_prefix[kPersistMaxBlocks][7];  // BC items of the block's faces before face f; [6]: all
+  int plane_base[kPersistMaxBlocks];
+};
+static_assert(sizeof(PersistParams) <= 32764, "kernel parameter space");
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__host__ __device__ __forceinline__ int64_t chunks_of(int64_t n, int64_t per) { return (n + per - 1) / per; }
+
+// Flux chunks (kFluxCells cells) that overlap i-plane q of a block with si
+// cells per plane.
+__device__ __forceinline__ int flux_chunks_in_plane(int64_t si, int q) {
+  return (int)(((int64_t)(q + 1) * si - 1) / kFluxCells - ((int64_t)q * si) / kFluxCells + 1);
+}
+
+// Thread 0: wait until *p >= target, polling at most the wait limit times
+// (0: give up at once; negative: the default).  Giving up records the error
+// and raises the abort flag.
+__device__ bool wait_ge(const PersistParams& P, const int* p, int target) {
+  if (target <= 0) return true;
+  const long long lim = P.wait_limit < 0 ? kDefaultWaitPolls : (long long)P.wait_limit;
+  for (long long it = 0; it < lim; ++it) {
+    if (ld_acquire(p) >= target) return true;
+    if (ld_relaxed(P.ctl + kCtlAbort) != 0) return false;
+    __nanosleep(it < 64 ? 64 : 256);
+  }
+  atomicOr(P.ctl + kCtlErr, 1);
+  atomicExch(P.ctl + kCtlAbort, 1);
+  return false;
+}
+
+// Thread 0: the waits of an item (see the file comment).
+__device__ bool item_deps(const PersistParams& P, uint32_t code, int chunk) {
+  const int type = code & 15, stage = (code >> 4) & 15, face = (code >> 8) & 15, idx = (int)(code >> 12);
+  int* const ctl = P.ctl;
+  switch (type) {
+    case kItGather:
+      return true;
+    case kItScatter:
+      return wait_ge(P, ctl + kCtlGather, P.n_gather);
+    case kItBc: {
+      const int X = P.bcs[idx].block;
+      return wait_ge(P, ctl + kCtlScatter + X, P.scatter_total[X]) &&
+             wait_ge(P, ctl + kCtlBc + X, P.bc_prefix[X][face]);
+    }
+    case kItPrims:
+      return wait_ge(P, ctl + kCtlScatter + idx, P.scatter_total[idx]) &&
+             wait_ge(P, ctl + kCtlBc + idx, P.bc_prefix[idx][6]);
+    case kItFlux: {
+      const SplitBlock& B = P.tab.b[idx].blk;
+      const int64_t N = (int64_t)B.ni * B.nj * B.nk;
+      if (stage == 1) return wait_ge(P, ctl + kCtlPrims + idx, (int)chunks_of(N, kFluxCells));
+      return wait_ge(P, ctl + kCtlAsm + kPersistMaxBlocks * (stage - 2) + idx, (int)chunks_of(N, kAsmCells));
+    }
+    default: {  // kItAsm
+      const SplitBlock& B = P.tab.b[idx].blk;
+      const int64_t si = (int64_t)B.nj * B.nk, N = si * B.ni;
+      const int64_t c0 = (int64_t)chunk * kAsmCells, c1 = min(c0 + kAsmCells, N) - 1;
+      const int pl0 = (int)(c0 / si), pl1 = (int)(c1 / si);
+      const int* f = ctl + kCtlFlux + (stage - 1) * P.total_planes + P.plane_base[idx];
+      const int lo = max(pl0 - 1, 0), hi = min(pl1 + 1, B.ni - 1);
+      for (int q = lo; q <= hi; ++q)
+        if (!wait_ge(P, f + q, flux_chunks_in_plane(si, q))) return false;
+      // the viscous stencil's periodic i wrap
+      if (pl0 == 0 && hi < B.ni - 1 && !wait_ge(P, f + B.ni - 1, flux_chunks_in_plane(si, B.ni - 1))) return false;
+      if (pl1 == B.ni - 1 && lo > 0 && !wait_ge(P, f, flux_chunks_in_plane(si, 0))) return false;
+      return true;
+    }
+  }
+}
+
+// Thread 0, after the item's barrier: publish its completion.
+__device__ void item_done(const PersistParams& P, uint32_t code, int chunk) {
+  const int type = code & 15, stage = (code >> 4) & 15, idx = (int)(code >> 12);
+  int* const ctl = P.ctl;
+  __threadfence();
+  switch (type) {
+    case kItGather: atomicAdd(ctl + kCtlGather, 1); break;
+    case kItScatter: atomicAdd(ctl + kCtlScatter + P.links[idx].tgt_block, 1); break;
+    case kItBc: atomicAdd(ctl + kCtlBc + P.bcs[idx].block, 1); break;
+    case kItPrims: atomicAdd(ctl + kCtlPrims + idx, 1); break;
+    case kItFlux: {
+      const SplitBlock& B = P.tab.b[idx].blk;
+      const int64_t si = (int64_t)B.nj * B.nk, N = si * B.ni;
+      const int64_t c0 = (int64_t)chunk * kFluxCells, c1 = min(c0 + kFluxCells, N) - 1;
+      int* f = ctl + kCtlFlux + (stage - 1) * P.total_planes + P.plane_base[idx];
+      for (int q = (int)(c0 / si); q <= (int)(c1 / si); ++q) atomicAdd(f + q, 1);
+      break;
+    }
+    default: atomicAdd(ctl + kCtlAsm + kPersistMaxBlocks * (stage - 1) + idx, 1);
+  }
+}
+
+// All threads: the item's work.
+__device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code, int chunk) {
+  const int type = code & 15, stage = (code >> 4) & 15, idx = (int)(code >> 12);
+  if (type == kItFlux) {
+    const Dev& d = P.tab.b[idx];
+    SplitBlock B = d.blk;
+    if (stage == 2) B.prim = d.blk.prim_next;  // the primitives alternate between two buffers
+    Cell x;
+    if (decode_cell(d, (int64_t)chunk * kFluxCells + threadIdx.x, x)) flux_cell<float, true, false>(B, x, P.ph, kFlags);
+  } else if (type == kItAsm) {
+    const Dev& d = P.tab.b[idx];
+    SplitBlock B = d.blk;
+    B.q = stage == 1 ? d.blk.q : P.qs[idx][stage - 2];
+    B.out = P.qs[idx][stage - 1];
+    if (stage == 2) {
+      B.prim = d.blk.prim_next;
+      B.prim_next = const_cast<void*>(d.blk.prim);
+    }
+    asm_chunk<float, true, false>(d, B, (int64_t)chunk * kAsmCells, kFlags, stage, stage < 3 ? 1 : 0, P.gm1, P.R,
+                                  P.iR, P.ph);
+  } else if (type == kItPrims) {
+    const SplitBlock& B = P.tab.b[idx].blk;
+    const int64_t c = (int64_t)chunk * kFluxCells + threadIdx.x;
+    if (c < (int64_t)B.ni * B.nj * B.nk) prims_cell<float>(B, (int32_t)c, P.gm1, P.R, P.iR, P.ph.p_ref);
+  } else if (type == kItGather) {
+    const HaloDesc& d = P.links[idx];
+    const double* src = P.tab.b[d.src_block].blk.q;
+    const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
+    const int64_t NS = (int64_t)d.sn[0] * d.sn[1] * d.sn[2];
+    const int64_t t1 = min((int64_t)(chunk + 1) * kHaloChunk, 5 * V);
+    for (int64_t t = (int64_t)chunk * kHaloChunk + threadIdx.x; t < t1; t += kSplitThreads) {
+      const int v = (int)(t / V);
+      int a, b, c;
+      hd::slab_coords(d, t - v * V, a, b, c);
+      P.halo[d.off + t] = src[v * NS + d.s0 + a * d.sstr[0] + b * d.sstr[1] + c * d.sstr[2]];
+    }
+  } else if (type == kItScatter) {
+    const HaloDesc& d = P.links[idx];
+    double* tgt = const_cast<double*>(P.tab.b[d.tgt_block].blk.q);
+    const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
+    const int64_t NT = (int64_t)d.tn[0] * d.tn[1] * d.tn[2];
+    const int64_t r1 = min((int64_t)(chunk + 1) * kHaloChunk, V);
+    for (int64_t r = (int64_t)chunk * kHaloChunk + threadIdx.x; r < r1; r += kSplitThreads) {
+      int a, b, c;
+      hd::slab_coords(d, r, a, b, c);
+      const int ti = d.tlo[0] + a, tj = d.tlo[1] + b, tk = d.tlo[2] + c;
+      bool later = false;
+      for (int L2 = idx + 1; L2 < P.nlinks && !later; ++L2)
+        later = P.links[L2].tgt_block == d.tgt_block && hd::slab_covers(P.links[L2], ti, tj, tk);
+      if (later) continue;
+      const int64_t tc = hd::cell_index(d.tn, ti, tj, tk);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) tgt[v * NT + tc] = P.halo[d.off + v * V + r];
+    }
+  } else {  // kItBc
+    const BcDesc& d = P.bcs[idx];
+    double* q = const_cast<double*>(P.tab.b[d.block].blk.q);
+    const int ax = d.face >> 1;
+    const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
+    const int64_t V = (int64_t)P.ghost * d.n[oa] * d.n[ob];
+    const int64_t r1 = min((int64_t)(chunk + 1) * kHaloChunk, V);
+    for (int64_t r = (int64_t)chunk * kHaloChunk + threadIdx.x; r < r1; r += kSplitThreads) {
+      const int y = (int)(r % d.n[ob]);
+      const int x = (int)((r / d.n[ob]) % d.n[oa]);
+      const int o = (int)(r / ((int64_t)d.n[ob] * d.n[oa]));
+      hd::bc_cell(d, q, ax, oa, ob, o, x, y, P.ghost, P.gamma, P.R);
+    }
+  }
+}
+
+// Thread 0 claims the next item while the CTA works on the current one, so
+// the claim's round trip to L2 overlaps the work.  Holding a claim on a later
+// item cannot deadlock: the earliest unfinished item is always some CTA's
+// current item (a CTA only claims after taking its current one), and it
+// waits only for earlier items, which are finished.
+template <int OCC>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_step_persist(const __grid_constant__ PersistParams P) {
+  // the current and the claimed next item live in shared memory (thread 0
+  // writes them), so nothing stays in registers across an item's work
+  __shared__ uint2 s_it, s_nxt_it;
+  __shared__ int s_valid, s_ok, s_nxt;
+  if (threadIdx.x == 0) {
+    const int i = atomicAdd(P.ctl + kCtlNext, 1);
+    s_nxt = i;
+    s_nxt_it = i < P.n_items ? P.items[i] : make_uint2(0u, 0u);
+  }
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_valid = s_nxt < P.n_items && ld_relaxed(P.ctl + kCtlAbort) == 0 ? 1 : 0;
+      s_it = s_nxt_it;
+    }
+    __syncthreads();
+    if (!s_valid) return;
+    const uint2 it = s_it;
+    if (threadIdx.x == 0) {
+      const int i = atomicAdd(P.ctl + kCtlNext, 1);
+      const bool ok = item_deps(P, it.x, (int)it.y);
+      if (ok) __threadfence();
+      s_ok = ok ? 1 : 0;
+      s_nxt = i;
+      s_nxt_it = i < P.n_items ? P.items[i] : make_uint2(0u, 0u);
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    item_work(P, it.x, (int)it.y);
+    __syncthreads();
+    if (threadIdx.x == 0) item_done(P, it.x, (int)it.y);
+  }
+}
+
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cudaGetLastError();
+  }
+  return n;
+}
+
+int resident_grid(int occ) {
+  int per_sm = 0;
+  const cudaError_t e = occ == 3
+                            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_persist<3>, kSplitThreads, 0)
+                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_persist<4>, kSplitThreads, 0);
+  if (e != cudaSuccess || per_sm <= 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sm_count();
+}
+
+// The stage part of the work-list: per stage, per block, the flux / assembly
+// wavefront (see the file comment).
+void stage_items(const fj_block* blocks, int nblocks, int lag, std::vector<uint2>& out) {
+  for (int s = 1; s <= 3; ++s)
+    for (int X = 0; X < nblocks; ++X) {
+      const int64_t si = (int64_t)blocks[X].nj * blocks[X].nk, N = si * blocks[X].ni;
+      const int ni = blocks[X].ni;
+      const int nF = (int)chunks_of(N, kFluxCells), nA = (int)chunks_of(N, kAsmCells);
+      // slot[a]: the flux chunk after which assembly chunk a is taken
+      std::vector<std::vector<int>> after(nF);
+      for (int a = 0; a < nA; ++a) {
+        const int64_t c0 = (int64_t)a * kAsmCells, c1 = std::min<int64_t>(c0 + kAsmCells, N) - 1;
+        const int pl0 = (int)(c0 / si), pl1 = (int)(c1 / si);
+        // the last flux chunk of plane min(pl1 + 1, ni - 1); all of them for plane 0 (wrap)
+        const int need_plane = std::min(pl1 + 1, ni - 1);
+        int64_t f_need = (pl0 == 0 && ni > 1) ? nF - 1 : ((int64_t)(need_plane + 1) * si - 1) / kFluxCells;
+        const int slot = (int)std::min<int64_t>(f_need + lag, nF - 1);
+        after[slot].push_back(a);
+      }
+      for (int f = 0; f < nF; ++f) {
+        out.push_back(make_uint2(item_code(kItFlux, s, 0, X), (unsigned)f));
+        for (int a : after[f]) out.push_back(make_uint2(item_code(kItAsm, s, 0, X), (unsigned)a));
+      }
+    }
+}
+
+}  // namespace
+
+PersistPlan::~PersistPlan() {
+  if (items) cudaFree(items);
+  if (links) cudaFree(links);
+  if (bcs) cudaFree(bcs);
+  if (ctl) cudaFree(ctl);
+}
+
+size_t persist_tail_bytes(const fj_block* blocks, int nblocks, const fj_link* links, int nlinks, int ghost) {
+  int64_t cells = 0;
+  for (int b = 0; b < nblocks; ++b) cells += (int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk;
+  const size_t split = (split_scratch_bytes(FJ_PREC_F32FLUX, cells) + 255) & ~(size_t)255;
+  return split + halo_ws_bytes(blocks, links, nlinks, ghost);
+}
+
+bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                   const fj_bc* bcs, int nbcs, const fj_params* p, PersistPlan& pp, std::string* why) {
+  auto fail = [&](const std::string& w) {
+    if (why) *why = w;
+    return false;
+  };
+  if (p->precision != FJ_PREC_F32FLUX) return fail("the persistent step is the FP32-flux path's");
+  if (nblocks < 1 || nblocks > kPersistMaxBlocks) return fail("the persistent step takes 1..64 blocks");
+  for (int b = 0; b < nblocks; ++b) {
+    if ((int64_t)16 * blocks[b].ni * blocks[b].nj * blocks[b].nk > INT32_MAX)
+      return fail("block too large for 32-bit record offsets");
+    if (blocks[b].ni < 1 || blocks[b].nj < 1 || blocks[b].nk < 1) return fail("empty block");
+  }
+  std::vector<HaloDesc> descs;
+  size_t nd = 0;
+  if (hd::build_links(ctx, blocks, nblocks, links, nlinks, p->ghost, descs, nd) != FJ_OK)
+    return fail("halo links: " + (ctx ? ctx->last_error : std::string()));
+  if (descs.size() >= (1u << 20)) return fail("too many links");
+  pp.scatter_total.assign(kPersistMaxBlocks, 0);
+  pp.bc_prefix.assign(kPersistMaxBlocks * 7, 0);
+  pp.plane_base.assign(kPersistMaxBlocks, 0);
+  std::vector<uint2> head;
+  // 1. gathers, 2. scatters (link order)
+  pp.n_gather = 0;
+  for (size_t L = 0; L < descs.size(); ++L) {
+    descs[L].tgt = nullptr;
+    descs[L].src = nullptr;
+    const int64_t V = (int64_t)descs[L].ext[0] * descs[L].ext[1] * descs[L].ext[2];
+    const int64_t g = chunks_of(5 * V, kHaloChunk);
+    for (int64_t c = 0; c < g; ++c) head.push_back(make_uint2(item_code(kItGather, 0, 0, (int)L), (unsigned)c));
+    pp.n_gather += (int)g;
+  }
+  for (size_t L = 0; L < descs.size(); ++L) {
+    const int64_t V = (int64_t)descs[L].ext[0] * descs[L].ext[1] * descs[L].ext[2];
+    const int64_t n = chunks_of(V, kHaloChunk);
+    for (int64_t c = 0; c < n; ++c) head.push_back(make_uint2(item_code(kItScatter, 0, 0, (int)L), (unsigned)c));
+    pp.scatter_total[descs[L].tgt_block] += (int)n;
+  }
+  // 3. boundary conditions, Face order, list order within a face
+  std::vector<BcDesc> bds;
+  std::vector<int64_t> bc_chunks(nbcs, 0);
+  for (int e = 0; e < nbcs; ++e) {
+    const fj_bc& bc = bcs[e];
+    if (bc.block < 0 || bc.block >= nblocks || bc.face < 0 || bc.face > 5) return fail("bc entry out of range");
+    if (bc.type != FJ_BC_WALL && bc.type != FJ_BC_SYMMETRY && bc.type != FJ_BC_FARFIELD)
+      return fail("unsupported bc type");
+    const fj_block& blk = blocks[bc.block];
+    BcDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.q = nullptr;
+    d.n[0] = blk.ni;
+    d.n[1] = blk.nj;
+    d.n[2] = blk.nk;
+    d.face = bc.face;
+    d.type = bc.type;
+    d.iso = bc.isothermal;
+    d.T_wall = bc.T_wall;
+    for (int v = 0; v < 5; ++v) d.qinf[v] = bc.q_inf[v];
+    d.block = bc.block;
+    bds.push_back(d);
+    const int ax = bc.face >> 1;
+    const int64_t area = (int64_t)blk.ni * blk.nj * blk.nk / d.n[ax];
+    bc_chunks[e] = chunks_of(area * p->ghost, kHaloChunk);
+  }
+  for (int face = 0; face < 6; ++face)
+    for (int e = 0; e < nbcs; ++e) {
+      if (bcs[e].face != face) continue;
+      for (int64_t c = 0; c < bc_chunks[e]; ++c) head.push_back(make_uint2(item_code(kItBc, 0, face, e), (unsigned)c));
+      // later faces of this block wait for these items
+      for (int f = face + 1; f <= 6; ++f) pp.bc_prefix[bcs[e].block * 7 + f] += (int)bc_chunks[e];
+    }
+  // 4. primitives, block order
+  int planes = 0;
+  for (int X = 0; X < nblocks; ++X) {
+    const int64_t N = (int64_t)blocks[X].ni * blocks[X].nj * blocks[X].nk;
+    for (int64_t c = 0; c < chunks_of(N, kFluxCells); ++c)
+      head.push_back(make_uint2(item_code(kItPrims, 0, 0, X), (unsigned)c));
+    pp.plane_base[X] = planes;
+    planes += blocks[X].ni;
+  }
+  pp.total_planes = planes;
+  pp.reset_from = kCtlReset;
+  pp.ctl_ints = kCtlFlux + 3 * planes;
+  pp.nlinks = (int)descs.size();
+  pp.nbcs = (int)bds.size();
+  pp.split_bytes = persist_tail_bytes(blocks, nblocks, nullptr, 0, p->ghost);
+  pp.head.swap(head);
+  // device tables
+  auto upload = [](void** dst, const void* src, size_t bytes) {
+    if (bytes == 0) return true;
+    if (cudaMalloc(dst, bytes) != cudaSuccess) {
+      *dst = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+    return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  if (!upload(&pp.links, descs.data(), descs.size() * sizeof(HaloDesc)) ||
+      !upload(&pp.bcs, bds.data(), bds.size() * sizeof(BcDesc)))
+    return fail("persistent step tables: device allocation failed");
+  if (cudaMalloc((void**)&pp.ctl, (size_t)pp.ctl_ints * sizeof(int)) != cudaSuccess ||
+      cudaMemset(pp.ctl, 0, (size_t)pp.ctl_ints * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail("persistent step control block: device allocation failed");
+  }
+  if (!persist_reshape(pp, blocks, nblocks, 4, 1.0)) return fail("persistent step work-list upload failed");
+  return true;
+}
+
+bool persist_reshape(PersistPlan& pp, const fj_block* blocks, int nblocks, int occ, double lag_scale) {
+  if (occ != 3 && occ != 4) return false;
+  const int grid = resident_grid(occ);
+  if (grid <= 0) return false;
+  std::vector<uint2> items(pp.head);
+  const int lag = std::max(0, (int)(lag_scale * grid / 2));
+  stage_items(blocks, nblocks, lag, items);
+  if (items.size() >= (size_t)INT32_MAX) return false;
+  if (pp.items && (int)items.size() != pp.n_items) {
+    cudaFree(pp.items);
+    pp.items = nullptr;
+  }
+  if (!pp.items && cudaMalloc(&pp.items, items.size() * sizeof(uint2)) != cudaSuccess) {
+    pp.items = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaMemcpy(pp.items, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  pp.n_items = (int)items.size();
+  pp.grid = std::min<int64_t>(grid, pp.n_items);
+  pp.occ = occ;
+  pp.lag = lag;
+  return true;
+}
+
+int persist_step(fj_ctx* ctx, const PersistPlan& pp, const fj_block* blocks, int nblocks, double* const* q1s,
+                 double* const* q2s, double* const* q_out, const fj_params* p, double p_ref, const double* mu0_b,
+                 const double* dt_b, double dt, void* const* kmet, void* tail, int wait_limit, cudaStream_t st) {
+  if (nblocks < 1 || nblocks > kPersistMaxBlocks || !kmet || !pp.items || !pp.ctl)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "persistent step: plan not set up");
+  std::unique_ptr<PersistParams> hold(new (std::nothrow) PersistParams());  // 14 KB: off the stack
+  if (!hold) return set_err(ctx, FJ_ERR_NO_MEMORY, "persistent step parameters");
+  PersistParams& P = *hold;
+  std::vector<SplitBlock> sb(nblocks);
+  for (int b = 0; b < nblocks; ++b) {
+    SplitBlock& e = sb[b];
+    e = SplitBlock{};
+    e.q = blocks[b].q;
+    e.q0 = blocks[b].q;
+    e.out = nullptr;
+    e.kxyz = blocks[b].kxyz;
+    e.kaos = kmet[b];
+    e.vol = blocks[b].vol;
+    e.mu0 = mu0_b ? mu0_b[b] : p->mu0;
+    e.dt = dt_b ? dt_b[b] : dt;
+    e.ni = blocks[b].ni;
+    e.nj = blocks[b].nj;
+    e.nk = blocks[b].nk;
+    if (!e.kaos) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "persistent step: metric records missing");
+  }
+  split_assign_scratch(FJ_PREC_F32FLUX, sb.data(), nblocks, tail);
+  P.tab.n = nblocks;
+  for (int b = 0; b < nblocks; ++b) {
+    P.tab.b[b].blk = sb[b];
+    P.tab.b[b].dk.init((uint32_t)sb[b].nk);
+    P.tab.b[b].dj.init((uint32_t)sb[b].nj);
+    P.qs[b][0] = q1s[b];
+    P.qs[b][1] = q2s[b];
+    P.qs[b][2] = q_out[b];
+    P.scatter_total[b] = pp.scatter_total[b];
+    for (int f = 0; f < 7; ++f) P.bc_prefix[b][f] = pp.bc_prefix[b * 7 + f];
+    P.plane_base[b] = pp.plane_base[b];
+  }
+  P.ph = make_phys(p);
+  P.ph.p_ref = p_ref;
+  P.gamma = p->gamma;
+  P.gm1 = p->gamma - 1.0;
+  P.R = p->R;
+  P.iR = 1.0 / p->R;
+  P.items = (const uint2*)pp.items;
+  P.links = (const HaloDesc*)pp.links;
+  P.bcs = (const BcDesc*)pp.bcs;
+  P.halo = (double*)((char*)tail + pp.split_bytes);
+  P.ctl = pp.ctl;
+  P.n_items = pp.n_items;
+  P.nlinks = pp.nlinks;
+  P.ghost = p->ghost;
+  P.wait_limit = wait_limit;
+  P.n_gather = pp.n_gather;
+  P.total_planes = pp.total_planes;
+  int s = cuda_status(ctx,
+                      cudaMemsetAsync(pp.ctl + pp.reset_from, 0, (size_t)(pp.ctl_ints - pp.reset_from) * sizeof(int), st),
+                      "persistent step counters");
+  if (s != FJ_OK) return s;
+  if (pp.occ == 3)
+    k_step_persist<3><<<pp.grid, kSplitThreads, 0, st>>>(P);
+  else
+    k_step_persist<4><<<pp.grid, kSplitThreads, 0, st>>>(P);
+  ctx->launches += 1;
+  return launch_status(ctx, "persistent step launch");
+}
+
+int persist_read_error(const PersistPlan& pp, int* out, cudaStream_t st) {
+  *out = 0;
+  if (!pp.ctl) return FJ_OK;
+  cudaError_t e = cudaMemcpyAsync(out, pp.ctl + kCtlErr, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
+}
+
+int persist_clear_error(const PersistPlan& pp, cudaStream_t st) {
+  if (!pp.ctl) return FJ_OK;
+  return cudaMemsetAsync(pp.ctl + kCtlErr, 0, sizeof(int), st) == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
+}
+
+}  // namespace fj

@@ -111,13 +111,15 @@ class StepPlan:
         self.dts = None if dt is None else [float(v) for v in dt]
 
     def autotune(self, qs, outs, dt: float, reps: int = 3):
-        """Times every launch shape of the FP32-flux split kernels and both
-        stream counts, and the fused tile kernel, over `reps` steps qs -> outs
+        """Times every launch shape of the split kernels and both stream
+        counts and, on FP32-flux plans, the fused tile kernel and the
+        persistent step in each of its shapes, over `reps` steps qs -> outs
         (outs is overwritten) and keeps the fastest; returns (chosen, mean step
         ms per candidate), the candidate index being shape +
-        NUM_SPLIT_VARIANTS * (streams - 1), or 2 * NUM_SPLIT_VARIANTS for the
-        tile kernel."""
-        n = 2 * _capi.NUM_SPLIT_VARIANTS + 1
+        NUM_SPLIT_VARIANTS * (streams - 1), 2 * NUM_SPLIT_VARIANTS for the
+        tile kernel, or 2 * NUM_SPLIT_VARIANTS + 1 + k for the persistent step
+        in shape k."""
+        n = _capi.AUTOTUNE_CANDIDATES
         ms = (ctypes.c_double * n)()
         ch = ctypes.c_int()
         c = _capi.ctx(self.device)
@@ -132,8 +134,10 @@ class StepPlan:
 
     def set_kernel(self, kernel: str) -> None:
         """Stage kernels of an FP32-flux plan: "split" (three kernels per stage
-        through scratch) or "tile" (one persistent fused kernel per stage over a
-        (tile, i-plane) work-list, primitive planes staged by TMA)."""
+        through scratch), "tile" (one persistent fused kernel per stage over a
+        (tile, i-plane) work-list, primitive planes staged by TMA) or
+        "persistent" (the whole step -- halo, boundary faces and the three
+        stages -- in one launch over a dependency-ordered work-list)."""
         if kernel not in _capi.KERNELS:
             raise KeyError(kernel)
         c = _capi.ctx(self.device)
@@ -146,15 +150,22 @@ class StepPlan:
         _capi.check(self._lib.fj_plan_get_kernel(self._handle, ctypes.byref(k)), "fj_plan_get_kernel", c)
         return {v: n for n, v in _capi.KERNELS.items()}[k.value]
 
+    def set_persist_shape(self, shape: int) -> None:
+        """Launch shape of the persistent step (0 .. NUM_PERSIST_SHAPES-1)."""
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_set_persist_shape(self._handle, int(shape)), "fj_plan_set_persist_shape", c)
+
     def set_wait_limit(self, limit: int) -> None:
-        """Tries of each bounded wait in the tile kernel (-1: the default)."""
+        """Tries of each bounded wait in the tile kernel and the persistent
+        step (-1: the default)."""
         c = _capi.ctx(self.device)
         _capi.check(self._lib.fj_plan_set_wait_limit(self._handle, int(limit)), "fj_plan_set_wait_limit", c)
 
     def check(self) -> int:
-        """Waits for the plan's work on the current stream and returns the tile
-        kernel's error word (0: no bounded wait gave up), clearing it; raises
-        RuntimeError when it was nonzero."""
+        """Waits for the plan's work on the current stream and returns the
+        error words of the tile kernel (bit 0) and the persistent step (bit 1)
+        (0: no bounded wait gave up), clearing them; raises RuntimeError when
+        one was nonzero."""
         w = ctypes.c_int()
         c = _capi.ctx(self.device)
         _capi.check(self._lib.fj_plan_check(self._handle, ctypes.byref(w), _capi.stream(self.device)),

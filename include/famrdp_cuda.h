@@ -287,18 +287,41 @@ int fj_plan_set_variant(fj_plan* plan, int variant);
  * results agree to FP32 rounding (the face arithmetic is the same; the
  * temperature is formed in FP32).  FJ_KERNEL_TILE returns
  * FJ_ERR_NOT_IMPLEMENTED for FP64 or non-split plans and when the driver's
- * tensor-map encoder is unavailable.  Changing it drops captured graphs. */
+ * tensor-map encoder is unavailable.
+ * FJ_KERNEL_PERSIST runs the WHOLE step (halo gathers and scatters, boundary
+ * faces, primitives and the three stages of all blocks) as ONE persistent
+ * launch over a work-list fixed at plan creation; every item waits on device
+ * completion counters for the items it reads (a halo scatter for all gathers,
+ * a block's BC faces for the scatters into it and its earlier faces, an
+ * assembly chunk for the flux chunks of its neighbouring i-planes, a stage of
+ * a block for the previous stage of that block), and the flux and assembly
+ * chunks of a stage are interleaved so both kinds of work share the SMs.  Its
+ * arithmetic is the split kernels', and its results are bit-identical to
+ * FJ_KERNEL_SPLIT's.  FJ_ERR_NOT_IMPLEMENTED for FP64 or non-split plans and
+ * plans of more than 64 blocks.  fj_plan_stage runs the split kernels for it.
+ * Changing the kernel drops captured graphs. */
 #define FJ_KERNEL_SPLIT 0
 #define FJ_KERNEL_TILE 1
+#define FJ_KERNEL_PERSIST 2
 int fj_plan_set_kernel(fj_plan* plan, int kernel);
 int fj_plan_get_kernel(const fj_plan* plan, int* kernel);
-/* Diagnostics of the tile kernel's bounded waits: every wait for a TMA copy
- * gives up after `limit` tries (-1 restores the default, about a second);
- * a CTA whose wait gave up records it in the plan's error word, stops and
- * exits after its copies in flight have landed (never a trap or a hang).
- * fj_plan_check waits for `stream`, stores the word (0 = no wait gave up) in
- * *word, clears it, and returns FJ_ERR_CUDA when it was nonzero.  limit = 0
- * makes every wait give up at once (used by the tests). */
+/* Launch shape of FJ_KERNEL_PERSIST, one of FJ_NUM_PERSIST_SHAPES (0 is the
+ * default): resident CTAs per SM (its register cap) and how many flux chunks
+ * an assembly chunk trails the last flux chunk it reads by.  Results do not
+ * depend on it.  Drops captured graphs. */
+#define FJ_NUM_PERSIST_SHAPES 4
+int fj_plan_set_persist_shape(fj_plan* plan, int shape);
+/* Diagnostics of the bounded waits of the tile kernel (every wait for a TMA
+ * copy) and of the persistent step (every wait on a completion counter): a
+ * wait gives up after `limit` tries (-1 restores the default, about a
+ * second); a CTA whose wait gave up records it in the plan's error word and
+ * exits (the tile kernel after its copies in flight have landed; the
+ * persistent step raises an abort flag on which every other CTA stops taking
+ * items) -- never a trap or a hang.  fj_plan_check waits for `stream`, stores
+ * the words (bit 0: the tile kernel's, bit 1: the persistent step's; 0 = no
+ * wait gave up) in *word, clears them, and returns FJ_ERR_CUDA when one was
+ * nonzero.  limit = 0 makes every wait give up at once (used by the tests;
+ * the persistent step's results are then incomplete). */
 int fj_plan_set_wait_limit(fj_plan* plan, int limit);
 int fj_plan_check(fj_plan* plan, int* word, void* stream);
 /* Split-pipeline plans of two or more blocks: n = 2 splits the blocks into two
@@ -310,12 +333,14 @@ int fj_plan_set_streams(fj_plan* plan, int n);
 /* The autotuner: times `reps` steps q_in -> q_out (after one untimed step) for
  * every launch shape (split plans, both precisions) and stream count (split plans of
  * two or more blocks) with CUDA events on `stream`, keeps the fastest in the
- * plan and reports it as shape + FJ_NUM_SPLIT_VARIANTS * (streams - 1), or
- * 2 * FJ_NUM_SPLIT_VARIANTS for the tile kernel (FP32-flux plans whose tile
- * kernel is available: one more candidate) (and, if ms_out is non-NULL, the
- * 2 * FJ_NUM_SPLIT_VARIANTS + 1 mean step times at those indices; 0 where not
- * timed).  q_out is overwritten; q_in is not changed.  Synchronises the
- * stream. */
+ * plan and reports it as shape + FJ_NUM_SPLIT_VARIANTS * (streams - 1),
+ * 2 * FJ_NUM_SPLIT_VARIANTS for the tile kernel, or
+ * 2 * FJ_NUM_SPLIT_VARIANTS + 1 + k for the persistent step in shape k
+ * (FP32-flux plans where those kernels are available: more candidates) (and,
+ * if ms_out is non-NULL, the FJ_AUTOTUNE_CANDIDATES mean step times at those
+ * indices; 0 where not timed).  q_out is overwritten; q_in is not changed.
+ * Synchronises the stream. */
+#define FJ_AUTOTUNE_CANDIDATES (2 * FJ_NUM_SPLIT_VARIANTS + 1 + FJ_NUM_PERSIST_SHAPES)
 int fj_plan_autotune(fj_plan* plan, double* const* q_in, double* const* q_out, double dt, int reps,
                      int* chosen, double* ms_out, void* stream);
 int fj_plan_step_graph(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,

@@ -507,8 +507,9 @@ def test_residual_and_monitored_run(cuda_device, tmp_path):
 def test_autotune_launch_shapes_agree(cuda_device, precision):
     """Every launch shape of the split kernels and both stream counts (block
     groups on two streams, also captured as a graph) give the same step bit for
-    bit, in both precisions; the autotuner keeps one of them (or, FP32-flux,
-    the tile kernel)."""
+    bit, in both precisions, and so does (FP32-flux) the persistent step in
+    every launch shape; the autotuner keeps one of them (or, FP32-flux, the
+    tile kernel or the persistent step)."""
     import dataclasses
     from famrdp_jax_b200 import _capi
     from famrdp_jax_b200.solver.step import StepPlan
@@ -527,16 +528,30 @@ def test_autotune_launch_shapes_agree(cuda_device, precision):
                 o = [torch.empty_like(q) for q in qs]
                 plan.run(qs, o, dt, graph=graph)
                 outs.append(o)
+    if precision == "f32":
+        # the persistent step in every launch shape, plain and as a graph
+        plan.set_streams(1)
+        plan.set_kernel("persistent")
+        for shape in range(_capi.NUM_PERSIST_SHAPES):
+            plan.set_persist_shape(shape)
+            for graph in (False, True):
+                o = [torch.empty_like(q) for q in qs]
+                plan.run(qs, o, dt, graph=graph)
+                outs.append(o)
+        assert plan.check() == 0
+        plan.set_kernel("split")
     for o in outs[1:]:
         for a, b in zip(o, outs[0]):
             assert torch.equal(a, b)
     chosen, ms = plan.autotune(qs, [torch.empty_like(q) for q in qs], dt, reps=2)
     n = _capi.NUM_SPLIT_VARIANTS
     # candidates: every split shape at one and two streams, then (FP32-flux) the
-    # tile kernel
+    # tile kernel and the persistent step's shapes
     timed = ms if precision == "f32" else ms[:2 * n]
-    assert 0 <= chosen <= 2 * n and len(ms) == 2 * n + 1 and min(timed) > 0
-    assert plan.kernel == ("tile" if chosen == 2 * n else "split")
+    assert 0 <= chosen < _capi.AUTOTUNE_CANDIDATES and len(ms) == _capi.AUTOTUNE_CANDIDATES and min(timed) > 0
+    if precision == "f64":
+        assert chosen < 2 * n and not any(ms[2 * n:])
+    assert plan.kernel == ("tile" if chosen == 2 * n else "persistent" if chosen > 2 * n else "split")
 
 
 def test_plan_argument_errors(cuda_device):
