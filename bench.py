@@ -608,11 +608,16 @@ def run_ours(args):
             plan.set_variant(args.shape)
             if args.kernel != "auto":
                 plan.set_kernel(args.kernel)
+            if args.kernel == "persistent":
+                plan.set_persist_shape(args.persist_shape)
         q0s = [b.q for b in st0.blocks]
         qin = [q.clone() for q in q0s]  # the stage input, distinct from the step's start state
         outs = [torch.empty_like(q) for q in q0s]
         for _ in range(4):
-            plan.stage(qin, q0s, outs, dt, 2)
+            if plan.kernel == "persistent":  # its one launch is a whole step
+                plan.run(qin, outs, dt)
+            else:
+                plan.stage(qin, q0s, outs, dt, 2)
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"stage_only": True, "precision": args.precision, "shape": args.shape,
@@ -703,8 +708,11 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--stage-only", action="store_true",
-                    help="only run four standalone stage-2 evaluations (for a profiler)")
+                    help="only run four standalone stage-2 evaluations (four steps with --kernel persistent), "
+                         "for a profiler")
     ap.add_argument("--shape", type=int, default=1, help="FP32 launch shape for --stage-only")
+    ap.add_argument("--persist-shape", type=int, default=0,
+                    help="launch shape of the persistent step for --stage-only --kernel persistent")
     ap.add_argument("--kernel", choices=["auto", "split", "tile", "persistent"], default="auto",
                     help="FP32 stage kernels: auto = the autotuner's choice (split shapes, the tile kernel and the "
                          "persistent step's shapes)")

@@ -25,7 +25,7 @@ struct PersistShape {
   int occ;
   double lag_scale;
 };
-constexpr PersistShape kPersistShapes[] = {{4, 1.0}, {3, 1.0}, {4, 0.5}, {4, 2.0}};
+constexpr PersistShape kPersistShapes[] = {{4, 4.0}, {3, 4.0}, {4, 1e6}, {3, 1e6}};
 static_assert(sizeof(kPersistShapes) / sizeof(kPersistShapes[0]) == FJ_NUM_PERSIST_SHAPES, "shape table");
 
 // Host-side plan data of the persistent step: the work-list and the

@@ -9,15 +9,17 @@
 //   3. boundary-condition faces in Face order (physics/bc/dispatch.py:15),
 //      each after every scatter into its block and its block's earlier faces;
 //   4. the primitives of each block's halo-filled state;
-//   5. per stage, per block, a wavefront of flux chunks (256 cells: the
+//   5. per stage, per block, a wavefront of flux chunks (224 cells: the
 //      viscous components and the i and j faces, k_split_fluxes) and
-//      assembly chunks (248 cells: the k faces, the flux differences, the
+//      assembly chunks (217 cells: the k faces, the flux differences, the
 //      viscous divergence and the RK3 combine, k_split_assemble), each
 //      assembly chunk trailing the last flux chunk it reads by `lag` chunks,
 //      so that flux work (issue-bound) and assembly work (bound by loads)
 //      share the SMs and the intermediates are read back while still in L2.
-// A grid of resident CTAs takes items from an atomic counter.  An item first
-// waits (thread 0, bounded) for the completion counters of what it reads:
+// A grid of resident CTAs takes items from an atomic counter; in each CTA a
+// scheduler warp claims items, waits (bounded) for the completion counters
+// of what an item reads and publishes completions, while seven worker warps
+// compute the items it hands over (k_step_persist).  An item waits for:
 //   scatter   all gathers;
 //   BC face   all scatters into its block, its block's BC items of earlier faces;
 //   primitive all scatters into and BC items of its block;
@@ -28,9 +30,10 @@
 //             previous stage is done with all of it);
 //   assembly  the flux chunks of the i-planes next to its own (p-1 .. p+1,
 //             and the far end plane for the wrap at planes 0 and ni-1);
-// then does its work and bumps its counter (release).  Because every wait
+// then is computed, and its counter is bumped (release).  Because every wait
 // is for an item taken earlier, by a CTA that is running, no item waits for
-// an item that cannot start: the launch needs no co-residency guarantee.
+// an item that cannot start: the launch needs no co-residency guarantee
+// (schedule() keeps this true for the items a CTA holds back).
 // The arithmetic is the split kernels' (fj_split_dev.cuh) with plain loads
 // in place of the read-only path (the intermediates are written within the
 // launch), so a step is bit-identical to the three-kernel pipeline's.
@@ -71,7 +74,13 @@ static_assert(kPersistMaxBlocks <= kMaxSplitBlocks, "block table");
 // entry); the second word is the chunk.
 enum : uint32_t { kItGather = 0, kItScatter = 1, kItBc = 2, kItPrims = 3, kItFlux = 4, kItAsm = 5 };
 constexpr int kHaloChunk = 2048;  // slab elements per halo / BC item
-constexpr int kFluxCells = kSplitThreads;
+// A CTA is seven worker warps and one scheduler warp (see k_step_persist).
+constexpr int kWorkWarps = 7;
+constexpr int kWorkThreads = kWorkWarps * 32;
+constexpr int kCtaThreads = kWorkThreads + 32;
+static_assert(kCtaThreads == kSplitThreads, "launch bounds");
+constexpr int kFluxCells = kWorkThreads;       // cells per flux / primitive chunk (one per worker thread)
+constexpr int kAsmCellsP = kWorkWarps * 31;    // cells per assembly chunk (31 per worker warp)
 constexpr int kFlags = kRhsInvscd | kRhsViscous;
 // Waits give up after this many polls (64-256 ns apart: about a second)
 // unless the plan sets a limit.
@@ -98,12 +107,6 @@ struct PersistParams {
 };
 static_assert(sizeof(PersistParams) <= 32764, "kernel parameter space");
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
 __device__ __forceinline__ int ld_relaxed(const int* p) {
   int v;
   asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -118,14 +121,17 @@ __device__ __forceinline__ int flux_chunks_in_plane(int64_t si, int q) {
   return (int)(((int64_t)(q + 1) * si - 1) / kFluxCells - ((int64_t)q * si) / kFluxCells + 1);
 }
 
-// Thread 0: wait until *p >= target, polling at most the wait limit times
-// (0: give up at once; negative: the default).  Giving up records the error
+// Scheduler lane 0: wait until *p >= target (relaxed polls; the caller
+// fences once all waits of an item have passed).  once: a single look that
+// neither waits nor records anything.  Otherwise at most the wait limit polls
+// (0: give up at once; negative: the default); giving up records the error
 // and raises the abort flag.
-__device__ bool wait_ge(const PersistParams& P, const int* p, int target) {
+__device__ bool wait_ge(const PersistParams& P, const int* p, int target, bool once) {
   if (target <= 0) return true;
+  if (once) return ld_relaxed(p) >= target;
   const long long lim = P.wait_limit < 0 ? kDefaultWaitPolls : (long long)P.wait_limit;
   for (long long it = 0; it < lim; ++it) {
-    if (ld_acquire(p) >= target) return true;
+    if (ld_relaxed(p) >= target) return true;
     if (ld_relaxed(P.ctl + kCtlAbort) != 0) return false;
     __nanosleep(it < 64 ? 64 : 256);
   }
@@ -134,47 +140,51 @@ __device__ bool wait_ge(const PersistParams& P, const int* p, int target) {
   return false;
 }
 
-// Thread 0: the waits of an item (see the file comment).
-__device__ bool item_deps(const PersistParams& P, uint32_t code, int chunk) {
+// Scheduler lane 0: the waits of an item (see the file comment); once: one
+// look at each counter, nothing recorded.
+__device__ bool item_deps(const PersistParams& P, uint32_t code, int chunk, bool once) {
   const int type = code & 15, stage = (code >> 4) & 15, face = (code >> 8) & 15, idx = (int)(code >> 12);
   int* const ctl = P.ctl;
   switch (type) {
     case kItGather:
       return true;
     case kItScatter:
-      return wait_ge(P, ctl + kCtlGather, P.n_gather);
+      return wait_ge(P, ctl + kCtlGather, P.n_gather, once);
     case kItBc: {
       const int X = P.bcs[idx].block;
-      return wait_ge(P, ctl + kCtlScatter + X, P.scatter_total[X]) &&
-             wait_ge(P, ctl + kCtlBc + X, P.bc_prefix[X][face]);
+      return wait_ge(P, ctl + kCtlScatter + X, P.scatter_total[X], once) &&
+             wait_ge(P, ctl + kCtlBc + X, P.bc_prefix[X][face], once);
     }
     case kItPrims:
-      return wait_ge(P, ctl + kCtlScatter + idx, P.scatter_total[idx]) &&
-             wait_ge(P, ctl + kCtlBc + idx, P.bc_prefix[idx][6]);
+      return wait_ge(P, ctl + kCtlScatter + idx, P.scatter_total[idx], once) &&
+             wait_ge(P, ctl + kCtlBc + idx, P.bc_prefix[idx][6], once);
     case kItFlux: {
       const SplitBlock& B = P.tab.b[idx].blk;
       const int64_t N = (int64_t)B.ni * B.nj * B.nk;
-      if (stage == 1) return wait_ge(P, ctl + kCtlPrims + idx, (int)chunks_of(N, kFluxCells));
-      return wait_ge(P, ctl + kCtlAsm + kPersistMaxBlocks * (stage - 2) + idx, (int)chunks_of(N, kAsmCells));
+      if (stage == 1) return wait_ge(P, ctl + kCtlPrims + idx, (int)chunks_of(N, kFluxCells), once);
+      return wait_ge(P, ctl + kCtlAsm + kPersistMaxBlocks * (stage - 2) + idx, (int)chunks_of(N, kAsmCellsP), once);
     }
     default: {  // kItAsm
       const SplitBlock& B = P.tab.b[idx].blk;
       const int64_t si = (int64_t)B.nj * B.nk, N = si * B.ni;
-      const int64_t c0 = (int64_t)chunk * kAsmCells, c1 = min(c0 + kAsmCells, N) - 1;
+      const int64_t c0 = (int64_t)chunk * kAsmCellsP, c1 = min(c0 + kAsmCellsP, N) - 1;
       const int pl0 = (int)(c0 / si), pl1 = (int)(c1 / si);
       const int* f = ctl + kCtlFlux + (stage - 1) * P.total_planes + P.plane_base[idx];
       const int lo = max(pl0 - 1, 0), hi = min(pl1 + 1, B.ni - 1);
       for (int q = lo; q <= hi; ++q)
-        if (!wait_ge(P, f + q, flux_chunks_in_plane(si, q))) return false;
+        if (!wait_ge(P, f + q, flux_chunks_in_plane(si, q), once)) return false;
       // the viscous stencil's periodic i wrap
-      if (pl0 == 0 && hi < B.ni - 1 && !wait_ge(P, f + B.ni - 1, flux_chunks_in_plane(si, B.ni - 1))) return false;
-      if (pl1 == B.ni - 1 && lo > 0 && !wait_ge(P, f, flux_chunks_in_plane(si, 0))) return false;
+      if (pl0 == 0 && hi < B.ni - 1 && !wait_ge(P, f + B.ni - 1, flux_chunks_in_plane(si, B.ni - 1), once))
+        return false;
+      if (pl1 == B.ni - 1 && lo > 0 && !wait_ge(P, f, flux_chunks_in_plane(si, 0), once)) return false;
       return true;
     }
   }
 }
 
-// Thread 0, after the item's barrier: publish its completion.
+// Scheduler lane 0, once the workers are done with the item: publish its
+// completion (the workers' writes are ordered before this by the named
+// barrier; the fence makes them visible at device scope before the count).
 __device__ void item_done(const PersistParams& P, uint32_t code, int chunk) {
   const int type = code & 15, stage = (code >> 4) & 15, idx = (int)(code >> 12);
   int* const ctl = P.ctl;
@@ -196,7 +206,7 @@ __device__ void item_done(const PersistParams& P, uint32_t code, int chunk) {
   }
 }
 
-// All threads: the item's work.
+// Worker threads (threadIdx.x < kWorkThreads): the item's work.
 __device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code, int chunk) {
   const int type = code & 15, stage = (code >> 4) & 15, idx = (int)(code >> 12);
   if (type == kItFlux) {
@@ -214,7 +224,7 @@ __device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code,
       B.prim = d.blk.prim_next;
       B.prim_next = const_cast<void*>(d.blk.prim);
     }
-    asm_chunk<float, true, false>(d, B, (int64_t)chunk * kAsmCells, kFlags, stage, stage < 3 ? 1 : 0, P.gm1, P.R,
+    asm_chunk<float, true, false>(d, B, (int64_t)chunk * kAsmCellsP, kFlags, stage, stage < 3 ? 1 : 0, P.gm1, P.R,
                                   P.iR, P.ph);
   } else if (type == kItPrims) {
     const SplitBlock& B = P.tab.b[idx].blk;
@@ -226,7 +236,7 @@ __device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code,
     const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
     const int64_t NS = (int64_t)d.sn[0] * d.sn[1] * d.sn[2];
     const int64_t t1 = min((int64_t)(chunk + 1) * kHaloChunk, 5 * V);
-    for (int64_t t = (int64_t)chunk * kHaloChunk + threadIdx.x; t < t1; t += kSplitThreads) {
+    for (int64_t t = (int64_t)chunk * kHaloChunk + threadIdx.x; t < t1; t += kWorkThreads) {
       const int v = (int)(t / V);
       int a, b, c;
       hd::slab_coords(d, t - v * V, a, b, c);
@@ -238,7 +248,7 @@ __device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code,
     const int64_t V = (int64_t)d.ext[0] * d.ext[1] * d.ext[2];
     const int64_t NT = (int64_t)d.tn[0] * d.tn[1] * d.tn[2];
     const int64_t r1 = min((int64_t)(chunk + 1) * kHaloChunk, V);
-    for (int64_t r = (int64_t)chunk * kHaloChunk + threadIdx.x; r < r1; r += kSplitThreads) {
+    for (int64_t r = (int64_t)chunk * kHaloChunk + threadIdx.x; r < r1; r += kWorkThreads) {
       int a, b, c;
       hd::slab_coords(d, r, a, b, c);
       const int ti = d.tlo[0] + a, tj = d.tlo[1] + b, tk = d.tlo[2] + c;
@@ -257,7 +267,7 @@ __device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code,
     const int oa = ax == 0 ? 1 : 0, ob = ax == 2 ? 1 : 2;
     const int64_t V = (int64_t)P.ghost * d.n[oa] * d.n[ob];
     const int64_t r1 = min((int64_t)(chunk + 1) * kHaloChunk, V);
-    for (int64_t r = (int64_t)chunk * kHaloChunk + threadIdx.x; r < r1; r += kSplitThreads) {
+    for (int64_t r = (int64_t)chunk * kHaloChunk + threadIdx.x; r < r1; r += kWorkThreads) {
       const int y = (int)(r % d.n[ob]);
       const int x = (int)((r / d.n[ob]) % d.n[oa]);
       const int o = (int)(r / ((int64_t)d.n[ob] * d.n[oa]));
@@ -266,43 +276,105 @@ __device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code,
   }
 }
 
-// Thread 0 claims the next item while the CTA works on the current one, so
-// the claim's round trip to L2 overlaps the work.  Holding a claim on a later
-// item cannot deadlock: the earliest unfinished item is always some CTA's
-// current item (a CTA only claims after taking its current one), and it
-// waits only for earlier items, which are finished.
-template <int OCC>
-__global__ void __launch_bounds__(kSplitThreads, OCC) k_step_persist(const __grid_constant__ PersistParams P) {
-  // the current and the claimed next item live in shared memory (thread 0
-  // writes them), so nothing stays in registers across an item's work
-  __shared__ uint2 s_it, s_nxt_it;
-  __shared__ int s_valid, s_ok, s_nxt;
-  if (threadIdx.x == 0) {
-    const int i = atomicAdd(P.ctl + kCtlNext, 1);
-    s_nxt = i;
-    s_nxt_it = i < P.n_items ? P.items[i] : make_uint2(0u, 0u);
+// Named barriers of the hand-over between the scheduler warp and the workers:
+// slot b (two slots) is "full" when the scheduler has put an item there and
+// "empty" when the workers are done with it.
+__device__ __forceinline__ void named_sync(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kCtaThreads) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(kCtaThreads) : "memory");
+}
+constexpr int kBarFull = 1, kBarEmpty = 3;  // + slot
+
+// The scheduler warp (lane 0 does the memory operations, the warp takes part
+// in the barriers).  Per item k (slot k & 1): make sure the workers are done
+// with item k-2 and publish it, take the item claimed one round earlier and
+// claim the next, look at its counters once and, if they are not there yet,
+// first finish and publish item k-1 (it may be one of them) and then wait;
+// hand the item over.  So the claim, the waits and the publication overlap
+// the workers' compute, and the scheduler never waits for an item that it
+// holds back itself.
+__device__ void schedule(const PersistParams& P, uint2* slot, int* end) {
+  const unsigned all = 0xffffffffu;
+  const bool l0 = (threadIdx.x & 31) == 0;
+  int claim = 0;
+  if (l0) claim = atomicAdd(P.ctl + kCtlNext, 1);
+  claim = __shfl_sync(all, claim, 0);
+  uint2 held0 = make_uint2(0u, 0u), held1 = make_uint2(0u, 0u);  // the items in the slots (lane 0)
+  int done = -1;  // items handed out up to this one are published
+  for (int k = 0;; ++k) {
+    const int b = k & 1;
+    if (k >= 2 && done < k - 2) {
+      named_sync(kBarEmpty + b);
+      if (l0) item_done(P, b ? held1.x : held0.x, (int)(b ? held1.y : held0.y));
+      done = k - 2;
+    }
+    const int cur = claim;
+    int stop = 0;
+    uint2 it = make_uint2(0u, 0u);
+    if (l0) {
+      stop = cur >= P.n_items || ld_relaxed(P.ctl + kCtlAbort) != 0;
+      if (!stop) {
+        it = P.items[cur];
+        claim = atomicAdd(P.ctl + kCtlNext, 1);
+      }
+    }
+    stop = __shfl_sync(all, stop, 0);
+    claim = __shfl_sync(all, claim, 0);
+    if (!stop) {
+      int ready = l0 ? (int)item_deps(P, it.x, (int)it.y, true) : 0;
+      ready = __shfl_sync(all, ready, 0);
+      if (!ready) {
+        if (k >= 1 && done < k - 1) {
+          named_sync(kBarEmpty + (b ^ 1));
+          if (l0) item_done(P, b ? held0.x : held1.x, (int)(b ? held0.y : held1.y));
+          done = k - 1;
+        }
+        int ok = l0 ? (int)item_deps(P, it.x, (int)it.y, false) : 0;
+        stop = !__shfl_sync(all, ok, 0);
+      }
+      if (!stop && l0) __threadfence();  // acquire: what the counters published is visible from here on
+    }
+    if (l0) {
+      end[b] = stop;
+      slot[b] = it;
+      if (b) held1 = it;
+      else held0 = it;
+    }
+    __syncwarp();
+    named_arrive(kBarFull + b);
+    if (stop) {
+      // the workers finish item k-1 before they see the end mark
+      if (k >= 1 && done < k - 1) {
+        named_sync(kBarEmpty + (b ^ 1));
+        if (l0) item_done(P, b ? held0.x : held1.x, (int)(b ? held0.y : held1.y));
+      }
+      return;
+    }
   }
-  for (;;) {
-    if (threadIdx.x == 0) {
-      s_valid = s_nxt < P.n_items && ld_relaxed(P.ctl + kCtlAbort) == 0 ? 1 : 0;
-      s_it = s_nxt_it;
-    }
-    __syncthreads();
-    if (!s_valid) return;
-    const uint2 it = s_it;
-    if (threadIdx.x == 0) {
-      const int i = atomicAdd(P.ctl + kCtlNext, 1);
-      const bool ok = item_deps(P, it.x, (int)it.y);
-      if (ok) __threadfence();
-      s_ok = ok ? 1 : 0;
-      s_nxt = i;
-      s_nxt_it = i < P.n_items ? P.items[i] : make_uint2(0u, 0u);
-    }
-    __syncthreads();
-    if (!s_ok) return;
+}
+
+// One CTA = seven worker warps + one scheduler warp (warp 7).  Items are
+// handed over through two shared-memory slots behind named barriers.  Every
+// wait is bounded (the scheduler's counter polls) or ends when bounded work
+// ends (the barriers), and a wait that gives up raises the abort flag, on
+// which every scheduler hands its workers the end mark.
+template <int OCC>
+__global__ void __launch_bounds__(kCtaThreads, OCC) k_step_persist(const __grid_constant__ PersistParams P) {
+  __shared__ uint2 s_slot[2];
+  __shared__ int s_end[2];
+  if (threadIdx.x >= kWorkThreads) {
+    schedule(P, s_slot, s_end);
+    return;
+  }
+  for (int k = 0;; ++k) {
+    const int b = k & 1;
+    named_sync(kBarFull + b);
+    if (*(volatile int*)&s_end[b]) return;
+    const uint2 it = s_slot[b];
     item_work(P, it.x, (int)it.y);
-    __syncthreads();
-    if (threadIdx.x == 0) item_done(P, it.x, (int)it.y);
+    named_arrive(kBarEmpty + b);
   }
 }
 
@@ -336,11 +408,11 @@ void stage_items(const fj_block* blocks, int nblocks, int lag, std::vector<uint2
     for (int X = 0; X < nblocks; ++X) {
       const int64_t si = (int64_t)blocks[X].nj * blocks[X].nk, N = si * blocks[X].ni;
       const int ni = blocks[X].ni;
-      const int nF = (int)chunks_of(N, kFluxCells), nA = (int)chunks_of(N, kAsmCells);
+      const int nF = (int)chunks_of(N, kFluxCells), nA = (int)chunks_of(N, kAsmCellsP);
       // slot[a]: the flux chunk after which assembly chunk a is taken
       std::vector<std::vector<int>> after(nF);
       for (int a = 0; a < nA; ++a) {
-        const int64_t c0 = (int64_t)a * kAsmCells, c1 = std::min<int64_t>(c0 + kAsmCells, N) - 1;
+        const int64_t c0 = (int64_t)a * kAsmCellsP, c1 = std::min<int64_t>(c0 + kAsmCellsP, N) - 1;
         const int pl0 = (int)(c0 / si), pl1 = (int)(c1 / si);
         // the last flux chunk of plane min(pl1 + 1, ni - 1); all of them for plane 0 (wrap)
         const int need_plane = std::min(pl1 + 1, ni - 1);
