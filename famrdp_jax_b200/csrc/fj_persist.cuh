@@ -20,12 +20,15 @@ constexpr int kPersistMaxBlocks = 64;
 
 // Launch shapes (FJ_NUM_PERSIST_SHAPES): resident CTAs per SM and the lag of
 // the assembly chunks behind the flux chunks they read, in units of half the
-// resident CTAs (about the flux chunks in flight).
+// resident CTAs (about the flux chunks in flight); a negative lag mixes each
+// sweep's assembly chunks into the next sweep's (another block's) flux chunks.
 struct PersistShape {
   int occ;
   double lag_scale;
 };
-constexpr PersistShape kPersistShapes[] = {{4, 4.0}, {3, 4.0}, {4, 1e6}, {3, 1e6}};
+// Shape 0 (each sweep's assembly chunks after all its flux chunks) measured
+// fastest: any mixing of the two kinds of chunks made the step slower.
+constexpr PersistShape kPersistShapes[] = {{4, 1e6}, {3, 1e6}, {4, -1.0}, {4, 3.0}};
 static_assert(sizeof(kPersistShapes) / sizeof(kPersistShapes[0]) == FJ_NUM_PERSIST_SHAPES, "shape table");
 
 // Host-side plan data of the persistent step: the work-list and the
@@ -42,6 +45,7 @@ struct PersistPlan {
   int n_gather = 0;        // gather items (the scatters wait for all of them)
   std::vector<uint2> head;  // the halo, BC and primitive items (the part of the list the shape leaves alone)
   std::vector<int> scatter_total, bc_prefix, plane_base;  // per block (bc_prefix: 7 per block)
+  std::vector<int> link_tgt, bc_block;  // per link its target block, per boundary entry its block
   int total_planes = 0;
   size_t split_bytes = 0;  // offset of the halo slabs in the tail (after the intermediates)
   int grid = 0;            // resident CTAs (occupancy x SMs)
@@ -63,7 +67,8 @@ size_t persist_tail_bytes(const fj_block* blocks, int nblocks, const fj_link* li
 bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
                    const fj_bc* bcs, int nbcs, const fj_params* p, PersistPlan& pp, std::string* why);
 // Rebuilds the work-list with another launch shape: occ CTAs per SM (3 or 4)
-// and lag_scale (the assembly lag in units of half the resident CTAs).
+// and lag_scale (see kPersistShapes).  Refuses (false) a list in which an
+// item would wait for one behind it.
 bool persist_reshape(PersistPlan& pp, const fj_block* blocks, int nblocks, int occ, double lag_scale);
 // One step: blocks[b].q is the step's start state (written in place by the
 // halo and BC items), q1s / q2s / q_out the stage results.  tail: the plan

@@ -62,6 +62,29 @@ struct Cell {
   int ni, nj, nk;
 };
 
+// The pointers of a block that change from stage to stage: the stage input,
+// the stage result, the input's primitive records and where the result's go.
+// The split kernels read them from the block table where they are used
+// (TablePtrs); the persistent step passes them alongside it (StagePtrs).
+struct StagePtrs {
+  const double* q_;
+  double* out_;
+  const void* prim_;
+  void* prim_next_;
+  __device__ __forceinline__ const double* q() const { return q_; }
+  __device__ __forceinline__ double* out() const { return out_; }
+  __device__ __forceinline__ const void* prim() const { return prim_; }
+  __device__ __forceinline__ void* prim_next() const { return prim_next_; }
+};
+
+struct TablePtrs {
+  const SplitBlock& B;
+  __device__ __forceinline__ const double* q() const { return B.q; }
+  __device__ __forceinline__ double* out() const { return B.out; }
+  __device__ __forceinline__ const void* prim() const { return B.prim; }
+  __device__ __forceinline__ void* prim_next() const { return B.prim_next; }
+};
+
 // Coordinates of cell c of block d; false past the block's end.
 __device__ __forceinline__ bool decode_cell(const Dev& d, int64_t c, Cell& x) {
   const SplitBlock& B = d.blk;
@@ -360,8 +383,9 @@ struct GlobalSrc {
 // solver/step.py:45-53) from the intermediates Src provides.
 // fk_m / fk_p: the k faces c-1 | c and c | c+1 (the flux records hold only the
 // i and j faces); kk / gcl: the metric record of c, loaded by the caller.
-template <typename T, bool K_AOS, class Src>
-__device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x, const Src& src, int flags,
+template <typename T, bool K_AOS, class Src, class SP>
+__device__ __forceinline__ void assemble_cell(const SplitBlock& B, const SP& sp, const Cell& x, const Src& src,
+                                              int flags,
                                               int stage, int next_prims, double gm1, double R, double iR,
                                               double ph_p_ref, const T fk_m[5], const T fk_p[5], const T kk[9],
                                               const T gcl[3]) {
@@ -442,14 +466,14 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
 #pragma unroll
     for (int e = 0; e < 4; ++e) r[e + 1] += (double)acc[e];
   }
-  double* out = B.out + c;
+  double* out = sp.out() + c;
   if (stage == 0) {
 #pragma unroll
     for (int v = 0; v < 5; ++v) out[(size_t)v * N] = r[v];
   } else {
     const double ca = stage == 2 ? 0.75 : 1.0 / 3.0;
     const double cb = stage == 2 ? 0.25 : 2.0 / 3.0;
-    const double* q = B.q + c;
+    const double* q = sp.q() + c;
     const double* q0 = B.q0 + c;
     double qn[5];
 #pragma unroll
@@ -462,7 +486,7 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
       double pv[6];
       prims_of(qn, gm1, R, iR, pv);
       const T rec[kRecP] = {(T)pv[0], (T)pv[1], (T)pv[2], (T)pv[3], (T)(pv[4] - ph_p_ref), (T)pv[5], T(0), T(0)};
-      st_rec<T, kRecP>((T*)B.prim_next + (size_t)c * kRecP, rec);
+      st_rec<T, kRecP>((T*)sp.prim_next() + (size_t)c * kRecP, rec);
     }
   }
 }
@@ -472,9 +496,9 @@ __device__ __forceinline__ void assemble_cell(const SplitBlock& B, const Cell& x
 // The k face c-1 | c (rhs/invscd.py:62-100) from the stage input's primitive
 // records of c-2 .. c+1, the k row of the metrics of c-1 and kr, that of c.
 template <typename T, bool K_AOS, bool NC = true>
-__device__ __forceinline__ void k_face_left(const SplitBlock& B, int32_t N, int32_t c, const T kr[3],
-                                            const Phys& ph, T F[5]) {
-  const T* __restrict__ P = (const T*)B.prim;
+__device__ __forceinline__ void k_face_left(const SplitBlock& B, const void* prim, int32_t N, int32_t c,
+                                            const T kr[3], const Phys& ph, T F[5]) {
+  const T* __restrict__ P = (const T*)prim;
   const Cell6<T> a0 = load_cell<T, NC>(P, c - 2), a1 = load_cell<T, NC>(P, c - 1), a2 = load_cell<T, NC>(P, c),
                  a3 = load_cell<T, NC>(P, c + 1);
   T kl[3];
@@ -518,12 +542,13 @@ __device__ __forceinline__ void prims_cell(const SplitBlock& B, int32_t c, doubl
 // jnp.roll) and the Roe faces c | c+e_i and c | c+e_j (rhs/invscd.py:53-100)
 // for c_a in [1, n_a-3].
 template <typename T, bool K_AOS, bool NC>
-__device__ __forceinline__ void flux_cell(const SplitBlock& B, const Cell& x, const Phys& ph, int flags) {
+__device__ __forceinline__ void flux_cell(const SplitBlock& B, const void* prim, const Cell& x, const Phys& ph,
+                                          int flags) {
   using M = FastMath<T>;
   // 32-bit cell indices: kRecF N < 2^31 is checked on the host
   const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
   const int32_t si = x.nj * x.nk, sj = x.nk;
-  const T* __restrict__ P = (const T*)B.prim;
+  const T* __restrict__ P = (const T*)prim;
   const bool vis = (flags & kRhsViscous) != 0, inv = (flags & kRhsInvscd) != 0;
 
   // neighbour offsets with the padded-array wrap (jnp.roll) for the viscous
@@ -607,9 +632,10 @@ __device__ __forceinline__ void flux_cell(const SplitBlock& B, const Cell& x, co
 // barrier is needed; lane 31's cell is the next warp's first, for which it
 // only supplies the face.  With next_prims, also writes the primitives of the
 // stage result (the next stage's input).
-template <typename T, bool K_AOS, bool NC>
-__device__ __forceinline__ void asm_chunk(const Dev& d, const SplitBlock& B, int64_t c0, int flags, int stage,
+template <typename T, bool K_AOS, bool NC, class SP>
+__device__ __forceinline__ void asm_chunk(const Dev& d, const SP& sp, int64_t c0, int flags, int stage,
                                           int next_prims, double gm1, double R, double iR, const Phys& ph) {
+  const SplitBlock& B = d.blk;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
   const int64_t c = c0 + warp * 31 + lane;
@@ -632,11 +658,11 @@ __device__ __forceinline__ void asm_chunk(const Dev& d, const SplitBlock& B, int
   T fl[5] = {T(0), T(0), T(0), T(0), T(0)}, fr[5];
   // face c-1 | c exists for k-1 in [1, nk-3]
   if ((flags & kRhsInvscd) && alive && x.k >= 2 && x.k <= x.nk - 2)
-    k_face_left<T, K_AOS, NC>(B, (int32_t)N, (int32_t)c, kk + 6, ph, fl);
+    k_face_left<T, K_AOS, NC>(B, sp.prim(), (int32_t)N, (int32_t)c, kk + 6, ph, fl);
 #pragma unroll
   for (int v = 0; v < 5; ++v) fr[v] = __shfl_down_sync(0xffffffffu, fl[v], 1);
   if (lane == 31 || !alive) return;
-  assemble_cell<T, K_AOS>(B, x, src, flags, stage, next_prims, gm1, R, iR, K_AOS ? ph.p_ref : 0.0, fl, fr, kk,
+  assemble_cell<T, K_AOS>(B, sp, x, src, flags, stage, next_prims, gm1, R, iR, K_AOS ? ph.p_ref : 0.0, fl, fr, kk,
                           gcl);
 }
 

@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table
   grid_dep_wait();
   Cell x;
   if (!decode(tab.b[b], blockIdx.x, x)) return;
-  flux_cell<T, K_AOS, true>(tab.b[b].blk, x, ph, flags);
+  flux_cell<T, K_AOS, true>(tab.b[b].blk, tab.b[b].blk.prim, x, ph, flags);
 }
 
 template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
@@ -74,8 +74,8 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
   const SplitBlock& B = d.blk;
   if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
   grid_dep_wait();
-  asm_chunk<T, K_AOS, true>(d, B, (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells, flags, stage, next_prims,
-                            gm1, R, iR, ph);
+  asm_chunk<T, K_AOS, true>(d, TablePtrs{B}, (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells, flags, stage,
+                            next_prims, gm1, R, iR, ph);
 }
 
 // ---- field-major variant (the FP64 path) ----------------------------------

@@ -121,88 +121,131 @@ __device__ __forceinline__ int flux_chunks_in_plane(int64_t si, int q) {
   return (int)(((int64_t)(q + 1) * si - 1) / kFluxCells - ((int64_t)q * si) / kFluxCells + 1);
 }
 
-// Scheduler lane 0: wait until *p >= target (relaxed polls; the caller
-// fences once all waits of an item have passed).  once: a single look that
-// neither waits nor records anything.  Otherwise at most the wait limit polls
-// (0: give up at once; negative: the default); giving up records the error
-// and raises the abort flag.
-__device__ bool wait_ge(const PersistParams& P, const int* p, int target, bool once) {
-  if (target <= 0) return true;
-  if (once) return ld_relaxed(p) >= target;
-  const long long lim = P.wait_limit < 0 ? kDefaultWaitPolls : (long long)P.wait_limit;
-  for (long long it = 0; it < lim; ++it) {
-    if (ld_relaxed(p) >= target) return true;
-    if (ld_relaxed(P.ctl + kCtlAbort) != 0) return false;
-    __nanosleep(it < 64 ? 64 : 256);
-  }
-  atomicOr(P.ctl + kCtlErr, 1);
-  atomicExch(P.ctl + kCtlAbort, 1);
-  return false;
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+__device__ __forceinline__ void red_add(int* p, int v) {
+  asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Scheduler lane 0: the waits of an item (see the file comment); once: one
-// look at each counter, nothing recorded.
-__device__ bool item_deps(const PersistParams& P, uint32_t code, int chunk, bool once) {
+// The completion counters an item waits for (see the file comment), as
+// (counter, target) pairs 0 .. n-1; dep_pair returns n and, for i < n, pair i.
+__device__ int dep_pair(const PersistParams& P, uint32_t code, int chunk, int i, const int*& p, int& target) {
   const int type = code & 15, stage = (code >> 4) & 15, face = (code >> 8) & 15, idx = (int)(code >> 12);
-  int* const ctl = P.ctl;
+  const int* const ctl = P.ctl;
+  p = nullptr;
+  target = 0;
   switch (type) {
     case kItGather:
-      return true;
+      return 0;
     case kItScatter:
-      return wait_ge(P, ctl + kCtlGather, P.n_gather, once);
+      if (i == 0) p = ctl + kCtlGather, target = P.n_gather;
+      return 1;
     case kItBc: {
       const int X = P.bcs[idx].block;
-      return wait_ge(P, ctl + kCtlScatter + X, P.scatter_total[X], once) &&
-             wait_ge(P, ctl + kCtlBc + X, P.bc_prefix[X][face], once);
+      if (i == 0) p = ctl + kCtlScatter + X, target = P.scatter_total[X];
+      if (i == 1) p = ctl + kCtlBc + X, target = P.bc_prefix[X][face];
+      return 2;
     }
     case kItPrims:
-      return wait_ge(P, ctl + kCtlScatter + idx, P.scatter_total[idx], once) &&
-             wait_ge(P, ctl + kCtlBc + idx, P.bc_prefix[idx][6], once);
+      if (i == 0) p = ctl + kCtlScatter + idx, target = P.scatter_total[idx];
+      if (i == 1) p = ctl + kCtlBc + idx, target = P.bc_prefix[idx][6];
+      return 2;
     case kItFlux: {
       const SplitBlock& B = P.tab.b[idx].blk;
       const int64_t N = (int64_t)B.ni * B.nj * B.nk;
-      if (stage == 1) return wait_ge(P, ctl + kCtlPrims + idx, (int)chunks_of(N, kFluxCells), once);
-      return wait_ge(P, ctl + kCtlAsm + kPersistMaxBlocks * (stage - 2) + idx, (int)chunks_of(N, kAsmCellsP), once);
+      if (i == 0) {
+        if (stage == 1) p = ctl + kCtlPrims + idx, target = (int)chunks_of(N, kFluxCells);
+        else p = ctl + kCtlAsm + kPersistMaxBlocks * (stage - 2) + idx, target = (int)chunks_of(N, kAsmCellsP);
+      }
+      return 1;
     }
-    default: {  // kItAsm
+    default: {  // kItAsm: the flux planes lo .. hi, then the periodic i wrap's far plane
       const SplitBlock& B = P.tab.b[idx].blk;
       const int64_t si = (int64_t)B.nj * B.nk, N = si * B.ni;
       const int64_t c0 = (int64_t)chunk * kAsmCellsP, c1 = min(c0 + kAsmCellsP, N) - 1;
       const int pl0 = (int)(c0 / si), pl1 = (int)(c1 / si);
-      const int* f = ctl + kCtlFlux + (stage - 1) * P.total_planes + P.plane_base[idx];
       const int lo = max(pl0 - 1, 0), hi = min(pl1 + 1, B.ni - 1);
-      for (int q = lo; q <= hi; ++q)
-        if (!wait_ge(P, f + q, flux_chunks_in_plane(si, q), once)) return false;
-      // the viscous stencil's periodic i wrap
-      if (pl0 == 0 && hi < B.ni - 1 && !wait_ge(P, f + B.ni - 1, flux_chunks_in_plane(si, B.ni - 1), once))
-        return false;
-      if (pl1 == B.ni - 1 && lo > 0 && !wait_ge(P, f, flux_chunks_in_plane(si, 0), once)) return false;
-      return true;
+      const bool wrap_hi = pl0 == 0 && hi < B.ni - 1, wrap_lo = pl1 == B.ni - 1 && lo > 0;
+      const int n = hi - lo + 1 + (wrap_hi ? 1 : 0) + (wrap_lo ? 1 : 0);
+      int q = -1;
+      if (i <= hi - lo) q = lo + i;
+      else if (i == hi - lo + 1) q = wrap_hi ? B.ni - 1 : 0;
+      else if (i == hi - lo + 2) q = 0;
+      if (q >= 0 && i < n) {
+        p = ctl + kCtlFlux + (stage - 1) * P.total_planes + P.plane_base[idx] + q;
+        target = flux_chunks_in_plane(si, q);
+      }
+      return n;
     }
   }
 }
 
+// Scheduler warp: whether every counter of the item has reached its target,
+// the lanes polling the pairs in parallel (relaxed loads; the caller fences
+// once they have).  once: a single look that neither waits nor records
+// anything.  Otherwise each lane polls at most the wait limit times (0: give
+// up at once if there is anything to wait for; negative: the default);
+// giving up records the error and raises the abort flag, and an abort raised
+// elsewhere ends the wait as well.
+__device__ bool deps_warp(const PersistParams& P, uint2 it, bool once) {
+  const unsigned all = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int* p0;
+  int t0;
+  const int n = dep_pair(P, it.x, (int)it.y, 0, p0, t0);
+  const long long lim = P.wait_limit < 0 ? kDefaultWaitPolls : (long long)P.wait_limit;
+  for (int base = 0; base < n; base += 32) {
+    const int* p = nullptr;
+    int target = 0;
+    if (base + lane < n) dep_pair(P, it.x, (int)it.y, base + lane, p, target);
+    const bool need = p != nullptr && target > 0;
+    bool ok = !need || ld_relaxed(p) >= target;
+    if (once) {
+      if (!__all_sync(all, ok)) return false;
+      continue;
+    }
+    if (lim == 0 && __any_sync(all, need)) ok = false;  // give up at once
+    for (long long poll = 0; !__all_sync(all, ok); ++poll) {
+      int give_up = poll >= lim;
+      if (lane == 0 && !give_up && ld_relaxed(P.ctl + kCtlAbort) != 0) give_up = 2;
+      give_up = __shfl_sync(all, give_up, 0);
+      if (give_up) {
+        if (lane == 0 && give_up == 1) {
+          atomicOr(P.ctl + kCtlErr, 1);
+          atomicExch(P.ctl + kCtlAbort, 1);
+        }
+        return false;
+      }
+      __nanosleep(poll < 64 ? 64 : 256);
+      if (!ok) ok = ld_relaxed(p) >= target;
+    }
+  }
+  return true;
+}
+
 // Scheduler lane 0, once the workers are done with the item: publish its
 // completion (the workers' writes are ordered before this by the named
-// barrier; the fence makes them visible at device scope before the count).
-__device__ void item_done(const PersistParams& P, uint32_t code, int chunk) {
+// barrier; the fence makes them visible at device scope before the counts).
+__device__ void item_done(const PersistParams& P, uint2 it) {
+  const uint32_t code = it.x;
+  const int chunk = (int)it.y;
   const int type = code & 15, stage = (code >> 4) & 15, idx = (int)(code >> 12);
   int* const ctl = P.ctl;
-  __threadfence();
+  fence_acq_rel();
   switch (type) {
-    case kItGather: atomicAdd(ctl + kCtlGather, 1); break;
-    case kItScatter: atomicAdd(ctl + kCtlScatter + P.links[idx].tgt_block, 1); break;
-    case kItBc: atomicAdd(ctl + kCtlBc + P.bcs[idx].block, 1); break;
-    case kItPrims: atomicAdd(ctl + kCtlPrims + idx, 1); break;
+    case kItGather: red_add(ctl + kCtlGather, 1); break;
+    case kItScatter: red_add(ctl + kCtlScatter + P.links[idx].tgt_block, 1); break;
+    case kItBc: red_add(ctl + kCtlBc + P.bcs[idx].block, 1); break;
+    case kItPrims: red_add(ctl + kCtlPrims + idx, 1); break;
     case kItFlux: {
       const SplitBlock& B = P.tab.b[idx].blk;
       const int64_t si = (int64_t)B.nj * B.nk, N = si * B.ni;
       const int64_t c0 = (int64_t)chunk * kFluxCells, c1 = min(c0 + kFluxCells, N) - 1;
       int* f = ctl + kCtlFlux + (stage - 1) * P.total_planes + P.plane_base[idx];
-      for (int q = (int)(c0 / si); q <= (int)(c1 / si); ++q) atomicAdd(f + q, 1);
+      for (int q = (int)(c0 / si); q <= (int)(c1 / si); ++q) red_add(f + q, 1);
       break;
     }
-    default: atomicAdd(ctl + kCtlAsm + kPersistMaxBlocks * (stage - 1) + idx, 1);
+    default: red_add(ctl + kCtlAsm + kPersistMaxBlocks * (stage - 1) + idx, 1);
   }
 }
 
@@ -211,20 +254,17 @@ __device__ __forceinline__ void item_work(const PersistParams& P, uint32_t code,
   const int type = code & 15, stage = (code >> 4) & 15, idx = (int)(code >> 12);
   if (type == kItFlux) {
     const Dev& d = P.tab.b[idx];
-    SplitBlock B = d.blk;
-    if (stage == 2) B.prim = d.blk.prim_next;  // the primitives alternate between two buffers
+    // the primitives alternate between two buffers
+    const void* prim = stage == 2 ? d.blk.prim_next : d.blk.prim;
     Cell x;
-    if (decode_cell(d, (int64_t)chunk * kFluxCells + threadIdx.x, x)) flux_cell<float, true, false>(B, x, P.ph, kFlags);
+    if (decode_cell(d, (int64_t)chunk * kFluxCells + threadIdx.x, x))
+      flux_cell<float, true, false>(d.blk, prim, x, P.ph, kFlags);
   } else if (type == kItAsm) {
     const Dev& d = P.tab.b[idx];
-    SplitBlock B = d.blk;
-    B.q = stage == 1 ? d.blk.q : P.qs[idx][stage - 2];
-    B.out = P.qs[idx][stage - 1];
-    if (stage == 2) {
-      B.prim = d.blk.prim_next;
-      B.prim_next = const_cast<void*>(d.blk.prim);
-    }
-    asm_chunk<float, true, false>(d, B, (int64_t)chunk * kAsmCellsP, kFlags, stage, stage < 3 ? 1 : 0, P.gm1, P.R,
+    const StagePtrs sp{stage == 1 ? d.blk.q : P.qs[idx][stage - 2], P.qs[idx][stage - 1],
+                       stage == 2 ? d.blk.prim_next : d.blk.prim,
+                       stage == 2 ? const_cast<void*>(d.blk.prim) : d.blk.prim_next};
+    asm_chunk<float, true, false>(d, sp, (int64_t)chunk * kAsmCellsP, kFlags, stage, stage < 3 ? 1 : 0, P.gm1, P.R,
                                   P.iR, P.ph);
   } else if (type == kItPrims) {
     const SplitBlock& B = P.tab.b[idx].blk;
@@ -287,70 +327,101 @@ __device__ __forceinline__ void named_arrive(int id) {
 }
 constexpr int kBarFull = 1, kBarEmpty = 3;  // + slot
 
-// The scheduler warp (lane 0 does the memory operations, the warp takes part
-// in the barriers).  Per item k (slot k & 1): make sure the workers are done
-// with item k-2 and publish it, take the item claimed one round earlier and
-// claim the next, look at its counters once and, if they are not there yet,
-// first finish and publish item k-1 (it may be one of them) and then wait;
-// hand the item over.  So the claim, the waits and the publication overlap
+// The scheduler warp.  Lane 0 keeps two claims ahead of the item in hand
+// (the next item's list entry already loaded, the one after it claimed), so
+// the claim's atomic and the entry's load complete while the workers compute.
+// Per item k (slot k & 1): make sure the workers are done with item k-2 (its
+// slot is reused); look at the item's counters once and, if they are not all
+// there, first publish every item handed out before (the one the workers are
+// on may be among those waited for) and then wait; hand the item over; then
+// publish item k-2.  So the claims, the waits and the publication overlap
 // the workers' compute, and the scheduler never waits for an item that it
 // holds back itself.
 __device__ void schedule(const PersistParams& P, uint2* slot, int* end) {
   const unsigned all = 0xffffffffu;
-  const bool l0 = (threadIdx.x & 31) == 0;
-  int claim = 0;
-  if (l0) claim = atomicAdd(P.ctl + kCtlNext, 1);
-  claim = __shfl_sync(all, claim, 0);
+  const int lane = threadIdx.x & 31;
+  const bool l0 = lane == 0;
+  int c1 = 0, c2 = 0, aborted = 0;  // lane 0: the next item's index and the one after it
+  uint2 it1 = make_uint2(0u, 0u);   // lane 0: the next item's entry
+  if (l0) {
+    c1 = atomicAdd(P.ctl + kCtlNext, 1);
+    c2 = atomicAdd(P.ctl + kCtlNext, 1);
+    if (c1 < P.n_items) it1 = P.items[c1];
+  }
   uint2 held0 = make_uint2(0u, 0u), held1 = make_uint2(0u, 0u);  // the items in the slots (lane 0)
-  int done = -1;  // items handed out up to this one are published
+  uint2 pend_it = make_uint2(0u, 0u);
+  bool pend = false;  // the workers are done with pend_it, its completion is not published yet
+  int done = -1;      // the workers are done with the items handed out up to this one
   for (int k = 0;; ++k) {
     const int b = k & 1;
     if (k >= 2 && done < k - 2) {
       named_sync(kBarEmpty + b);
-      if (l0) item_done(P, b ? held1.x : held0.x, (int)(b ? held1.y : held0.y));
+      pend = true;
+      pend_it = b ? held1 : held0;
       done = k - 2;
     }
-    const int cur = claim;
-    int stop = 0;
+    int cur = 0;
     uint2 it = make_uint2(0u, 0u);
     if (l0) {
-      stop = cur >= P.n_items || ld_relaxed(P.ctl + kCtlAbort) != 0;
-      if (!stop) {
-        it = P.items[cur];
-        claim = atomicAdd(P.ctl + kCtlNext, 1);
+      cur = c1;
+      it = it1;
+      // advance the claims: the entry after this one, and a new claim
+      c1 = c2;
+      if (cur < P.n_items) {
+        if (c1 < P.n_items) it1 = P.items[c1];
+        c2 = atomicAdd(P.ctl + kCtlNext, 1);
       }
     }
-    stop = __shfl_sync(all, stop, 0);
-    claim = __shfl_sync(all, claim, 0);
+    cur = __shfl_sync(all, cur, 0);
+    it = make_uint2(__shfl_sync(all, it.x, 0), __shfl_sync(all, it.y, 0));
+    bool stop = cur >= P.n_items || aborted;
     if (!stop) {
-      int ready = l0 ? (int)item_deps(P, it.x, (int)it.y, true) : 0;
-      ready = __shfl_sync(all, ready, 0);
+      // a few looks while the workers are still on item k-1, before giving
+      // up the overlap and publishing it
+      bool ready = P.wait_limit != 0 && deps_warp(P, it, true);
+      for (int look = 0; look < 12 && !ready && P.wait_limit != 0; ++look) {
+        __nanosleep(128);
+        ready = deps_warp(P, it, true);
+      }
       if (!ready) {
+        if (pend) {
+          if (l0) item_done(P, pend_it);
+          pend = false;
+        }
         if (k >= 1 && done < k - 1) {
           named_sync(kBarEmpty + (b ^ 1));
-          if (l0) item_done(P, b ? held0.x : held1.x, (int)(b ? held0.y : held1.y));
+          if (l0) item_done(P, b ? held0 : held1);
           done = k - 1;
         }
-        int ok = l0 ? (int)item_deps(P, it.x, (int)it.y, false) : 0;
-        stop = !__shfl_sync(all, ok, 0);
+        stop = !deps_warp(P, it, false);
       }
-      if (!stop && l0) __threadfence();  // acquire: what the counters published is visible from here on
+      if (!stop && l0) fence_acq_rel();  // acquire: what the counters published is visible from here on
     }
     if (l0) {
-      end[b] = stop;
+      end[b] = stop ? 1 : 0;
       slot[b] = it;
       if (b) held1 = it;
       else held0 = it;
     }
     __syncwarp();
     named_arrive(kBarFull + b);
+    if (pend) {
+      if (l0) item_done(P, pend_it);
+      pend = false;
+    }
     if (stop) {
       // the workers finish item k-1 before they see the end mark
       if (k >= 1 && done < k - 1) {
         named_sync(kBarEmpty + (b ^ 1));
-        if (l0) item_done(P, b ? held0.x : held1.x, (int)(b ? held0.y : held1.y));
+        if (l0) item_done(P, b ? held0 : held1);
       }
       return;
+    }
+    // an abort raised elsewhere ends this CTA at its next item (looked at
+    // every 16 items, and by every wait)
+    if ((k & 15) == 15) {
+      if (l0) aborted = ld_relaxed(P.ctl + kCtlAbort);
+      aborted = __shfl_sync(all, aborted, 0);
     }
   }
 }
@@ -427,6 +498,101 @@ void stage_items(const fj_block* blocks, int nblocks, int lag, std::vector<uint2
     }
 }
 
+// The stage part of the work-list with the mixing across blocks: the sweeps
+// (stage, block) in stage-major order, each sweep's flux chunks in order and,
+// spread evenly among them, the previous sweep's assembly chunks, which come
+// after all of that sweep's flux chunks (so an assembly chunk never waits on
+// a flux chunk near it in the list).  A sweep whose next sweep is the same
+// block's next stage (one block) keeps its assembly chunks to itself, after
+// its flux chunks: that stage's flux chunks wait for all of them.
+void stage_items_across(const fj_block* blocks, int nblocks, std::vector<uint2>& out) {
+  int prev_X = -1, prev_s = 0, prev_nA = 0;
+  auto flush_prev = [&]() {
+    for (int a = 0; a < prev_nA; ++a) out.push_back(make_uint2(item_code(kItAsm, prev_s, 0, prev_X), (unsigned)a));
+    prev_nA = 0;
+  };
+  for (int s = 1; s <= 3; ++s)
+    for (int X = 0; X < nblocks; ++X) {
+      const int64_t N = (int64_t)blocks[X].ni * blocks[X].nj * blocks[X].nk;
+      const int nF = (int)chunks_of(N, kFluxCells), nA = (int)chunks_of(N, kAsmCellsP);
+      if (prev_nA > 0 && prev_X == X) flush_prev();  // one block: its next stage waits for all of them
+      // the previous sweep's assembly chunk a follows flux chunk floor(a nF / nA)
+      int a = 0;
+      for (int f = 0; f < nF; ++f) {
+        out.push_back(make_uint2(item_code(kItFlux, s, 0, X), (unsigned)f));
+        for (; a < prev_nA && (int64_t)a * nF / prev_nA <= f; ++a)
+          out.push_back(make_uint2(item_code(kItAsm, prev_s, 0, prev_X), (unsigned)a));
+      }
+      for (; a < prev_nA; ++a) out.push_back(make_uint2(item_code(kItAsm, prev_s, 0, prev_X), (unsigned)a));
+      prev_X = X;
+      prev_s = s;
+      prev_nA = nA;
+    }
+  flush_prev();
+}
+
+// Whether every item of the list waits only for items ahead of it: in a
+// sequential run, item by item, the counters must already have reached every
+// target an item waits for (the host restatement of dep_pair and item_done).
+// A list that passes cannot deadlock the launch.
+bool list_is_ordered(const PersistPlan& pp, const fj_block* blocks, int nblocks, const std::vector<uint2>& items) {
+  std::vector<int64_t> scatter(nblocks, 0), bc(nblocks, 0), prims(nblocks, 0), asmc(3 * nblocks, 0),
+      flux(3 * (size_t)pp.total_planes, 0);
+  int64_t gather = 0;
+  auto chunks_in_plane = [](int64_t si, int q) {
+    return ((int64_t)(q + 1) * si - 1) / kFluxCells - ((int64_t)q * si) / kFluxCells + 1;
+  };
+  for (const uint2& it : items) {
+    const uint32_t code = it.x;
+    const int type = code & 15, stage = (code >> 4) & 15, face = (code >> 8) & 15, idx = (int)(code >> 12);
+    const int64_t chunk = it.y;
+    switch (type) {
+      case kItGather:
+        ++gather;
+        break;
+      case kItScatter:
+        if (gather < pp.n_gather) return false;
+        ++scatter[pp.link_tgt[idx]];
+        break;
+      case kItBc: {
+        const int X = pp.bc_block[idx];
+        if (scatter[X] < pp.scatter_total[X] || bc[X] < pp.bc_prefix[X * 7 + face]) return false;
+        ++bc[X];
+        break;
+      }
+      case kItPrims:
+        if (scatter[idx] < pp.scatter_total[idx] || bc[idx] < pp.bc_prefix[idx * 7 + 6]) return false;
+        ++prims[idx];
+        break;
+      case kItFlux: {
+        const int64_t si = (int64_t)blocks[idx].nj * blocks[idx].nk, N = si * blocks[idx].ni;
+        if (stage == 1 ? prims[idx] < chunks_of(N, kFluxCells)
+                       : asmc[(stage - 2) * nblocks + idx] < chunks_of(N, kAsmCellsP))
+          return false;
+        const int64_t c0 = chunk * kFluxCells, c1 = std::min<int64_t>(c0 + kFluxCells, N) - 1;
+        for (int64_t q = c0 / si; q <= c1 / si; ++q) ++flux[(stage - 1) * (size_t)pp.total_planes + pp.plane_base[idx] + q];
+        break;
+      }
+      case kItAsm: {
+        const int ni = blocks[idx].ni;
+        const int64_t si = (int64_t)blocks[idx].nj * blocks[idx].nk, N = si * ni;
+        const int64_t c0 = chunk * kAsmCellsP, c1 = std::min<int64_t>(c0 + kAsmCellsP, N) - 1;
+        const int pl0 = (int)(c0 / si), pl1 = (int)(c1 / si);
+        const int64_t* f = flux.data() + (stage - 1) * (size_t)pp.total_planes + pp.plane_base[idx];
+        for (int q = std::max(pl0 - 1, 0); q <= std::min(pl1 + 1, ni - 1); ++q)
+          if (f[q] < chunks_in_plane(si, q)) return false;
+        if (pl0 == 0 && f[ni - 1] < chunks_in_plane(si, ni - 1)) return false;
+        if (pl1 == ni - 1 && f[0] < chunks_in_plane(si, 0)) return false;
+        ++asmc[(stage - 1) * nblocks + idx];
+        break;
+      }
+      default:
+        return false;
+    }
+  }
+  return true;
+}
+
 }  // namespace
 
 PersistPlan::~PersistPlan() {
@@ -480,6 +646,7 @@ bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
     const int64_t n = chunks_of(V, kHaloChunk);
     for (int64_t c = 0; c < n; ++c) head.push_back(make_uint2(item_code(kItScatter, 0, 0, (int)L), (unsigned)c));
     pp.scatter_total[descs[L].tgt_block] += (int)n;
+    pp.link_tgt.push_back(descs[L].tgt_block);
   }
   // 3. boundary conditions, Face order, list order within a face
   std::vector<BcDesc> bds;
@@ -503,6 +670,7 @@ bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
     for (int v = 0; v < 5; ++v) d.qinf[v] = bc.q_inf[v];
     d.block = bc.block;
     bds.push_back(d);
+    pp.bc_block.push_back(bc.block);
     const int ax = bc.face >> 1;
     const int64_t area = (int64_t)blk.ni * blk.nj * blk.nk / d.n[ax];
     bc_chunks[e] = chunks_of(area * p->ghost, kHaloChunk);
@@ -548,7 +716,8 @@ bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
     cudaGetLastError();
     return fail("persistent step control block: device allocation failed");
   }
-  if (!persist_reshape(pp, blocks, nblocks, 4, 1.0)) return fail("persistent step work-list upload failed");
+  if (!persist_reshape(pp, blocks, nblocks, kPersistShapes[0].occ, kPersistShapes[0].lag_scale))
+    return fail("persistent step work-list: set-up failed");
   return true;
 }
 
@@ -558,8 +727,12 @@ bool persist_reshape(PersistPlan& pp, const fj_block* blocks, int nblocks, int o
   if (grid <= 0) return false;
   std::vector<uint2> items(pp.head);
   const int lag = std::max(0, (int)(lag_scale * grid / 2));
-  stage_items(blocks, nblocks, lag, items);
+  if (lag_scale < 0)
+    stage_items_across(blocks, nblocks, items);
+  else
+    stage_items(blocks, nblocks, lag, items);
   if (items.size() >= (size_t)INT32_MAX) return false;
+  if (!list_is_ordered(pp, blocks, nblocks, items)) return false;
   if (pp.items && (int)items.size() != pp.n_items) {
     cudaFree(pp.items);
     pp.items = nullptr;

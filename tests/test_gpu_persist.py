@@ -141,6 +141,22 @@ def test_persistent_graph_replay_and_shapes(cuda_device):
                     assert torch.equal(a, b), shape
 
 
+def test_persistent_shapes_on_large_blocks(cuda_device):
+    """Blocks large enough that every launch shape's ordering interleaves
+    flux and assembly chunks of one block (the lag shapes) or of two blocks
+    (the mixing shapes): every shape bit-identical to the split kernels."""
+    for c in (cases.tgv(n=60, noise=0.01, seed=4), cases.tree24(nblocks=3, lo=40, hi=64, seed=8)):
+        dt = _dt(c)
+        ref_plan, ref_st = _plan(c, "split")
+        ref = _steps(ref_plan, ref_st, 1, dt)[0]
+        plan, st = _plan(c, "persistent")
+        for shape in range(_capi.NUM_PERSIST_SHAPES):
+            plan.set_persist_shape(shape)
+            got = _steps(plan, st, 1, dt)[0]
+            for a, b in zip(got, ref):
+                assert torch.equal(a, b), shape
+
+
 def test_persistent_ensemble_matches_split(cuda_device):
     from famrdp_jax_b200.core.types import State
     from famrdp_jax_b200.solver import diagnostics
