@@ -79,6 +79,7 @@ SIGNATURES = {
     "fj_plan_set_streams": (_I, [_P, _I]),
     "fj_plan_set_kernel": (_I, [_P, _I]),
     "fj_plan_set_persist_shape": (_I, [_P, _I]),
+    "fj_persist_list_check": (_I, [_P, _I, _P, _I, _P, _I, _P, _I, _I, ctypes.POINTER(ctypes.c_int64)]),
     "fj_plan_get_kernel": (_I, [_P, ctypes.POINTER(_I)]),
     "fj_plan_set_wait_limit": (_I, [_P, _I]),
     "fj_plan_check": (_I, [_P, ctypes.POINTER(_I), _P]),

@@ -609,8 +609,13 @@ size_t persist_tail_bytes(const fj_block* blocks, int nblocks, const fj_link* li
   return split + halo_ws_bytes(blocks, links, nlinks, ghost);
 }
 
-bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
-                   const fj_bc* bcs, int nbcs, const fj_params* p, PersistPlan& pp, std::string* why) {
+namespace {
+
+// The host part of the set-up: validation, the halo and BC descriptor tables,
+// the halo / BC / primitive items and the counters' targets.  No device work.
+bool persist_tables(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                    const fj_bc* bcs, int nbcs, const fj_params* p, PersistPlan& pp, std::vector<HaloDesc>& descs,
+                    std::vector<BcDesc>& bds, std::string* why) {
   auto fail = [&](const std::string& w) {
     if (why) *why = w;
     return false;
@@ -622,7 +627,8 @@ bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
       return fail("block too large for 32-bit record offsets");
     if (blocks[b].ni < 1 || blocks[b].nj < 1 || blocks[b].nk < 1) return fail("empty block");
   }
-  std::vector<HaloDesc> descs;
+  descs.clear();
+  bds.clear();
   size_t nd = 0;
   if (hd::build_links(ctx, blocks, nblocks, links, nlinks, p->ghost, descs, nd) != FJ_OK)
     return fail("halo links: " + (ctx ? ctx->last_error : std::string()));
@@ -649,7 +655,6 @@ bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
     pp.link_tgt.push_back(descs[L].tgt_block);
   }
   // 3. boundary conditions, Face order, list order within a face
-  std::vector<BcDesc> bds;
   std::vector<int64_t> bc_chunks(nbcs, 0);
   for (int e = 0; e < nbcs; ++e) {
     const fj_bc& bc = bcs[e];
@@ -698,6 +703,33 @@ bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
   pp.nbcs = (int)bds.size();
   pp.split_bytes = persist_tail_bytes(blocks, nblocks, nullptr, 0, p->ghost);
   pp.head.swap(head);
+  return true;
+}
+
+// The whole work-list for a grid of `grid` resident CTAs: the head and the
+// stage items in the shape's order.
+void build_list(const PersistPlan& pp, const fj_block* blocks, int nblocks, int grid, double lag_scale,
+                std::vector<uint2>& items, int* lag_out) {
+  items = pp.head;
+  const int lag = std::max(0, (int)(lag_scale * grid / 2));
+  if (lag_scale < 0)
+    stage_items_across(blocks, nblocks, items);
+  else
+    stage_items(blocks, nblocks, lag, items);
+  if (lag_out) *lag_out = lag;
+}
+
+}  // namespace
+
+bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                   const fj_bc* bcs, int nbcs, const fj_params* p, PersistPlan& pp, std::string* why) {
+  auto fail = [&](const std::string& w) {
+    if (why) *why = w;
+    return false;
+  };
+  std::vector<HaloDesc> descs;
+  std::vector<BcDesc> bds;
+  if (!persist_tables(ctx, blocks, nblocks, links, nlinks, bcs, nbcs, p, pp, descs, bds, why)) return false;
   // device tables
   auto upload = [](void** dst, const void* src, size_t bytes) {
     if (bytes == 0) return true;
@@ -725,12 +757,9 @@ bool persist_reshape(PersistPlan& pp, const fj_block* blocks, int nblocks, int o
   if (occ != 3 && occ != 4) return false;
   const int grid = resident_grid(occ);
   if (grid <= 0) return false;
-  std::vector<uint2> items(pp.head);
-  const int lag = std::max(0, (int)(lag_scale * grid / 2));
-  if (lag_scale < 0)
-    stage_items_across(blocks, nblocks, items);
-  else
-    stage_items(blocks, nblocks, lag, items);
+  std::vector<uint2> items;
+  int lag = 0;
+  build_list(pp, blocks, nblocks, grid, lag_scale, items, &lag);
   if (items.size() >= (size_t)INT32_MAX) return false;
   if (!list_is_ordered(pp, blocks, nblocks, items)) return false;
   if (pp.items && (int)items.size() != pp.n_items) {
@@ -834,3 +863,21 @@ int persist_clear_error(const PersistPlan& pp, cudaStream_t st) {
 }
 
 }  // namespace fj
+
+extern "C" int fj_persist_list_check(const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                                     const fj_bc* bcs, int nbcs, const fj_params* p, int grid, int shape,
+                                     int64_t* n_items) {
+  using namespace fj;
+  if (!blocks || !p || grid < 1 || shape < 0 || shape >= FJ_NUM_PERSIST_SHAPES || (nlinks > 0 && !links) ||
+      (nbcs > 0 && !bcs) || nlinks < 0 || nbcs < 0)
+    return FJ_ERR_INVALID_ARGUMENT;
+  PersistPlan pp;
+  std::vector<hd::HaloDesc> descs;
+  std::vector<hd::BcDesc> bds;
+  if (!persist_tables(nullptr, blocks, nblocks, links, nlinks, bcs, nbcs, p, pp, descs, bds, nullptr))
+    return FJ_ERR_NOT_IMPLEMENTED;
+  std::vector<uint2> items;
+  build_list(pp, blocks, nblocks, grid, kPersistShapes[shape].lag_scale, items, nullptr);
+  if (n_items) *n_items = (int64_t)items.size();
+  return list_is_ordered(pp, blocks, nblocks, items) ? FJ_OK : FJ_ERR_INVALID_ARGUMENT;
+}

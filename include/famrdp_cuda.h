@@ -311,6 +311,17 @@ int fj_plan_get_kernel(const fj_plan* plan, int* kernel);
  * depend on it.  Drops captured graphs. */
 #define FJ_NUM_PERSIST_SHAPES 4
 int fj_plan_set_persist_shape(fj_plan* plan, int shape);
+/* Diagnostic of FJ_KERNEL_PERSIST's work-list, host only (no device work; the
+ * q / kxyz / vol pointers of blocks are not read): builds the list the plan of
+ * these blocks, links and boundary entries would run for `grid` resident CTAs
+ * in launch shape `shape`, stores its length in *n_items (may be NULL) and
+ * returns FJ_OK when every item waits only for items ahead of it (the
+ * property that makes the launch deadlock-free), FJ_ERR_INVALID_ARGUMENT
+ * when not (or for bad arguments), FJ_ERR_NOT_IMPLEMENTED when the persistent
+ * step does not apply to the configuration. */
+int fj_persist_list_check(const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                          const fj_bc* bcs, int nbcs, const fj_params* p, int grid, int shape,
+                          int64_t* n_items);
 /* Diagnostics of the bounded waits of the tile kernel (every wait for a TMA
  * copy) and of the persistent step (every wait on a completion counter): a
  * wait gives up after `limit` tries (-1 restores the default, about a
