@@ -713,7 +713,7 @@ def main(argv=None):
     ap.add_argument("--shape", type=int, default=1, help="FP32 launch shape for --stage-only")
     ap.add_argument("--persist-shape", type=int, default=0,
                     help="launch shape of the persistent step for --stage-only --kernel persistent")
-    ap.add_argument("--kernel", choices=["auto", "split", "tile", "persistent"], default="auto",
+    ap.add_argument("--kernel", choices=["auto", "split", "tile", "persistent", "split_fill"], default="auto",
                     help="FP32 stage kernels: auto = the autotuner's choice (split shapes, the tile kernel and the "
                          "persistent step's shapes)")
     ap.add_argument("--seed", type=int, default=0)

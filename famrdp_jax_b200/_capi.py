@@ -172,9 +172,10 @@ PIPELINES = {"fused": 0, "staged": 1, "split": 2}
 
 
 NUM_SPLIT_VARIANTS = 6  # FJ_NUM_SPLIT_VARIANTS
-KERNELS = {"split": 0, "tile": 1, "persistent": 2}  # FJ_KERNEL_SPLIT, FJ_KERNEL_TILE, FJ_KERNEL_PERSIST
+# FJ_KERNEL_SPLIT, FJ_KERNEL_TILE, FJ_KERNEL_PERSIST, FJ_KERNEL_SPLIT_FILL
+KERNELS = {"split": 0, "tile": 1, "persistent": 2, "split_fill": 3}
 NUM_PERSIST_SHAPES = 4  # FJ_NUM_PERSIST_SHAPES
-AUTOTUNE_CANDIDATES = 2 * NUM_SPLIT_VARIANTS + 1 + NUM_PERSIST_SHAPES  # FJ_AUTOTUNE_CANDIDATES
+AUTOTUNE_CANDIDATES = 2 * NUM_SPLIT_VARIANTS + 2 + NUM_PERSIST_SHAPES  # FJ_AUTOTUNE_CANDIDATES
 TILES = {"8x32": 0, "4x32": 1, "6x32": 2, "8x16": 3, "16x32": 4, "8x64": 5, "16x16": 6}
 
 

@@ -203,6 +203,9 @@ struct StepOpts {
   // the whole step with the persistent kernel
   const TileMaps* tile = nullptr;
   const PersistPlan* persist = nullptr;
+  // split kernels for the stages, the halo, BCs and stage-1 primitives as one
+  // persistent launch (the persistent step's work-list head)
+  const PersistPlan* fill = nullptr;
   int wait_limit = -1;
 };
 
@@ -261,9 +264,15 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
   if (ctx->pipeline == FJ_PIPELINE_SPLIT && o.persist && p->precision == FJ_PREC_F32FLUX && kmet)
     return persist_step(ctx, *o.persist, out.data(), nblocks, q1s, q2s, q_out, p, o.p_ref, mu0_b, dt_b, dt, kmet,
                         tail, o.wait_limit, st);
-  s = halo_exchange(ctx, out.data(), nblocks, links, nlinks, p->ghost, (double*)tail, tail_b, st);
-  if (s != FJ_OK) return s;
-  s = apply_bc(ctx, out.data(), nblocks, bcs, nbcs, p, st);
+  const bool fused_fill = ctx->pipeline == FJ_PIPELINE_SPLIT && o.fill && p->precision == FJ_PREC_F32FLUX && kmet;
+  if (fused_fill) {
+    s = persist_step(ctx, *o.fill, out.data(), nblocks, q1s, q2s, q_out, p, o.p_ref, mu0_b, dt_b, dt, kmet, tail,
+                     o.wait_limit, st, true);
+  } else {
+    s = halo_exchange(ctx, out.data(), nblocks, links, nlinks, p->ghost, (double*)tail, tail_b, st);
+    if (s != FJ_OK) return s;
+    s = apply_bc(ctx, out.data(), nblocks, bcs, nbcs, p, st);
+  }
   if (s != FJ_OK) return s;
   const int flags = kRhsInvscd | kRhsViscous;
   if (ctx->pipeline == FJ_PIPELINE_SPLIT && o.tile && p->precision == FJ_PREC_F32FLUX && kmet)
@@ -311,8 +320,9 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
       }
       if (v.empty()) return FJ_OK;
       // the assembly of stages 1 and 2 also writes the next stage's primitives
-      return split_stage(ctx, v.data(), (int)v.size(), ph, flags, stage, p->precision, gs, stage > 1, stage < 3,
-                         variant, after_fluxes);
+      // (the fused ghost fill writes stage 1's)
+      return split_stage(ctx, v.data(), (int)v.size(), ph, flags, stage, p->precision, gs, stage > 1 || fused_fill,
+                         stage < 3, variant, after_fluxes);
     };
     if (two) {
       s = cuda_status(ctx, cudaEventRecord(o.fork, st), "fork");
@@ -684,6 +694,10 @@ static int plan_step_impl(fj_plan* pl, double* const* q_in, double* const* q_out
     opts.persist = (const PersistPlan*)pl->persist;
     opts.wait_limit = pl->wait_limit;
   }
+  if (pl->kernel == FJ_KERNEL_SPLIT_FILL && pl->persist) {
+    opts.fill = (const PersistPlan*)pl->persist;
+    opts.wait_limit = pl->wait_limit;
+  }
   if (pl->streams == 2) {
     opts.side = pl->side_stream;
     opts.fork = pl->ev_fork;
@@ -750,12 +764,13 @@ int fj_plan_set_streams(fj_plan* pl, int n) {
 
 int fj_plan_set_kernel(fj_plan* pl, int kernel) {
   if (!pl) return FJ_ERR_INVALID_ARGUMENT;
-  if (kernel != FJ_KERNEL_SPLIT && kernel != FJ_KERNEL_TILE && kernel != FJ_KERNEL_PERSIST)
+  if (kernel != FJ_KERNEL_SPLIT && kernel != FJ_KERNEL_TILE && kernel != FJ_KERNEL_PERSIST &&
+      kernel != FJ_KERNEL_SPLIT_FILL)
     return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "unknown stage kernel");
   if (kernel == FJ_KERNEL_TILE && !pl->tile)
     return set_err(pl->ctx, FJ_ERR_NOT_IMPLEMENTED,
                    "the tile kernel needs an FP32-flux split plan and the driver's tensor-map encoder");
-  if (kernel == FJ_KERNEL_PERSIST && !pl->persist)
+  if ((kernel == FJ_KERNEL_PERSIST || kernel == FJ_KERNEL_SPLIT_FILL) && !pl->persist)
     return set_err(pl->ctx, FJ_ERR_NOT_IMPLEMENTED,
                    "the persistent step needs an FP32-flux split plan of at most 64 blocks");
   if (kernel != pl->kernel) drop_graphs(pl);
@@ -883,6 +898,21 @@ int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, dou
       }
     }
   }
+  // the split kernels behind the fused ghost fill, in the best split shape so far
+  if (with_persist && s == FJ_OK && best_k == FJ_KERNEL_SPLIT) {
+    s = fj_plan_set_variant(pl, best_v);
+    if (s == FJ_OK) s = fj_plan_set_streams(pl, best_s);
+    if (s == FJ_OK) s = fj_plan_set_kernel(pl, FJ_KERNEL_SPLIT_FILL);
+    float ms = 0.0f;
+    if (s == FJ_OK) s = time_steps(ms);
+    if (s == FJ_OK) {
+      if (ms_out) ms_out[2 * FJ_NUM_SPLIT_VARIANTS + 1 + FJ_NUM_PERSIST_SHAPES] = ms / reps;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_k = FJ_KERNEL_SPLIT_FILL;
+      }
+    }
+  }
   for (int k = 0; with_persist && k < FJ_NUM_PERSIST_SHAPES && s == FJ_OK; ++k) {
     s = fj_plan_set_streams(pl, 1);
     if (s == FJ_OK) s = fj_plan_set_kernel(pl, FJ_KERNEL_PERSIST);
@@ -906,9 +936,10 @@ int fj_plan_autotune(fj_plan* pl, double* const* q_in, double* const* q_out, dou
   if (r == FJ_OK) r = fj_plan_set_kernel(pl, s == FJ_OK ? best_k : keep_k);
   if (r == FJ_OK && pl->persist) r = fj_plan_set_persist_shape(pl, s == FJ_OK ? best_p : keep_p);
   if (s == FJ_OK) s = r;
-  *chosen = pl->kernel == FJ_KERNEL_TILE      ? 2 * FJ_NUM_SPLIT_VARIANTS
-            : pl->kernel == FJ_KERNEL_PERSIST ? 2 * FJ_NUM_SPLIT_VARIANTS + 1 + pl->persist_shape
-                                              : pl->variant + FJ_NUM_SPLIT_VARIANTS * (pl->streams - 1);
+  *chosen = pl->kernel == FJ_KERNEL_TILE         ? 2 * FJ_NUM_SPLIT_VARIANTS
+            : pl->kernel == FJ_KERNEL_PERSIST    ? 2 * FJ_NUM_SPLIT_VARIANTS + 1 + pl->persist_shape
+            : pl->kernel == FJ_KERNEL_SPLIT_FILL ? 2 * FJ_NUM_SPLIT_VARIANTS + 1 + FJ_NUM_PERSIST_SHAPES
+                                                 : pl->variant + FJ_NUM_SPLIT_VARIANTS * (pl->streams - 1);
   return s;
 }
 

@@ -72,10 +72,14 @@ bool persist_setup(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_li
 bool persist_reshape(PersistPlan& pp, const fj_block* blocks, int nblocks, int occ, double lag_scale);
 // One step: blocks[b].q is the step's start state (written in place by the
 // halo and BC items), q1s / q2s / q_out the stage results.  tail: the plan
-// tail (persist_tail_bytes); kmet: the FP32 metric records.
+// tail (persist_tail_bytes); kmet: the FP32 metric records.  fill_only: only
+// the list's head -- halo gathers and scatters, BC faces and the stage-1
+// primitives (into the split layout's first primitive buffer) -- in one
+// launch; the caller runs the stages with the split kernels.
 int persist_step(fj_ctx* ctx, const PersistPlan& pp, const fj_block* blocks, int nblocks, double* const* q1s,
                  double* const* q2s, double* const* q_out, const fj_params* p, double p_ref, const double* mu0_b,
-                 const double* dt_b, double dt, void* const* kmet, void* tail, int wait_limit, cudaStream_t st);
+                 const double* dt_b, double dt, void* const* kmet, void* tail, int wait_limit, cudaStream_t st,
+                 bool fill_only = false);
 // The sticky error word (nonzero: a bounded wait gave up); clear resets it.
 int persist_read_error(const PersistPlan& pp, int* out, cudaStream_t st);
 int persist_clear_error(const PersistPlan& pp, cudaStream_t st);

@@ -784,7 +784,8 @@ bool persist_reshape(PersistPlan& pp, const fj_block* blocks, int nblocks, int o
 
 int persist_step(fj_ctx* ctx, const PersistPlan& pp, const fj_block* blocks, int nblocks, double* const* q1s,
                  double* const* q2s, double* const* q_out, const fj_params* p, double p_ref, const double* mu0_b,
-                 const double* dt_b, double dt, void* const* kmet, void* tail, int wait_limit, cudaStream_t st) {
+                 const double* dt_b, double dt, void* const* kmet, void* tail, int wait_limit, cudaStream_t st,
+                 bool fill_only) {
   if (nblocks < 1 || nblocks > kPersistMaxBlocks || !kmet || !pp.items || !pp.ctl)
     return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "persistent step: plan not set up");
   std::unique_ptr<PersistParams> hold(new (std::nothrow) PersistParams());  // 14 KB: off the stack
@@ -831,7 +832,8 @@ int persist_step(fj_ctx* ctx, const PersistPlan& pp, const fj_block* blocks, int
   P.bcs = (const BcDesc*)pp.bcs;
   P.halo = (double*)((char*)tail + pp.split_bytes);
   P.ctl = pp.ctl;
-  P.n_items = pp.n_items;
+  // the list's head (halo, BCs, primitives) is a prefix that depends on nothing after it
+  P.n_items = fill_only ? (int)pp.head.size() : pp.n_items;
   P.nlinks = pp.nlinks;
   P.ghost = p->ghost;
   P.wait_limit = wait_limit;
@@ -841,10 +843,11 @@ int persist_step(fj_ctx* ctx, const PersistPlan& pp, const fj_block* blocks, int
                       cudaMemsetAsync(pp.ctl + pp.reset_from, 0, (size_t)(pp.ctl_ints - pp.reset_from) * sizeof(int), st),
                       "persistent step counters");
   if (s != FJ_OK) return s;
+  const int grid = std::max(1, std::min(pp.grid, P.n_items));
   if (pp.occ == 3)
-    k_step_persist<3><<<pp.grid, kSplitThreads, 0, st>>>(P);
+    k_step_persist<3><<<grid, kSplitThreads, 0, st>>>(P);
   else
-    k_step_persist<4><<<pp.grid, kSplitThreads, 0, st>>>(P);
+    k_step_persist<4><<<grid, kSplitThreads, 0, st>>>(P);
   ctx->launches += 1;
   return launch_status(ctx, "persistent step launch");
 }

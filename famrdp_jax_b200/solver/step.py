@@ -117,8 +117,9 @@ class StepPlan:
         (outs is overwritten) and keeps the fastest; returns (chosen, mean step
         ms per candidate), the candidate index being shape +
         NUM_SPLIT_VARIANTS * (streams - 1), 2 * NUM_SPLIT_VARIANTS for the
-        tile kernel, or 2 * NUM_SPLIT_VARIANTS + 1 + k for the persistent step
-        in shape k."""
+        tile kernel, 2 * NUM_SPLIT_VARIANTS + 1 + k for the persistent step
+        in shape k, or 2 * NUM_SPLIT_VARIANTS + 1 + NUM_PERSIST_SHAPES for the
+        split kernels behind the fused ghost fill ("split_fill")."""
         n = _capi.AUTOTUNE_CANDIDATES
         ms = (ctypes.c_double * n)()
         ch = ctypes.c_int()
@@ -135,9 +136,12 @@ class StepPlan:
     def set_kernel(self, kernel: str) -> None:
         """Stage kernels of an FP32-flux plan: "split" (three kernels per stage
         through scratch), "tile" (one persistent fused kernel per stage over a
-        (tile, i-plane) work-list, primitive planes staged by TMA) or
+        (tile, i-plane) work-list, primitive planes staged by TMA),
         "persistent" (the whole step -- halo, boundary faces and the three
-        stages -- in one launch over a dependency-ordered work-list)."""
+        stages -- in one launch over a dependency-ordered work-list) or
+        "split_fill" (the split kernels after one launch that fills the
+        ghost cells -- halo and boundary faces -- and computes the stage-1
+        primitives)."""
         if kernel not in _capi.KERNELS:
             raise KeyError(kernel)
         c = _capi.ctx(self.device)

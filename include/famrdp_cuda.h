@@ -299,10 +299,16 @@ int fj_plan_set_variant(fj_plan* plan, int variant);
  * arithmetic is the split kernels', and its results are bit-identical to
  * FJ_KERNEL_SPLIT's.  FJ_ERR_NOT_IMPLEMENTED for FP64 or non-split plans and
  * plans of more than 64 blocks.  fj_plan_stage runs the split kernels for it.
+ * FJ_KERNEL_SPLIT_FILL runs the stages with the split kernels and the step's
+ * ghost fill -- halo gathers and scatters, boundary faces in Face order and
+ * the stage-1 primitives -- as ONE launch of FJ_KERNEL_PERSIST's work-list
+ * head (the boundary conditions fused with the halo); bit-identical to
+ * FJ_KERNEL_SPLIT, same conditions as FJ_KERNEL_PERSIST.
  * Changing the kernel drops captured graphs. */
 #define FJ_KERNEL_SPLIT 0
 #define FJ_KERNEL_TILE 1
 #define FJ_KERNEL_PERSIST 2
+#define FJ_KERNEL_SPLIT_FILL 3
 int fj_plan_set_kernel(fj_plan* plan, int kernel);
 int fj_plan_get_kernel(const fj_plan* plan, int* kernel);
 /* Launch shape of FJ_KERNEL_PERSIST, one of FJ_NUM_PERSIST_SHAPES (0 is the
@@ -345,13 +351,15 @@ int fj_plan_set_streams(fj_plan* plan, int n);
  * every launch shape (split plans, both precisions) and stream count (split plans of
  * two or more blocks) with CUDA events on `stream`, keeps the fastest in the
  * plan and reports it as shape + FJ_NUM_SPLIT_VARIANTS * (streams - 1),
- * 2 * FJ_NUM_SPLIT_VARIANTS for the tile kernel, or
- * 2 * FJ_NUM_SPLIT_VARIANTS + 1 + k for the persistent step in shape k
- * (FP32-flux plans where those kernels are available: more candidates) (and,
+ * 2 * FJ_NUM_SPLIT_VARIANTS for the tile kernel,
+ * 2 * FJ_NUM_SPLIT_VARIANTS + 1 + k for the persistent step in shape k, or
+ * 2 * FJ_NUM_SPLIT_VARIANTS + 1 + FJ_NUM_PERSIST_SHAPES for FJ_KERNEL_SPLIT_FILL
+ * in the best split shape (FP32-flux plans where those kernels are available:
+ * more candidates) (and,
  * if ms_out is non-NULL, the FJ_AUTOTUNE_CANDIDATES mean step times at those
  * indices; 0 where not timed).  q_out is overwritten; q_in is not changed.
  * Synchronises the stream. */
-#define FJ_AUTOTUNE_CANDIDATES (2 * FJ_NUM_SPLIT_VARIANTS + 1 + FJ_NUM_PERSIST_SHAPES)
+#define FJ_AUTOTUNE_CANDIDATES (2 * FJ_NUM_SPLIT_VARIANTS + 2 + FJ_NUM_PERSIST_SHAPES)
 int fj_plan_autotune(fj_plan* plan, double* const* q_in, double* const* q_out, double dt, int reps,
                      int* chosen, double* ms_out, void* stream);
 int fj_plan_step_graph(fj_plan* plan, double* const* q_in, double* const* q_out, double dt,

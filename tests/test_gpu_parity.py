@@ -538,6 +538,15 @@ def test_autotune_launch_shapes_agree(cuda_device, precision):
                 o = [torch.empty_like(q) for q in qs]
                 plan.run(qs, o, dt, graph=graph)
                 outs.append(o)
+        # the split kernels behind the fused ghost fill, every shape and stream count
+        plan.set_kernel("split_fill")
+        for streams in (1, 2):
+            plan.set_streams(streams)
+            for v in range(_capi.NUM_SPLIT_VARIANTS):
+                plan.set_variant(v)
+                o = [torch.empty_like(q) for q in qs]
+                plan.run(qs, o, dt, graph=v % 2 == 1)
+                outs.append(o)
         assert plan.check() == 0
         plan.set_kernel("split")
     for o in outs[1:]:
@@ -551,7 +560,9 @@ def test_autotune_launch_shapes_agree(cuda_device, precision):
     assert 0 <= chosen < _capi.AUTOTUNE_CANDIDATES and len(ms) == _capi.AUTOTUNE_CANDIDATES and min(timed) > 0
     if precision == "f64":
         assert chosen < 2 * n and not any(ms[2 * n:])
-    assert plan.kernel == ("tile" if chosen == 2 * n else "persistent" if chosen > 2 * n else "split")
+    fill = 2 * n + 1 + _capi.NUM_PERSIST_SHAPES
+    assert plan.kernel == ("tile" if chosen == 2 * n else "split_fill" if chosen == fill
+                           else "persistent" if chosen > 2 * n else "split")
 
 
 def test_plan_argument_errors(cuda_device):

@@ -5,7 +5,8 @@ dependency-ordered work-list (halo gathers and scatters, boundary faces,
 primitives, and the flux and assembly chunks of the three stages), so:
   * persistent vs split: bit-identical states after every step (halo links,
     farfield / wall / symmetry faces, uneven and ragged blocks, ensembles,
-    every launch shape, graph replays, the adjoint's saving step);
+    every launch shape, graph replays, the adjoint's saving step), and so is
+    the split path behind the fused ghost fill (the list's head alone);
   * persistent vs the FP64 oracle: relative L2 of q <= 1e-5 after the steps
     run (the FP32-flux bound of the other parity tests);
   * a bounded wait that runs out is reported by fj_plan_check and leaves the
@@ -97,17 +98,20 @@ def _case(name):
     raise KeyError(name)
 
 
+@pytest.mark.parametrize("kernel", ["persistent", "split_fill"])
 @pytest.mark.parametrize("name", ["tgv32", "wavy4", "tree24", "ragged", "mirror", "isothermal"])
-def test_persistent_step_is_bit_identical_to_split(cuda_device, name):
+def test_persistent_step_is_bit_identical_to_split(cuda_device, name, kernel):
+    """The persistent step, and the split kernels behind the fused ghost fill
+    (the work-list's head: halo, boundary faces, primitives in one launch)."""
     c, n = _case(name)
     dt = _dt(c)
     res = {}
-    for kernel in ("split", "persistent"):
-        plan, st = _plan(c, kernel)
-        res[kernel] = _steps(plan, st, n, dt)
+    for k in ("split", kernel):
+        plan, st = _plan(c, k)
+        res[k] = _steps(plan, st, n, dt)
     for s in range(n):
-        for a, b in zip(res["persistent"][s], res["split"][s]):
-            assert torch.equal(a, b), (name, s)
+        for a, b in zip(res[kernel][s], res["split"][s]):
+            assert torch.equal(a, b), (name, kernel, s)
 
 
 @pytest.mark.parametrize("name", ["wavy4", "tree24", "mirror"])
