@@ -116,9 +116,9 @@ __device__ __forceinline__ int ld_relaxed(const int* p) {
 __host__ __device__ __forceinline__ int64_t chunks_of(int64_t n, int64_t per) { return (n + per - 1) / per; }
 
 // Flux chunks (kFluxCells cells) that overlap i-plane q of a block with si
-// cells per plane.
-__device__ __forceinline__ int flux_chunks_in_plane(int64_t si, int q) {
-  return (int)(((int64_t)(q + 1) * si - 1) / kFluxCells - ((int64_t)q * si) / kFluxCells + 1);
+// cells per plane (32-bit: a block's cell count is below 2^27).
+__device__ __forceinline__ int flux_chunks_in_plane(uint32_t si, int q) {
+  return (int)(((uint32_t)(q + 1) * si - 1) / kFluxCells - ((uint32_t)q * si) / kFluxCells + 1);
 }
 
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
@@ -152,17 +152,18 @@ __device__ int dep_pair(const PersistParams& P, uint32_t code, int chunk, int i,
       return 2;
     case kItFlux: {
       const SplitBlock& B = P.tab.b[idx].blk;
-      const int64_t N = (int64_t)B.ni * B.nj * B.nk;
+      const uint32_t N = (uint32_t)B.ni * B.nj * B.nk;
       if (i == 0) {
-        if (stage == 1) p = ctl + kCtlPrims + idx, target = (int)chunks_of(N, kFluxCells);
-        else p = ctl + kCtlAsm + kPersistMaxBlocks * (stage - 2) + idx, target = (int)chunks_of(N, kAsmCellsP);
+        if (stage == 1) p = ctl + kCtlPrims + idx, target = (int)((N + kFluxCells - 1) / kFluxCells);
+        else p = ctl + kCtlAsm + kPersistMaxBlocks * (stage - 2) + idx, target = (int)((N + kAsmCellsP - 1) / kAsmCellsP);
       }
       return 1;
     }
     default: {  // kItAsm: the flux planes lo .. hi, then the periodic i wrap's far plane
+      // (32-bit: a block's cell count is below 2^27)
       const SplitBlock& B = P.tab.b[idx].blk;
-      const int64_t si = (int64_t)B.nj * B.nk, N = si * B.ni;
-      const int64_t c0 = (int64_t)chunk * kAsmCellsP, c1 = min(c0 + kAsmCellsP, N) - 1;
+      const uint32_t si = (uint32_t)B.nj * B.nk, N = si * B.ni;
+      const uint32_t c0 = (uint32_t)chunk * kAsmCellsP, c1 = min(c0 + kAsmCellsP, N) - 1;
       const int pl0 = (int)(c0 / si), pl1 = (int)(c1 / si);
       const int lo = max(pl0 - 1, 0), hi = min(pl1 + 1, B.ni - 1);
       const bool wrap_hi = pl0 == 0 && hi < B.ni - 1, wrap_lo = pl1 == B.ni - 1 && lo > 0;
@@ -180,14 +181,15 @@ __device__ int dep_pair(const PersistParams& P, uint32_t code, int chunk, int i,
   }
 }
 
-// Scheduler warp: whether every counter of the item has reached its target,
-// the lanes polling the pairs in parallel (relaxed loads; the caller fences
-// once they have).  once: a single look that neither waits nor records
-// anything.  Otherwise each lane polls at most the wait limit times (0: give
-// up at once if there is anything to wait for; negative: the default);
-// giving up records the error and raises the abort flag, and an abort raised
-// elsewhere ends the wait as well.
-__device__ bool deps_warp(const PersistParams& P, uint2 it, bool once) {
+// Scheduler warp: whether every counter the item waits for has reached its
+// target, the lanes polling the (counter, target) pairs in parallel (relaxed
+// loads; the caller fences once they have).  The pairs are set up once.
+// soft: at most `looks` looks 128 ns apart that neither wait longer nor
+// record anything (false: not yet).  Otherwise each lane polls at most the
+// wait limit times (0: give up at once if there is anything to wait for;
+// negative: the default); giving up records the error and raises the abort
+// flag, and an abort raised elsewhere ends the wait as well.
+__device__ bool deps_wait(const PersistParams& P, uint2 it, bool soft, int looks) {
   const unsigned all = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int* p0;
@@ -200,7 +202,11 @@ __device__ bool deps_warp(const PersistParams& P, uint2 it, bool once) {
     if (base + lane < n) dep_pair(P, it.x, (int)it.y, base + lane, p, target);
     const bool need = p != nullptr && target > 0;
     bool ok = !need || ld_relaxed(p) >= target;
-    if (once) {
+    if (soft) {
+      for (int look = 1; look < looks && !__all_sync(all, ok); ++look) {
+        __nanosleep(128);
+        if (!ok) ok = ld_relaxed(p) >= target;
+      }
       if (!__all_sync(all, ok)) return false;
       continue;
     }
@@ -239,8 +245,8 @@ __device__ void item_done(const PersistParams& P, uint2 it) {
     case kItPrims: red_add(ctl + kCtlPrims + idx, 1); break;
     case kItFlux: {
       const SplitBlock& B = P.tab.b[idx].blk;
-      const int64_t si = (int64_t)B.nj * B.nk, N = si * B.ni;
-      const int64_t c0 = (int64_t)chunk * kFluxCells, c1 = min(c0 + kFluxCells, N) - 1;
+      const uint32_t si = (uint32_t)B.nj * B.nk, N = si * B.ni;
+      const uint32_t c0 = (uint32_t)chunk * kFluxCells, c1 = min(c0 + kFluxCells, N) - 1;
       int* f = ctl + kCtlFlux + (stage - 1) * P.total_planes + P.plane_base[idx];
       for (int q = (int)(c0 / si); q <= (int)(c1 / si); ++q) red_add(f + q, 1);
       break;
@@ -378,11 +384,7 @@ __device__ void schedule(const PersistParams& P, uint2* slot, int* end) {
     if (!stop) {
       // a few looks while the workers are still on item k-1, before giving
       // up the overlap and publishing it
-      bool ready = P.wait_limit != 0 && deps_warp(P, it, true);
-      for (int look = 0; look < 12 && !ready && P.wait_limit != 0; ++look) {
-        __nanosleep(128);
-        ready = deps_warp(P, it, true);
-      }
+      const bool ready = P.wait_limit != 0 && deps_wait(P, it, true, 13);
       if (!ready) {
         if (pend) {
           if (l0) item_done(P, pend_it);
@@ -393,7 +395,7 @@ __device__ void schedule(const PersistParams& P, uint2* slot, int* end) {
           if (l0) item_done(P, b ? held0 : held1);
           done = k - 1;
         }
-        stop = !deps_warp(P, it, false);
+        stop = !deps_wait(P, it, false, 0);
       }
       if (!stop && l0) fence_acq_rel();  // acquire: what the counters published is visible from here on
     }
