@@ -235,3 +235,38 @@ def test_persistent_refused_where_it_does_not_apply(cuda_device):
     with pytest.raises(Exception):
         plan.set_kernel("persistent")
     assert plan.kernel == "split"
+
+
+@pytest.mark.parametrize("kernel", ["persistent", "split_fill"])
+def test_adjoint_through_persistent_forward(cuda_device, kernel):
+    """The checkpointed adjoint with its forward sweeps (plain, saving and
+    recomputing steps, some on a second stream) run by the persistent step or
+    the fused ghost fill: J bit-identical to the split kernels' (the forward
+    is); dJ/dq0 and dJ/dmu0 within 1e-6 relative, because the reverse sweep
+    accumulates face and viscosity adjoints with atomics, whose order (and so
+    rounding) differs from run to run even with the same forward."""
+    from famrdp_jax_b200.solver import adjoint
+    c = cases.tree24(nblocks=3, lo=8, hi=14, seed=13)
+    dt = _dt(c)
+    res = {}
+    for k in ("split", kernel):
+        plan, st = _plan(c, k)
+        J, g, dmu = adjoint.adjoint_kinetic_energy(st, dataclasses.replace(c.cfg, precision="f32"), dt, 6,
+                                                   checkpoint_every=2, plan=plan)
+        assert plan.check() == 0
+        res[k] = (float(J), [x.clone() for x in g], float(dmu))
+    assert res[kernel][0] == res["split"][0]
+    assert abs(res[kernel][2] - res["split"][2]) <= 1e-6 * abs(res["split"][2])
+    num = sum(float(torch.sum((a - b) ** 2)) for a, b in zip(res[kernel][1], res["split"][1]))
+    den = sum(float(torch.sum(b ** 2)) for b in res["split"][1])
+    assert (num / den) ** 0.5 <= 1e-6
+
+
+def test_persist_shape_argument_errors(cuda_device):
+    c = cases.tgv(n=8)
+    plan, st = _plan(c, "persistent")
+    for bad in (-1, _capi.NUM_PERSIST_SHAPES):
+        with pytest.raises(ValueError):
+            plan.set_persist_shape(bad)
+    plan.set_persist_shape(_capi.NUM_PERSIST_SHAPES - 1)
+    assert plan.kernel == "persistent"
