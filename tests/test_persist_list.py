@@ -98,3 +98,31 @@ def test_work_list_refused_where_the_step_does_not_apply():
     for grid, shape in ((0, 0), (592, -1), (592, _capi.NUM_PERSIST_SHAPES)):
         assert _capi.lib().fj_persist_list_check(blocks, len(shapes), la, len(links), ba, len(bcs),
                                                  ctypes.byref(p), grid, shape, None) == _capi.FJ_ERR_INVALID_ARGUMENT
+
+
+def test_work_list_with_mapped_and_overlapping_links():
+    """Links between faces of different axes in every mapped orientation,
+    target slabs that overlap at edges, a block linked to itself, and no
+    boundary faces."""
+    from famrdp_jax_b200.core.constants import Face, mapped_orientation as m
+    shapes = [(8, 9, 10), (9, 10, 7), (6, 10, 8)]
+    spec = [
+        [(Face.IMAX, 1, Face.KMIN, m(reverse_a=True)), (Face.JMIN, 2, Face.IMAX, m(swap=True, reverse_b=True)),
+         (Face.KMAX, 0, Face.KMIN, m(reverse_a=True, reverse_b=True)), (Face.KMIN, 0, Face.KMAX, 0)],
+        [(Face.KMIN, 0, Face.IMAX, m(reverse_a=True)), (Face.IMIN, 1, Face.IMAX, 0), (Face.IMAX, 1, Face.IMIN, m())],
+        [(Face.IMAX, 0, Face.JMIN, m(swap=True)), (Face.JMAX, 2, Face.JMIN, m(reverse_a=True, reverse_b=True))],
+    ]
+    links = [(b, int(f), sb, int(sf), o) for b, s in enumerate(spec) for f, sb, sf, o in s]
+    blocks = (_capi.FjBlock * 3)()
+    for b, (ni, nj, nk) in enumerate(shapes):
+        blocks[b].ni, blocks[b].nj, blocks[b].nk = ni, nj, nk
+    gas = cases.tgv(n=8).cfg.gas
+    p = _capi.params(gas, limiter="minmod", ghost=2, precision="f32")
+    expected = _expected_items(shapes, links, [], 2)
+    for shape in range(_capi.NUM_PERSIST_SHAPES):
+        for grid in (1, 5, 592):
+            n = ctypes.c_int64(-1)
+            st = _capi.lib().fj_persist_list_check(blocks, 3, _topology.link_array(links), len(links),
+                                                   _topology.bc_array([]), 0, ctypes.byref(p), grid, shape,
+                                                   ctypes.byref(n))
+            assert st == _capi.FJ_OK and n.value == expected, (shape, grid, st, n.value, expected)
