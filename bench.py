@@ -293,13 +293,21 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"),
     grads = {}
     stream = torch.cuda.current_stream(device)
 
-    def timed(fn):
+    clocks = {}
+
+    def timed(fn, clock_key=None):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(device)
+        clk = ClockSampler(_gpu_index(device.index or 0)) if clock_key else None
+        if clk:
+            clk.__enter__()
         e0.record(stream)
         r = fn()
         e1.record(stream)
         torch.cuda.synchronize(device)
+        if clk:
+            clk.__exit__(None, None, None)
+            clocks[clock_key] = clk.summary()
         return r, e0.elapsed_time(e1)
 
     for prec in precisions:
@@ -319,7 +327,7 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"),
                 plan.run(a, b, dt, graph=True)
                 a, b = b, a
 
-        _, t_fwd = timed(fwd)
+        _, t_fwd = timed(fwd, "forward")
         adjoint.adjoint_kinetic_energy(st, cfg, dt, 2, checkpoint_every=1, plan=plan)  # warm-up
         run = adjoint._Run(cfg=cfg, metrics=st.metrics, dt=float(dt), nsteps=nsteps, every=every, plan=plan,
                            tables=adjoint._Tables(cfg), dmu=torch.zeros(1, dtype=torch.float64, device=device))
@@ -328,7 +336,7 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"),
         adjoint._forward_with_checkpoints(run, [st.blocks[0].q])  # warm-up: captures the step graphs
         (final, checkpoints), t_ckpt = timed(lambda: adjoint._forward_with_checkpoints(run, [st.blocks[0].q]))
         lams = adjoint.kinetic_energy_grad(final, st.metrics, cfg.ghost)
-        g, t_rev = timed(lambda: adjoint._reverse_sweep(run, checkpoints, lams))
+        g, t_rev = timed(lambda: adjoint._reverse_sweep(run, checkpoints, lams), "reverse")
         fstate = dc.replace(st, blocks=(dc.replace(st.blocks[0], q=final[0]),))
         J = diagnostics.kinetic_energy(fstate, cfg.ghost)
         grads[prec] = g[0]
@@ -338,7 +346,10 @@ def adjoint_timing(device, n=96, nsteps=50, every=10, precisions=("f64", "f32"),
         out[prec] = {"forward_ms_per_step": t_fwd / nsteps, "checkpointed_forward_ms_per_step": t_ckpt / nsteps,
                      "reverse_sweep_ms_per_step": t_rev / nsteps, "adjoint_over_forward": t_rev / t_fwd,
                      "gradient_over_forward": (t_ckpt + t_rev) / t_fwd,
-                     "J": J, "dJ_dmu0": dmu, "dJ_dM0": dJ_dM0}
+                     "J": J, "dJ_dmu0": dmu, "dJ_dM0": dJ_dM0,
+                     # SM clocks during the timed forward and reverse sweeps: the
+                     # issue-bound adjoint kernels run under the power cap
+                     "clocks": dict(clocks)}
         del plan, run, final, checkpoints, lams, g, qa, qb
         torch.cuda.empty_cache()
     out["ratios_note"] = ("adjoint_over_forward = reverse sweep (segment recompute + step adjoints) / plain "
