@@ -76,6 +76,8 @@ SIGNATURES = {
     "fj_plan_step": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _D, _P]),
     "fj_plan_set_ensemble": (_I, [_P, _P, _P]),
     "fj_plan_set_variant": (_I, [_P, _I]),
+    "fj_plan_p_ref": (_I, [_P, ctypes.POINTER(_D)]),
+    "fj_plan_set_p_ref": (_I, [_P, _D]),
     "fj_plan_set_streams": (_I, [_P, _I]),
     "fj_plan_set_kernel": (_I, [_P, _I]),
     "fj_plan_set_persist_shape": (_I, [_P, _I]),
@@ -114,6 +116,10 @@ SIGNATURES = {
     "fj_rhs_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _P]),
     "fj_rhs_noalloc_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(FjParams), _P]),
     "fj_halo_exchange_f64": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjLink), _I, _I, _P]),
+    "fj_halo_pack_f64": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjLink), _I, _I,
+                              ctypes.POINTER(_I), ctypes.POINTER(_I64), _I, _P, _I64, _P]),
+    "fj_halo_unpack_f64": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjLink), _I, _I,
+                                ctypes.POINTER(_I), ctypes.POINTER(_I64), _I, _P, _I64, _P]),
     "fj_apply_bc_f64": (_I, [_P, ctypes.POINTER(FjBlock), _I, ctypes.POINTER(FjBc), _I,
                              ctypes.POINTER(FjParams), _P]),
     "fj_step_f64": (_I, [_P, ctypes.POINTER(FjBlock), ctypes.POINTER(_P), _I, ctypes.POINTER(FjLink), _I,

@@ -530,6 +530,41 @@ int fj_halo_exchange_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const
                        S(stream));
 }
 
+// Shared checks of fj_halo_pack_f64 / fj_halo_unpack_f64: every block's
+// dimensions (q may be NULL), the link list and the selection arrays.
+static int check_halo_part(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                           int ghost, const int* sel, const int64_t* off, int nsel, const void* buf,
+                           int64_t buf_doubles) {
+  if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
+  if (ghost != 2) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "the kernels require ghost == 2");
+  if (!blocks || nblocks <= 0) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "no blocks");
+  for (int b = 0; b < nblocks; ++b) {
+    int s = check_dims(ctx, blocks[b].ni, blocks[b].nj, blocks[b].nk);
+    if (s != FJ_OK) return s;
+  }
+  if (nlinks < 0 || (nlinks > 0 && !links)) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bad link list");
+  if (nsel < 0 || (nsel > 0 && (!sel || !off || !buf)) || buf_doubles < 0)
+    return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "bad selection or buffer");
+  return FJ_OK;
+}
+
+int fj_halo_pack_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks, int ghost,
+                     const int* sel, const int64_t* off, int nsel, double* buf, int64_t buf_doubles, void* stream) {
+  int s = check_halo_part(ctx, blocks, nblocks, links, nlinks, ghost, sel, off, nsel, buf, buf_doubles);
+  if (s != FJ_OK) return s;
+  return halo_pack_unpack(ctx, blocks, nblocks, links, nlinks, ghost, sel, off, nsel, buf, buf_doubles, false,
+                          S(stream));
+}
+
+int fj_halo_unpack_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                       int ghost, const int* sel, const int64_t* off, int nsel, const double* buf,
+                       int64_t buf_doubles, void* stream) {
+  int s = check_halo_part(ctx, blocks, nblocks, links, nlinks, ghost, sel, off, nsel, buf, buf_doubles);
+  if (s != FJ_OK) return s;
+  return halo_pack_unpack(ctx, blocks, nblocks, links, nlinks, ghost, sel, off, nsel, const_cast<double*>(buf),
+                          buf_doubles, true, S(stream));
+}
+
 int fj_apply_bc_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs, int nbcs,
                     const fj_params* p, void* stream) {
   if (!ctx) return FJ_ERR_INVALID_ARGUMENT;
@@ -734,6 +769,20 @@ int fj_plan_set_ensemble(fj_plan* pl, const double* mu0, const double* dt) {
   if (mu0) pl->mu0_b.assign(mu0, mu0 + nb);
   if (dt) pl->dt_b.assign(dt, dt + nb);
   drop_graphs(pl);
+  return FJ_OK;
+}
+
+int fj_plan_p_ref(const fj_plan* pl, double* out) {
+  if (!pl || !out) return FJ_ERR_INVALID_ARGUMENT;
+  *out = pl->p_ref;
+  return FJ_OK;
+}
+
+int fj_plan_set_p_ref(fj_plan* pl, double p_ref) {
+  if (!pl) return FJ_ERR_INVALID_ARGUMENT;
+  if (!std::isfinite(p_ref)) return set_err(pl->ctx, FJ_ERR_INVALID_ARGUMENT, "p_ref must be finite");
+  if (p_ref != pl->p_ref) drop_graphs(pl);
+  pl->p_ref = p_ref;
   return FJ_OK;
 }
 

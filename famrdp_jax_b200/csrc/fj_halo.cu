@@ -244,6 +244,51 @@ int halo_exchange(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_lin
   return FJ_OK;
 }
 
+int halo_pack_unpack(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks, int ghost,
+                     const int* sel, const int64_t* off, int nsel, double* buf, int64_t buf_doubles, bool unpack,
+                     cudaStream_t st) {
+  if (nsel == 0) return FJ_OK;
+  std::vector<fj_link> chosen((size_t)nsel);
+  for (int i = 0; i < nsel; ++i) {
+    if (sel[i] < 0 || sel[i] >= nlinks) return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "selected link out of range");
+    chosen[(size_t)i] = links[sel[i]];
+  }
+  std::vector<HaloDesc> descs;
+  size_t nd = 0;
+  int s = build_links(ctx, blocks, nblocks, chosen.data(), nsel, ghost, descs, nd);
+  if (s != FJ_OK) return s;
+  for (int i = 0; i < nsel; ++i) {
+    HaloDesc& d = descs[(size_t)i];
+    const int64_t len = 5ll * d.ext[0] * d.ext[1] * d.ext[2];
+    if (off[i] < 0 || off[i] > buf_doubles - len)
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "slab offset outside the buffer");
+    // the block this call reads (pack: the source) or writes (unpack: the target)
+    if (!(unpack ? d.tgt : d.src))
+      return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, unpack ? "link target q is NULL" : "link source q is NULL");
+    d.off = off[i];
+  }
+  // one table per kMaxLinksPerLaunch links in selection order: a later table
+  // runs after an earlier one, so its slabs overwrite the earlier ones
+  for (int base = 0; base < nsel; base += kMaxLinksPerLaunch) {
+    HaloTable tab;
+    tab.n = std::min(kMaxLinksPerLaunch, nsel - base);
+    int64_t vmax = 0;
+    for (int t = 0; t < tab.n; ++t) {
+      tab.d[t] = descs[(size_t)(base + t)];
+      vmax = std::max<int64_t>(vmax, (int64_t)tab.d[t].ext[0] * tab.d[t].ext[1] * tab.d[t].ext[2]);
+    }
+    dim3 grid((unsigned)std::min<int64_t>(grid_for(unpack ? vmax : 5 * vmax), 4096), tab.n);
+    if (unpack)
+      pdl_launch(k_halo_scatter, grid, kThreads, 0, st, tab, (const double*)buf);
+    else
+      pdl_launch(k_halo_gather, grid, kThreads, 0, st, tab, buf);
+    ctx->launches += 1;
+    s = launch_status(ctx, unpack ? "halo unpack launch" : "halo pack launch");
+    if (s != FJ_OK) return s;
+  }
+  return FJ_OK;
+}
+
 int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs, int nbcs,
              const fj_params* p, cudaStream_t st) {
   for (int b = 0; b < nbcs; ++b) {

@@ -38,6 +38,14 @@ int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs,
              const fj_params* p, cudaStream_t st);
 // Bytes of scratch the halo gather needs for these links (0 on shape errors).
 size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, int ghost);
+// One device's part of a halo fill whose blocks live on several devices: the
+// links sel[0..nsel) have their source slabs gathered into buf (pack) or the
+// slabs in buf written into their targets in selection order (unpack), slab i
+// at buf + off[i] (5 x the target's ghost box, in the gather's order).  Blocks
+// whose q this call does not touch may have q == NULL.
+int halo_pack_unpack(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks, int ghost,
+                     const int* sel, const int64_t* off, int nsel, double* buf, int64_t buf_doubles, bool unpack,
+                     cudaStream_t st);
 
 // ---- adjoint (fj_adjoint.cu, fj_halo.cu) ----
 // Elementwise epilogue of an RHS VJP V = (dL/dq)^T lam, applied in the kernel

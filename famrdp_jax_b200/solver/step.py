@@ -92,6 +92,20 @@ class StepPlan:
         _capi.check(fn(self._handle, _topology.ptr_array(qs), _topology.ptr_array(outs), float(dt),
                        _capi.stream(self.device)), "fj_plan_step_graph" if graph else "fj_plan_step", c)
 
+    def p_ref(self) -> float:
+        """The FP32-flux pressure offset (the mean pressure over the plan's
+        padded cells at creation; 0.0 on FP64 plans)."""
+        out = ctypes.c_double()
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_p_ref(self._handle, ctypes.byref(out)), "fj_plan_p_ref", c)
+        return out.value
+
+    def set_p_ref(self, value: float) -> None:
+        """Sets the FP32-flux pressure offset (changes only the rounding of
+        FP32-flux results; plans of the shards of one topology share one)."""
+        c = _capi.ctx(self.device)
+        _capi.check(self._lib.fj_plan_set_p_ref(self._handle, float(value)), "fj_plan_set_p_ref", c)
+
     def set_ensemble(self, mu0=None, dt=None) -> None:
         """Per-block viscosity scale and time step (independent instances):
         block b then uses mu0[b] and dt[b], and the dt argument of run/stage is

@@ -213,6 +213,31 @@ int fj_rhs_noalloc_f64(const double* q, const double* kxyz, const double* vol, d
  * pre-exchange arrays; later links overwrite earlier ones. */
 int fj_halo_exchange_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks,
                          const fj_link* links, int nlinks, int ghost, void* stream);
+/* One device's part of mesh/halo.py:56-92 when the blocks of a topology live
+ * on several devices (block sharding; the reference is single-device and has
+ * no counterpart).  `blocks` lists EVERY block of the topology (dimensions
+ * always; q may be NULL for a block this call neither reads nor writes) and
+ * `links` the whole link list.  sel[0..nsel) selects links by index; slab i
+ * occupies buf[off[i] .. off[i] + 5*V_i), V_i = the cells of the target face's
+ * ghost box (g layers x the target block's two other extents), values in
+ * (variable, a, b, c) order over that box.
+ *   fj_halo_pack_f64:   gathers each selected link's source slab (the source
+ *                       blocks' q must be set) into buf;
+ *   fj_halo_unpack_f64: writes the slabs into the selected links' targets
+ *                       (their q must be set) in selection order; where the
+ *                       ghost boxes of two selected links of one target block
+ *                       overlap, the later one wins.
+ * A sharded fill is: pack every link whose source is local (before any
+ * unpack, so that all sources are pre-exchange values), move the slabs of
+ * links whose target lives elsewhere to that device, then unpack every link
+ * whose target is local in list order.  Returns FJ_ERR_INVALID_ARGUMENT for a
+ * slab outside [0, buf_doubles) or a NULL q the call needs. */
+int fj_halo_pack_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                     int ghost, const int* sel, const int64_t* off, int nsel, double* buf,
+                     int64_t buf_doubles, void* stream);
+int fj_halo_unpack_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links, int nlinks,
+                       int ghost, const int* sel, const int64_t* off, int nsel, const double* buf,
+                       int64_t buf_doubles, void* stream);
 /* physics/bc/dispatch.py:11-32 apply_bc for all blocks */
 int fj_apply_bc_f64(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs,
                     int nbcs, const fj_params* p, void* stream);
@@ -270,6 +295,14 @@ int fj_plan_set_ensemble(fj_plan* plan, const double* mu0, const double* dt);
  * the FJ_PLAN_MAX_GRAPHS most recently used graphs (a ping-pong loop uses
  * two). */
 #define FJ_PLAN_MAX_GRAPHS 4
+/* The FP32-flux pressure offset p_ref (the mean pressure over the plan's
+ * padded cells at creation; 0 for FP64 plans, which do not use it).  Setting
+ * it (any finite value) changes only the rounding of FP32-flux results; plans
+ * that hold the shards of one topology set the same value so that their steps
+ * match one plan over all blocks bit for bit.  Changing it drops captured
+ * graphs.  The reference has no counterpart. */
+int fj_plan_p_ref(const fj_plan* plan, double* out);
+int fj_plan_set_p_ref(fj_plan* plan, double p_ref);
 /* Launch shape of the plan's split kernels (either precision; the shapes
  * differ between FP32-flux and FP64): the register caps (minimum resident CTAs
  * per SM) of the flux and assembly kernels, one of FJ_NUM_SPLIT_VARIANTS; 0 is
