@@ -709,6 +709,86 @@ def run_ours(args):
     return 0
 
 
+def run_sharded(args):
+    """--shard: the workload's blocks partitioned over the ranks (one GPU
+    each), every step exchanging the face slabs of links that cross ranks
+    (famrdp_jax_b200.solver.sharded: one NCCL send and receive per peer and
+    step).  Strong scaling: the whole topology's cells over the slowest rank's
+    time.  With one rank the same path runs over a one-rank group."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from famrdp_jax_b200 import _topology, cases
+    from famrdp_jax_b200.mesh.metric import compute_metrics
+    from famrdp_jax_b200.solver import sharded
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if not dist.is_initialized():
+        if ws > 1:
+            dist.init_process_group("nccl", device_id=device)
+        else:
+            with socket.socket() as so:
+                so.bind(("127.0.0.1", 0))
+                port = so.getsockname()[1]
+            dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                    device_id=device)
+
+    def metrics_fn(xyz):
+        m = compute_metrics(torch.as_tensor(xyz, dtype=torch.float64, device=device), ghost=2)
+        return m.jac.cpu().numpy(), m.kxyz.cpu().numpy(), m.vol.cpu().numpy()
+
+    case = build_case(args, metrics_fn)
+    if "mu0" in case.meta and isinstance(case.meta["mu0"], list):
+        raise SystemExit("--shard: the ensemble's instances are independent; run it as replicas")
+    cfg = dataclasses.replace(case.cfg, precision=args.precision)
+    state = cases.to_state(case, device)
+    shapes = [tuple(b.q.shape) for b in state.blocks]
+    owner = sharded.partition(shapes, _topology.links(cfg.topology), ws)
+    local_state = sharded.shard_state(state, owner, rank)
+    del state
+    torch.cuda.empty_cache()
+    step = sharded.ShardedStep(shapes, owner, rank, local_state, cfg)
+    dt = sharded.cfl_dt(local_state, cfg, case.cfl)
+    step.share_p_ref()
+    qa = [b.q.clone() for b in local_state.blocks]
+    qb = [torch.empty_like(q) for q in qa]
+    for _ in range(max(args.warmup, 3)):
+        step.run(qa, qb, dt, graph=True)
+        qa, qb = qb, qa
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step.run(qa, qb, dt, graph=True)
+        qa, qb = qb, qa
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    cut = sum(1 for (tb, _tf, sb, _sf, _o) in step.links if owner[tb] != owner[sb])
+    if rank == 0:
+        line = {"metric": METRIC, "value": case.interior_cells * 3 * args.steps / (ms / 1e3) / 1e6, "unit": UNIT,
+                "n_gpus": ws, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "f64" else "f32-flux/f64-state", "data": "synthetic",
+                "config": workload_desc(case, args) | {"parallelism": f"blocks over {ws} ranks",
+                                                       "links_cut": cut, "links": len(step.links),
+                                                       "blocks_per_rank": [owner.count(r) for r in range(ws)]}}
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    del step
+    dist.destroy_process_group()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -718,6 +798,8 @@ def main(argv=None):
     ap.add_argument("--workload", choices=["wavy4", "tgv32", "tree24", "ensemble64"], default="wavy4")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--shard", action="store_true",
+                    help="partition the workload's blocks over the ranks (halo slabs exchanged every step)")
     ap.add_argument("--stage-only", action="store_true",
                     help="only run four standalone stage-2 evaluations (four steps with --kernel persistent), "
                          "for a profiler")
@@ -753,6 +835,8 @@ def main(argv=None):
         return 0
     if args.impl == "reference":
         return run_reference(args)
+    if args.shard:
+        return run_sharded(args)
     return run_ours(args)
 
 
