@@ -7,7 +7,8 @@ multi-device path.  Here each rank owns some of the blocks (``partition``),
 steps them with a local StepPlan, and the one halo fill per step moves the
 face slabs of links that cross ranks with one grouped send/receive per peer:
 
-  1. the step's start state is copied into the rank's work arrays;
+  1. the step's start state is copied into the output arrays (the local
+     plan then steps them in place);
   2. pack: the source slab of every link whose source block is local is
      gathered -- into the fill buffer when its target is local too, else into
      the export buffer's region for the target's rank.  All packs run before
@@ -225,15 +226,13 @@ class ShardedStep:
         self.schedule = halo_schedule(self.shapes, self.links, self.owner, rank, cfg.ghost)
         self.device = local.blocks[0].q.device if local.blocks else torch.device("cpu")
         self.plan = StepPlan(local, local_config(cfg, self.ids)) if self.ids else None
-        self.work = [torch.empty_like(b.q) for b in local.blocks]
         self.fill = torch.zeros(max(self.schedule.fill_doubles, 1), dtype=torch.float64, device=self.device)
         self.export = torch.zeros(max(self.schedule.export_doubles, 1), dtype=torch.float64, device=self.device)
-        # the C table: every block's dimensions, q set for the local ones (the work arrays)
+        # the C table: every block's dimensions; q of the local ones is set per
+        # call to the arrays being filled (_bind), the others stay NULL
         self._blocks = (_capi.FjBlock * len(self.shapes))()
         for b, s in enumerate(self.shapes):
             self._blocks[b].ni, self._blocks[b].nj, self._blocks[b].nk = s[1], s[2], s[3]
-        for b, w in zip(self.ids, self.work):
-            self._blocks[b].q = _capi.dev_ptr(w, f"work[{b}]")
         self._links = _topology.link_array(self.links)
 
         def sel(pairs):
@@ -278,22 +277,32 @@ class ShardedStep:
         _capi.check(fn(c, self._blocks, len(self.shapes), self._links, len(self.links), int(self.cfg.ghost), idx,
                        off, n, _capi.dev_ptr(buf, "slab buffer"), buf.numel(), _capi.stream(self.device)), name, c)
 
-    def pack(self, qs) -> None:
-        """Steps 1-2: qs (the local blocks' start states) into the work arrays
-        and every locally sourced slab into the fill or export buffer."""
-        if len(qs) != len(self.work):
-            raise ValueError("one state per local block expected")
-        for w, q in zip(self.work, qs):
-            w.copy_(q)
+    def _bind(self, arrays) -> None:
+        if len(arrays) != len(self.ids):
+            raise ValueError(f"one state per local block expected ({len(self.ids)}), got {len(arrays)}")
+        for b, a in zip(self.ids, arrays):
+            if tuple(a.shape) != self.shapes[b]:
+                raise ValueError(f"block {b}: shape {tuple(a.shape)} differs from {self.shapes[b]}")
+            self._blocks[b].q = _capi.dev_ptr(a, f"state[{b}]")
+
+    def pack(self, qs, outs) -> None:
+        """Steps 1-2: qs (the local blocks' start states) into outs and every
+        locally sourced slab into the fill or export buffer."""
+        self._bind(outs)
+        for o, q in zip(outs, qs):
+            if o.data_ptr() != q.data_ptr():
+                o.copy_(q)
         self._halo_part(self._pack_local, self.fill, False)
         self._halo_part(self._pack_export, self.export, False)
 
     def finish(self, outs, dt: float, graph: bool = False) -> None:
-        """Steps 4-5: the ghost slabs of the local blocks, then the local
-        plan's boundary conditions and stages, work arrays -> outs."""
+        """Steps 4-5: the ghost slabs of the local blocks (outs, as left by
+        ``pack``), then the local plan's boundary conditions and stages, in
+        place on outs."""
+        self._bind(outs)
         self._halo_part(self._unpack, self.fill, True)
         if self.plan is not None:
-            self.plan.run(self.work, outs, dt, graph=graph)
+            self.plan.run(outs, outs, dt, graph=graph)
 
     def run(self, qs, outs, dt: float, graph: bool = False) -> None:
         """One step of the local blocks, exchanging with the other ranks of
@@ -304,7 +313,7 @@ class ShardedStep:
             import torch.distributed as dist
             dist.barrier(group=self.group)
             self._connected = True
-        self.pack(qs)
+        self.pack(qs, outs)
         exchange(self.schedule, self.export, self.fill, self.group)
         self.finish(outs, dt, graph=graph)
 

@@ -64,8 +64,8 @@ def test_sharded_steps_match_one_plan(cuda_device, name, world, precision):
     for n in range(3):
         full.run(qa, qb, dt)
         qa, qb = qb, qa
-        for s, x in zip(steps, sa):
-            s.pack(x)
+        for s, x, y in zip(steps, sa, sb):
+            s.pack(x, y)
         sharded.exchange_in_process(steps)
         for s, y in zip(steps, sb):
             s.finish(y, dt, graph=n > 0)
