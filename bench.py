@@ -715,6 +715,7 @@ def run_sharded(args):
     (famrdp_jax_b200.solver.sharded: one NCCL send and receive per peer and
     step).  Strong scaling: the whole topology's cells over the slowest rank's
     time.  With one rank the same path runs over a one-rank group."""
+    import datetime
     import socket
 
     import torch
@@ -727,15 +728,16 @@ def run_sharded(args):
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
+    timeout = datetime.timedelta(seconds=120)  # ranks that wait for one another end with an error
     if not dist.is_initialized():
         if ws > 1:
-            dist.init_process_group("nccl", device_id=device)
+            dist.init_process_group("nccl", device_id=device, timeout=timeout)
         else:
             with socket.socket() as so:
                 so.bind(("127.0.0.1", 0))
                 port = so.getsockname()[1]
             dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
-                                    device_id=device)
+                                    device_id=device, timeout=timeout)
 
     def metrics_fn(xyz):
         m = compute_metrics(torch.as_tensor(xyz, dtype=torch.float64, device=device), ghost=2)
