@@ -722,8 +722,9 @@ def run_sharded(args):
     import torch.distributed as dist
 
     from famrdp_jax_b200 import _topology, cases
+    from famrdp_jax_b200.core.types import State
     from famrdp_jax_b200.mesh.metric import compute_metrics
-    from famrdp_jax_b200.solver import sharded
+    from famrdp_jax_b200.solver import diagnostics, sharded
 
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
@@ -744,8 +745,6 @@ def run_sharded(args):
         return m.jac.cpu().numpy(), m.kxyz.cpu().numpy(), m.vol.cpu().numpy()
 
     case = build_case(args, metrics_fn)
-    if "mu0" in case.meta and isinstance(case.meta["mu0"], list):
-        raise SystemExit("--shard: the ensemble's instances are independent; run it as replicas")
     cfg = dataclasses.replace(case.cfg, precision=args.precision)
     state = cases.to_state(case, device)
     shapes = [tuple(b.q.shape) for b in state.blocks]
@@ -755,6 +754,15 @@ def run_sharded(args):
     torch.cuda.empty_cache()
     step = sharded.ShardedStep(shapes, owner, rank, local_state, cfg)
     dt = sharded.cfl_dt(local_state, cfg, case.cfl)
+    if "mu0" in case.meta and isinstance(case.meta["mu0"], list):
+        # independent instances (no links between blocks): each its own mu0 and
+        # dt, every rank stepping its share of them
+        dts = [0.0] * len(shapes)
+        for b, blk, m in zip(step.ids, local_state.blocks, local_state.metrics):
+            dts[b] = diagnostics.cfl_dt(State(blocks=(blk,), metrics=(m,)), cfg, case.cfl)
+        t = torch.tensor(dts, dtype=torch.float64, device=device)
+        dist.all_reduce(t)  # every block's dt comes from its owner, the others add 0
+        step.set_ensemble(case.meta["mu0"], [float(x) for x in t.tolist()])
     step.share_p_ref()
     qa = [b.q.clone() for b in local_state.blocks]
     qb = [torch.empty_like(q) for q in qa]

@@ -266,6 +266,18 @@ class ShardedStep:
         self.set_p_ref(value)
         return value
 
+    def set_ensemble(self, mu0=None, dt=None) -> None:
+        """Per-block viscosity scale and time step for independent instances
+        (StepPlan.set_ensemble), given for EVERY block of the topology; each
+        rank keeps its own blocks' values."""
+        n = len(self.shapes)
+        for name, x in (("mu0", mu0), ("dt", dt)):
+            if x is not None and len(x) != n:
+                raise ValueError(f"{name}: one value per block of the topology expected ({n})")
+        if self.plan is not None:
+            pick = (lambda x: None if x is None else [x[b] for b in self.ids])  # noqa: E731
+            self.plan.set_ensemble(pick(mu0), pick(dt))
+
     # -- one step --------------------------------------------------------------
     def _halo_part(self, which, buf: torch.Tensor, unpack: bool) -> None:
         idx, off, n = which

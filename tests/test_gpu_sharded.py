@@ -147,3 +147,41 @@ def test_sharded_run_through_a_process_group(cuda_device):
         assert all(torch.equal(a, b) for a, b in zip(sa, qa))
     finally:
         dist.destroy_process_group()
+
+
+def test_sharded_ensemble_matches_one_plan(cuda_device):
+    """Independent instances (each block its own mu0 and dt, no links between
+    blocks) spread over three shards step like one plan over all of them."""
+    from famrdp_jax_b200.core.types import State
+    c = cases.ensemble(ninst=7, n=10, seed=2)
+    state = cases.to_state(c, cuda_device)
+    cfg = c.cfg
+    mu0 = c.meta["mu0"]
+    dts = [diagnostics.cfl_dt(State(blocks=(b,), metrics=(m,)), cfg, c.cfl)
+           for b, m in zip(state.blocks, state.metrics)]
+    full = StepPlan(state, cfg)
+    full.set_ensemble(mu0, dts)
+    _, steps = _shards(state, cfg, 3)
+    assert cfg.precision == "f32"
+    for s in steps:
+        s.set_ensemble(mu0, dts)
+        s.set_p_ref(full.p_ref())
+        assert not s.schedule.send and not s.schedule.recv  # nothing crosses shards
+    with pytest.raises(ValueError):
+        steps[0].set_ensemble(mu0[:-1], None)
+    qa = [b.q.clone() for b in state.blocks]
+    qb = [torch.empty_like(q) for q in qa]
+    sa = [[qa[b].clone() for b in s.ids] for s in steps]
+    sb = [[torch.empty_like(q) for q in x] for x in sa]
+    for _ in range(3):
+        full.run(qa, qb, 0.0)
+        qa, qb = qb, qa
+        for s, x, y in zip(steps, sa, sb):
+            s.pack(x, y)
+        sharded.exchange_in_process(steps)
+        for s, y in zip(steps, sb):
+            s.finish(y, 0.0)
+        sa, sb = sb, sa
+    for s, x in zip(steps, sa):
+        for b, q in zip(s.ids, x):
+            assert torch.equal(q, qa[b]), b
