@@ -335,10 +335,32 @@ def cfl_dt(local: State, cfg: Config, cfl: float | None = None, group=None) -> f
     blocks, then the minimum over the ranks (an all-reduce)."""
     import torch.distributed as dist
     dt = diagnostics.cfl_dt(local, cfg, cfl) if local.blocks else float("inf")
+    return _all_reduce([dt], local, group, dist.ReduceOp.MIN)[0]
+
+
+def _all_reduce(values, local: State, group, op=None):
+    import torch.distributed as dist
     dev = local.blocks[0].q.device if local.blocks else torch.device("cpu")
-    t = torch.tensor([dt], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MIN, group=group)
-    return float(t.item())
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM if op is None else op, group=group)
+    return t.tolist()
+
+
+def kinetic_energy(local: State, ghost: int = 2, group=None) -> float:
+    """J over the whole topology: the ranks' sums over their blocks' interior
+    cells, added (an all-reduce)."""
+    j = diagnostics.kinetic_energy(local, ghost) if local.blocks else 0.0
+    return _all_reduce([j], local, group)[0]
+
+
+def residual(local: State, prev, dt: float, ghost: int = 2, group=None) -> list[float]:
+    """diagnostics.residual over the whole topology: each rank's per-component
+    RMS weighted by its interior cells, combined (an all-reduce)."""
+    n = float(sum((b.q.shape[1] - 2 * ghost) * (b.q.shape[2] - 2 * ghost) * (b.q.shape[3] - 2 * ghost)
+                  for b in local.blocks))
+    r = diagnostics.residual(local, prev, dt, ghost) if local.blocks else [0.0] * 5
+    tot = _all_reduce([x * x * n for x in r] + [n], local, group)
+    return [(x / tot[5]) ** 0.5 for x in tot[:5]]
 
 
 def shard_state(state: State, owner, rank: int) -> State:

@@ -145,6 +145,12 @@ def test_sharded_run_through_a_process_group(cuda_device):
             qa, qb, sa, sb = qb, qa, sb, sa
         torch.cuda.synchronize()
         assert all(torch.equal(a, b) for a, b in zip(sa, qa))
+        done = sharded.shard_state(dataclasses.replace(state, blocks=tuple(
+            dataclasses.replace(b, q=q) for b, q in zip(state.blocks, sa))), owner, 0)
+        assert sharded.kinetic_energy(done) == diagnostics.kinetic_energy(done)
+        res = sharded.residual(done, sb, dt)
+        ref = diagnostics.residual(done, sb, dt)
+        assert all(abs(a - b) <= 1e-12 * abs(b) for a, b in zip(res, ref)) and max(ref) > 0
     finally:
         dist.destroy_process_group()
 
