@@ -1,8 +1,11 @@
 // fj_pointwise.cu -- the per-cell / per-face building blocks of the hot path
 // exposed on their own (EOS, MUSCL-2, Roe, the RK3 combine), running the same
-// device functions the RHS kernels inline.
+// device functions the RHS kernels inline -- and the plan step's state copy.
 #include "fj_common.cuh"
 #include "fj_physics.cuh"
+#include "fj_rhs.cuh"
+
+#include <algorithm>
 
 namespace fj {
 
@@ -78,6 +81,52 @@ int pw_limiter(const double* a, const double* b, double* out, int64_t n, int lim
                cudaStream_t st) {
   k_limiter<<<grid_for(n), kThreads, 0, st>>>(a, b, out, n, limiter);
   return cudaGetLastError() == cudaSuccess ? FJ_OK : FJ_ERR_CUDA;
+}
+
+// Copies of whole state arrays (one per block, src[b] -> dst[b], len[b]
+// doubles) in one launch: blockIdx.y is the block, 16-byte accesses where both
+// pointers allow.  Launched with pdl_launch: the sources may be the previous
+// step's results.
+__global__ void k_copy_states(const CopyTable t) {
+  grid_dep_wait();
+  const int b = blockIdx.y;
+  const double* __restrict__ s = t.src[b];
+  double* __restrict__ d = t.dst[b];
+  const int64_t n = t.len[b];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d)) & 15) == 0) {
+    const int64_t n2 = n >> 1;
+    for (int64_t i = i0; i < n2; i += stride)
+      reinterpret_cast<double2*>(d)[i] = reinterpret_cast<const double2*>(s)[i];
+    if ((n & 1) && i0 == 0) d[n - 1] = s[n - 1];
+  } else {
+    for (int64_t i = i0; i < n; i += stride) d[i] = s[i];
+  }
+}
+
+int copy_states(const double* const* src, double* const* dst, const int64_t* len, int n, cudaStream_t st,
+                int64_t* launches) {
+  for (int base = 0; base < n; base += kMaxCopyBlocks) {
+    CopyTable t;
+    t.n = std::min(kMaxCopyBlocks, n - base);
+    int64_t longest = 0;
+    for (int i = 0; i < t.n; ++i) {
+      t.src[i] = src[base + i];
+      t.dst[i] = dst[base + i];
+      t.len[i] = len[base + i];
+      longest = std::max(longest, t.len[i]);
+    }
+    if (longest == 0) continue;
+    // about eight 256-thread CTAs per SM over all blocks of the launch, at most
+    // one per 512 doubles of the longest block
+    const int64_t per_block = std::max<int64_t>(1, 148 * 8 / t.n);
+    const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(per_block, (longest + 511) / 512));
+    cudaError_t e = pdl_launch(k_copy_states, dim3(gx, (unsigned)t.n), kThreads, 0, st, t);
+    if (e != cudaSuccess) return FJ_ERR_CUDA;
+    if (launches) *launches += 1;
+  }
+  return FJ_OK;
 }
 
 __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, int64_t n) {

@@ -29,6 +29,19 @@ cudaError_t staged_rhs_noctx(const double* q, const double* kxyz, const double* 
                              double* out, int ni, int nj, int nk, const Phys& ph, void* ws,
                              cudaStream_t st);
 
+// Whole-array copies src[b] -> dst[b] (len[b] doubles each, non-overlapping)
+// as SM kernels (fj_pointwise.cu), kMaxCopyBlocks arrays per launch;
+// *launches (if set) counts the launches.
+constexpr int kMaxCopyBlocks = 64;
+struct CopyTable {
+  int n;
+  const double* src[kMaxCopyBlocks];
+  double* dst[kMaxCopyBlocks];
+  int64_t len[kMaxCopyBlocks];
+};
+int copy_states(const double* const* src, double* const* dst, const int64_t* len, int n, cudaStream_t st,
+                int64_t* launches);
+
 // Halo fill + boundary conditions (fj_halo.cu), in place on blocks[].q.
 // `scratch` holds the gathered source slabs (halo_ws_bytes of them).
 int halo_exchange(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_link* links,
