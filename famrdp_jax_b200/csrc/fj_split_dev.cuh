@@ -102,9 +102,10 @@ __device__ __forceinline__ bool decode_cell(const Dev& d, int64_t c, Cell& x) {
   return true;
 }
 
-// The cell of this thread in flux / primitive CTA `cta` of the table.
-__device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x) {
-  return decode_cell(d, (int64_t)(cta - d.blk.cta_begin) * kSplitThreads + threadIdx.x, x);
+// The cell of this thread in flux / primitive CTA `cta` of the table (CTAs of
+// `cells` threads, one cell each).
+__device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x, int cells = kSplitThreads) {
+  return decode_cell(d, (int64_t)(cta - d.blk.cta_begin) * cells + threadIdx.x, x);
 }
 
 // ---- record access -------------------------------------------------------
@@ -120,11 +121,11 @@ constexpr int kRecP64 = 6;  // FP64 primitive record: rho, u, v, w, p, T (48 byt
 // fetched by earlier CTAs.  FIELD: the FP64 path (48-byte primitive records,
 // FP64 field-major kxyz).
 template <typename T, bool K_AOS, bool FIELD>
-__device__ __forceinline__ void prefetch_fluxes(const Dev& d, int cta) {
+__device__ __forceinline__ void prefetch_fluxes(const Dev& d, int cta, int cells = kSplitThreads) {
   const SplitBlock& B = d.blk;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk, si = (int64_t)B.nj * B.nk;
-  const int64_t c0 = (int64_t)(cta - B.cta_begin) * kSplitThreads;
-  const int64_t n = min((int64_t)kSplitThreads, N - c0);
+  const int64_t c0 = (int64_t)(cta - B.cta_begin) * cells;
+  const int64_t n = min((int64_t)cells, N - c0);
   const int64_t a2 = c0 + 2 * si, m2 = min(n, N - a2);
   const int rec = FIELD ? kRecP64 : kRecP;
   if (m2 > 0) l2_prefetch((const T*)B.prim + a2 * rec, m2 * rec * (int64_t)sizeof(T));
@@ -138,11 +139,11 @@ __device__ __forceinline__ void prefetch_fluxes(const Dev& d, int cta) {
 }
 
 // The L2 fill of the state range of primitive CTA `cta` (thread 0 only).
-__device__ __forceinline__ void prefetch_state(const Dev& d, int cta) {
+__device__ __forceinline__ void prefetch_state(const Dev& d, int cta, int cells = kSplitThreads) {
   const SplitBlock& B = d.blk;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
-  const int64_t c0 = (int64_t)(cta - B.cta_begin) * kSplitThreads;
-  const int64_t n = min((int64_t)kSplitThreads, N - c0);
+  const int64_t c0 = (int64_t)(cta - B.cta_begin) * cells;
+  const int64_t n = min((int64_t)cells, N - c0);
   for (int v = 0; v < 5; ++v) l2_prefetch(B.q + v * N + c0, n * 8);
 }
 

@@ -40,41 +40,44 @@ namespace {
 
 using namespace sd;
 
-template <typename T>
-__global__ void __launch_bounds__(kSplitThreads) k_split_prims(const Table tab, const double gm1,
-                                                              const double R, const double iR,
-                                                              const double p_ref) {
+// NW: warps per CTA.  8 normally; 2 for tables too small to give every SM two
+// 256-thread CTAs (the 32^3 block: 183 CTAs of 256 would leave a fifth of the
+// SMs with twice the work), with the same register caps (OCC counts
+// 256-thread CTAs).
+template <typename T, int NW = 8>
+__global__ void __launch_bounds__(32 * NW) k_split_prims(const Table tab, const double gm1, const double R,
+                                                         const double iR, const double p_ref) {
   const int b = find_block(tab, blockIdx.x);
-  if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
+  if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x, 32 * NW);
   grid_dep_wait();
   const SplitBlock& B = tab.b[b].blk;
-  const int32_t c = (blockIdx.x - B.cta_begin) * kSplitThreads + threadIdx.x;
+  const int32_t c = (blockIdx.x - B.cta_begin) * (32 * NW) + threadIdx.x;
   if (c >= B.ni * B.nj * B.nk) return;
   prims_cell<T>(B, c, gm1, R, iR, p_ref);
 }
 
-template <typename T, bool K_AOS, int OCC = SplitOcc<T>::fluxes>
-__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table tab, const Phys ph,
-                                                                     const int flags) {
+template <typename T, bool K_AOS, int OCC = SplitOcc<T>::fluxes, int NW = 8>
+__global__ void __launch_bounds__(32 * NW, OCC * 8 / NW) k_split_fluxes(const Table tab, const Phys ph,
+                                                                         const int flags) {
   const int b = find_block(tab, blockIdx.x);
-  if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x);
+  if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x, 32 * NW);
   grid_dep_wait();
   Cell x;
-  if (!decode(tab.b[b], blockIdx.x, x)) return;
+  if (!decode(tab.b[b], blockIdx.x, x, 32 * NW)) return;
   flux_cell<T, K_AOS, true>(tab.b[b].blk, tab.b[b].blk.prim, x, ph, flags);
 }
 
-template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
-__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Table tab, const int flags,
-                                                                       const int stage, const int next_prims,
-                                                                       const double gm1, const double R,
-                                                                       const double iR, const Phys ph) {
+template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble, int NW = 8>
+__global__ void __launch_bounds__(32 * NW, OCC * 8 / NW) k_split_assemble(const Table tab, const int flags,
+                                                                           const int stage, const int next_prims,
+                                                                           const double gm1, const double R,
+                                                                           const double iR, const Phys ph) {
   const int b = find_block_asm(tab, blockIdx.x);
   const Dev& d = tab.b[b];
   const SplitBlock& B = d.blk;
-  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
+  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, 31 * NW, B.cta_begin_asm);
   grid_dep_wait();
-  asm_chunk<T, K_AOS, true>(d, TablePtrs{B}, (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells, flags, stage,
+  asm_chunk<T, K_AOS, true>(d, TablePtrs{B}, (int64_t)(blockIdx.x - B.cta_begin_asm) * (31 * NW), flags, stage,
                             next_prims, gm1, R, iR, ph);
 }
 
@@ -484,20 +487,28 @@ void launch_pair64(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int
              ph.R, 1.0 / ph.R, ph);
 }
 
-template <typename T, bool K_AOS, int V>
+template <typename T, bool K_AOS, int V, int NW = 8>
 void launch_pair(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, int np,
                  cudaStream_t st, cudaEvent_t after_fluxes) {
   constexpr SplitShape sh = kSplitVariants[V];
-  pdl_launch(k_split_fluxes<T, K_AOS, sh.flux_occ>, ctas, kSplitThreads, 0, st, tab, ph, flags);
+  pdl_launch(k_split_fluxes<T, K_AOS, sh.flux_occ, NW>, ctas, 32 * NW, 0, st, tab, ph, flags);
   if (after_fluxes) cudaEventRecord(after_fluxes, st);
-  pdl_launch(k_split_assemble<T, K_AOS, sh.asm_occ>, asm_ctas, kSplitThreads, 0, st, tab, flags, stage, np, ph.gm1,
+  pdl_launch(k_split_assemble<T, K_AOS, sh.asm_occ, NW>, asm_ctas, 32 * NW, 0, st, tab, flags, stage, np, ph.gm1,
              ph.R, 1.0 / ph.R, ph);
 }
 
 template <typename T, bool K_AOS>
 int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, bool prims_ready,
-               bool next_prims, int variant, cudaStream_t st, cudaEvent_t after_fluxes) {
+               bool next_prims, int variant, cudaStream_t st, cudaEvent_t after_fluxes, int nw = 8) {
   const int np = next_prims ? 1 : 0;
+  if constexpr (sizeof(T) == 4) {
+    if (nw == 2) {  // a small table: 2-warp CTAs, the default shape's register caps
+      if (!prims_ready)
+        pdl_launch(k_split_prims<T, 2>, ctas, 64, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R, K_AOS ? ph.p_ref : 0.0);
+      launch_pair<T, K_AOS, 0, 2>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes);
+      return prims_ready ? 2 : 3;
+    }
+  }
   if constexpr (sizeof(T) == 8) {
     if (!prims_ready) pdl_launch(fm::k_fm_prims<double>, ctas, kSplitThreads, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R);
     switch (variant) {
@@ -527,9 +538,23 @@ template <typename T>
 int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys& ph, int flags,
                  int stage, bool prims_ready, bool next_prims, int variant, cudaStream_t st,
                  cudaEvent_t after_fluxes) {
+  static int sms = 0;  // SMs of the device (B200: 148)
+  if (sms == 0 && (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess || sms <= 0))
+    sms = 148;
   for (int base = 0; base < nblocks; base += kMaxSplitBlocks) {
     Table tab;
     tab.n = std::min(kMaxSplitBlocks, nblocks - base);
+    // FP32 tables with fewer 256-thread flux CTAs than two per SM run 2-warp CTAs
+    int nw = 8;
+    if (sizeof(T) == 4) {
+      int64_t wide = 0;
+      for (int t = 0; t < tab.n; ++t) {
+        const SplitBlock& sb = blocks[base + t];
+        wide += ((int64_t)sb.ni * sb.nj * sb.nk + kSplitThreads - 1) / kSplitThreads;
+      }
+      if (wide < 2 * (int64_t)sms) nw = 2;
+    }
+    const int fcells = 32 * nw, acells = 31 * nw;
     int ctas = 0, asm_ctas = 0;
     const bool k_aos = blocks[base].kaos != nullptr;
     for (int t = 0; t < tab.n; ++t) {
@@ -545,17 +570,17 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
       tab.b[t].dk.init((uint32_t)sb.nk);
       tab.b[t].dj.init((uint32_t)sb.nj);
       const int64_t N = (int64_t)sb.ni * sb.nj * sb.nk;
-      ctas += (int)((N + kSplitThreads - 1) / kSplitThreads);
-      asm_ctas += (int)((N + kAsmCells - 1) / kAsmCells);
+      ctas += (int)((N + fcells - 1) / fcells);
+      asm_ctas += (int)((N + acells - 1) / acells);
     }
     if (k_aos && sizeof(T) == 8)
       return set_err(ctx, FJ_ERR_INVALID_ARGUMENT, "the FP64 split path reads kxyz directly");
     // the event marks the first chunk's flux launch
     cudaEvent_t ev = base == 0 ? after_fluxes : nullptr;
     ctx->launches += k_aos ? launch_tab<T, true>(tab, ctas, asm_ctas, ph, flags, stage, prims_ready, next_prims,
-                                                 variant, st, ev)
+                                                 variant, st, ev, nw)
                            : launch_tab<T, false>(tab, ctas, asm_ctas, ph, flags, stage, prims_ready, next_prims,
-                                                  variant, st, ev);
+                                                  variant, st, ev, nw);
     int s = launch_status(ctx, "split stage launch");
     if (s != FJ_OK) return s;
   }
