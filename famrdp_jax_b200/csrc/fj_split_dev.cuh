@@ -626,6 +626,93 @@ __device__ __forceinline__ void flux_cell(const SplitBlock& B, const void* prim,
   }
 }
 
+// The flux work of cell x split into three independent parts for the
+// role-split kernel of small FP32 tables (k_split_fluxes_roles): each part
+// loads only its own operands and writes only its own values, with the
+// same arithmetic as flux_cell (bit-identical results).
+// The viscous flux components G(c) (the record and Gz).
+template <typename T, bool K_AOS>
+__device__ __forceinline__ void flux_visc_part(const SplitBlock& B, const void* prim, const Cell& x,
+                                               const Phys& ph) {
+  static_assert(sizeof(T) == 4, "the role-split flux kernel is the FP32 records path");
+  using M = FastMath<T>;
+  const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
+  const int32_t si = x.nj * x.nk, sj = x.nk;
+  const T* __restrict__ P = (const T*)prim;
+  const int32_t ip = x.i + 1 == x.ni ? c - (x.ni - 1) * si : c + si;
+  const int32_t im = x.i == 0 ? c + (x.ni - 1) * si : c - si;
+  const int32_t jp = x.j + 1 == x.nj ? c - (x.nj - 1) * sj : c + sj;
+  const int32_t jm = x.j == 0 ? c + (x.nj - 1) * sj : c - sj;
+  const int32_t kp = x.k + 1 == x.nk ? c - (x.nk - 1) : c + 1;
+  const int32_t km = x.k == 0 ? c + (x.nk - 1) : c - 1;
+  const Cell6<T> C0 = load_cell<T, true>(P, c);
+  const Cell6<T> Im = load_cell<T, true>(P, im), Ip = load_cell<T, true>(P, ip);
+  const Cell6<T> Jm = load_cell<T, true>(P, jm), Jp = load_cell<T, true>(P, jp);
+  const Cell6<T> Km = load_cell<T, true>(P, km), Kp = load_cell<T, true>(P, kp);
+  T kk[9];
+  metric9<T, K_AOS>(B, N, c, kk);
+  const T h = T(0.5);
+  const T d[4][3] = {{h * (Ip.u - Im.u), h * (Jp.u - Jm.u), h * (Kp.u - Km.u)},
+                     {h * (Ip.v - Im.v), h * (Jp.v - Jm.v), h * (Kp.v - Km.v)},
+                     {h * (Ip.w - Im.w), h * (Jp.w - Jm.w), h * (Kp.w - Km.w)},
+                     {h * (Ip.t - Im.t), h * (Jp.t - Jm.t), h * (Kp.t - Km.t)}};
+  T g[4][3];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) g[s][m] = d[s][0] * kk[m] + d[s][1] * kk[3 + m] + d[s][2] * kk[6 + m];
+  T mu = (T)B.mu0;
+  if (ph.visc_law == 0) {  // Sutherland (physics/eos.py:24-25)
+    const T r = C0.t * (T)ph.inv_T0;
+    mu = (T)B.mu0 * (r * M::sqrt_pos(r)) * (T)ph.sfac * M::rcp(C0.t + (T)ph.Ts);
+  }
+  const T kappa = (T)ph.kap_fac * mu;
+  const T third = (T)(1.0 / 3.0);
+  const T div_u = g[0][0] + g[1][1] + g[2][2];
+  const T t00 = T(2) * mu * (g[0][0] - div_u * third);
+  const T t01 = mu * (g[0][1] + g[1][0]);
+  const T t02 = mu * (g[0][2] + g[2][0]);
+  const T t11 = T(2) * mu * (g[1][1] - div_u * third);
+  const T t12 = mu * (g[1][2] + g[2][1]);
+  const T t22 = T(2) * mu * (g[2][2] - div_u * third);
+  const T rec[kRecG] = {t00, t01, t02, t11, t12, t22,
+                        C0.u * t00 + C0.v * t01 + C0.w * t02 + kappa * g[3][0],
+                        C0.u * t01 + C0.v * t11 + C0.w * t12 + kappa * g[3][1]};
+  st_rec<T, kRecG>((T*)B.G + (size_t)c * kRecG, rec);
+  ((T*)B.Gz)[c] = C0.u * t02 + C0.v * t12 + C0.w * t22 + kappa * g[3][2];
+}
+
+// The Roe face c | c+e_AXIS (AXIS 0: i, 1: j) for c_a in [1, n_a-3], zeros
+// elsewhere: AXIS 0 writes floats 0..4 of the cell's face record, AXIS 1
+// floats 5..7 and the Fz pair.
+template <typename T, bool K_AOS, int AXIS>
+__device__ __forceinline__ void flux_face_part(const SplitBlock& B, const void* prim, const Cell& x,
+                                               const Phys& ph) {
+  static_assert(sizeof(T) == 4, "the role-split flux kernel is the FP32 records path");
+  const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
+  const int32_t sa = AXIS == 0 ? x.nj * x.nk : x.nk;
+  const int ia = AXIS == 0 ? x.i : x.j, na = AXIS == 0 ? x.ni : x.nj;
+  const T* __restrict__ P = (const T*)prim;
+  T F[5] = {T(0), T(0), T(0), T(0), T(0)};
+  if (ia >= 1 && ia <= na - 3) {
+    const Cell6<T> A0 = load_cell<T, true>(P, c - sa), A1 = load_cell<T, true>(P, c),
+                   A2 = load_cell<T, true>(P, c + sa), A3 = load_cell<T, true>(P, c + 2 * sa);
+    T kc[3], kn[3];
+    metric_row<T, K_AOS>(B, N, AXIS, c, kc);
+    metric_row<T, K_AOS>(B, N, AXIS, c + sa, kn);
+    face_from_cells<T, K_AOS>(A0, A1, A2, A3, kc, kn, ph, F, K_AOS ? (T)ph.p_ref : T(0));
+  }
+  T* rec = (T*)B.F + (size_t)c * kRecFA;
+  if (AXIS == 0) {
+    reinterpret_cast<float4*>(rec)[0] = make_float4(F[0], F[1], F[2], F[3]);
+    rec[4] = F[4];
+  } else {
+    rec[5] = F[0];
+    reinterpret_cast<float2*>(rec + 6)[0] = make_float2(F[1], F[2]);
+    reinterpret_cast<float2*>(B.Fz)[c] = make_float2(F[3], F[4]);
+  }
+}
+
 // Assembly of the kAsmCells cells from c0 of B (k_split_assemble; all 256
 // threads of the CTA call it).  The k faces are evaluated here: lane l of a
 // warp evaluates the face on the left of its cell (c-1 | c) and takes the one

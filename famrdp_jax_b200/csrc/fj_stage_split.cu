@@ -67,6 +67,30 @@ __global__ void __launch_bounds__(32 * NW, OCC * 8 / NW) k_split_fluxes(const Ta
   flux_cell<T, K_AOS, true>(tab.b[b].blk, tab.b[b].blk.prim, x, ph, flags);
 }
 
+// The flux work of small FP32 tables split by warp roles: a CTA of 192 threads
+// takes the 64 cells of one 2-warp flux CTA; warps 0-1 evaluate their cells'
+// i faces, warps 2-3 the j faces, warps 4-5 the viscous components.  Each
+// thread's dependency chain is about a third of k_split_fluxes' (a small
+// table leaves most of the GPU's warp slots free, and its kernels' times are
+// set by those chains).
+template <typename T, bool K_AOS>
+__global__ void __launch_bounds__(192, 5) k_split_fluxes_roles(const Table tab, const Phys ph, const int flags) {
+  const int b = find_block(tab, blockIdx.x);
+  if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x, 64);
+  grid_dep_wait();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const SplitBlock& B = tab.b[b].blk;
+  Cell x;
+  if (!decode_cell(tab.b[b], (int64_t)(blockIdx.x - B.cta_begin) * 64 + (warp & 1) * 32 + lane, x)) return;
+  if (warp < 2) {
+    if (flags & kRhsInvscd) flux_face_part<T, K_AOS, 0>(B, B.prim, x, ph);
+  } else if (warp < 4) {
+    if (flags & kRhsInvscd) flux_face_part<T, K_AOS, 1>(B, B.prim, x, ph);
+  } else if (flags & kRhsViscous) {
+    flux_visc_part<T, K_AOS>(B, B.prim, x, ph);
+  }
+}
+
 template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble, int NW = 8>
 __global__ void __launch_bounds__(32 * NW, OCC * 8 / NW) k_split_assemble(const Table tab, const int flags,
                                                                            const int stage, const int next_prims,
@@ -502,10 +526,14 @@ int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int fla
                bool next_prims, int variant, cudaStream_t st, cudaEvent_t after_fluxes, int nw = 8) {
   const int np = next_prims ? 1 : 0;
   if constexpr (sizeof(T) == 4) {
-    if (nw == 2) {  // a small table: 2-warp CTAs, the default shape's register caps
+    if (nw == 2) {  // a small table: the role-split flux kernel and 2-warp assembly CTAs
       if (!prims_ready)
         pdl_launch(k_split_prims<T, 2>, ctas, 64, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R, K_AOS ? ph.p_ref : 0.0);
-      launch_pair<T, K_AOS, 0, 2>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes);
+      pdl_launch(k_split_fluxes_roles<T, K_AOS>, ctas, 192, 0, st, tab, ph, flags);
+      if (after_fluxes) cudaEventRecord(after_fluxes, st);
+      constexpr SplitShape sh = kSplitVariants[0];
+      pdl_launch(k_split_assemble<T, K_AOS, sh.asm_occ, 2>, asm_ctas, 64, 0, st, tab, flags, stage, np, ph.gm1,
+                 ph.R, 1.0 / ph.R, ph);
       return prims_ready ? 2 : 3;
     }
   }
