@@ -31,6 +31,8 @@ struct SplitBlock {
   void* Fz;              // FP32 only: the last two j-face components, two per cell
   void* G;               // scratch: viscous flux components (records: 8 per cell)
   void* Gz;              // records only: the ninth component, one per cell
+  void* Fk;              // FP32 only: the k face c | c+1 of each cell, 5 per cell (written and read only
+                         // by the kernels of tables too small to fill the GPU; zero where no face exists)
   double mu0;            // viscosity scale of this block (per-instance ensembles)
   double dt;             // time step of this block (stages 1..3)
   int ni, nj, nk;

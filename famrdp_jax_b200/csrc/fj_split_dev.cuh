@@ -682,16 +682,16 @@ __device__ __forceinline__ void flux_visc_part(const SplitBlock& B, const void* 
   ((T*)B.Gz)[c] = C0.u * t02 + C0.v * t12 + C0.w * t22 + kappa * g[3][2];
 }
 
-// The Roe face c | c+e_AXIS (AXIS 0: i, 1: j) for c_a in [1, n_a-3], zeros
-// elsewhere: AXIS 0 writes floats 0..4 of the cell's face record, AXIS 1
-// floats 5..7 and the Fz pair.
+// The Roe face c | c+e_AXIS for c_a in [1, n_a-3], zeros elsewhere: AXIS 0
+// (i) writes floats 0..4 of the cell's face record, AXIS 1 (j) floats 5..7
+// and the Fz pair, AXIS 2 (k) the cell's 5 values of Fk.
 template <typename T, bool K_AOS, int AXIS>
 __device__ __forceinline__ void flux_face_part(const SplitBlock& B, const void* prim, const Cell& x,
                                                const Phys& ph) {
   static_assert(sizeof(T) == 4, "the role-split flux kernel is the FP32 records path");
   const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
-  const int32_t sa = AXIS == 0 ? x.nj * x.nk : x.nk;
-  const int ia = AXIS == 0 ? x.i : x.j, na = AXIS == 0 ? x.ni : x.nj;
+  const int32_t sa = AXIS == 0 ? x.nj * x.nk : (AXIS == 1 ? x.nk : 1);
+  const int ia = AXIS == 0 ? x.i : (AXIS == 1 ? x.j : x.k), na = AXIS == 0 ? x.ni : (AXIS == 1 ? x.nj : x.nk);
   const T* __restrict__ P = (const T*)prim;
   T F[5] = {T(0), T(0), T(0), T(0), T(0)};
   if (ia >= 1 && ia <= na - 3) {
@@ -701,6 +701,12 @@ __device__ __forceinline__ void flux_face_part(const SplitBlock& B, const void* 
     metric_row<T, K_AOS>(B, N, AXIS, c, kc);
     metric_row<T, K_AOS>(B, N, AXIS, c + sa, kn);
     face_from_cells<T, K_AOS>(A0, A1, A2, A3, kc, kn, ph, F, K_AOS ? (T)ph.p_ref : T(0));
+  }
+  if (AXIS == 2) {
+    T* fk = (T*)B.Fk + (size_t)c * 5;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) fk[v] = F[v];
+    return;
   }
   T* rec = (T*)B.F + (size_t)c * kRecFA;
   if (AXIS == 0) {
@@ -750,6 +756,44 @@ __device__ __forceinline__ void asm_chunk(const Dev& d, const SP& sp, int64_t c0
 #pragma unroll
   for (int v = 0; v < 5; ++v) fr[v] = __shfl_down_sync(0xffffffffu, fl[v], 1);
   if (lane == 31 || !alive) return;
+  assemble_cell<T, K_AOS>(B, sp, x, src, flags, stage, next_prims, gm1, R, iR, K_AOS ? ph.p_ref : 0.0, fl, fr, kk,
+                          gcl);
+}
+
+// asm_chunk with the k faces read from Fk (written by the k-face role of
+// k_split_fluxes_roles) instead of evaluated: the face c-1 | c (for k-1 in
+// [1, nk-3]) is Fk of c-1, the face c | c+1 is Fk of c (zero where it does not
+// exist).  The same values as asm_chunk's shuffled ones, so the same result.
+template <typename T, bool K_AOS, class SP>
+__device__ __forceinline__ void asm_chunk_kmem(const Dev& d, const SP& sp, int64_t c0, int flags, int stage,
+                                               int next_prims, double gm1, double R, double iR, const Phys& ph) {
+  const SplitBlock& B = d.blk;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t N = (int64_t)B.ni * B.nj * B.nk;
+  const int64_t c = c0 + warp * 31 + lane;
+  if (lane == 31 || c >= N) return;
+  Cell x;
+  const uint32_t t1 = d.dk.div((uint32_t)c);
+  x.k = (int)((uint32_t)c - t1 * (uint32_t)B.nk);
+  x.i = (int)d.dj.div(t1);
+  x.j = (int)(t1 - (uint32_t)x.i * (uint32_t)B.nj);
+  x.c = c;
+  x.N = N;
+  x.ni = B.ni;
+  x.nj = B.nj;
+  x.nk = B.nk;
+  const GlobalSrc<T, K_AOS, true> src{B, (int32_t)N};
+  T kk[9], gcl[3] = {T(0), T(0), T(0)};
+  src.K9((int32_t)c, kk, K_AOS ? gcl : nullptr);
+  T fl[5] = {T(0), T(0), T(0), T(0), T(0)}, fr[5] = {T(0), T(0), T(0), T(0), T(0)};
+  if (flags & kRhsInvscd) {
+    const T* fk = (const T*)B.Fk;
+    if (x.k >= 2 && x.k <= x.nk - 2)
+#pragma unroll
+      for (int v = 0; v < 5; ++v) fl[v] = __ldg(fk + (c - 1) * 5 + v);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) fr[v] = __ldg(fk + c * 5 + v);
+  }
   assemble_cell<T, K_AOS>(B, sp, x, src, flags, stage, next_prims, gm1, R, iR, K_AOS ? ph.p_ref : 0.0, fl, fr, kk,
                           gcl);
 }

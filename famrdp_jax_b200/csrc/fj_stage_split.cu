@@ -67,14 +67,15 @@ __global__ void __launch_bounds__(32 * NW, OCC * 8 / NW) k_split_fluxes(const Ta
   flux_cell<T, K_AOS, true>(tab.b[b].blk, tab.b[b].blk.prim, x, ph, flags);
 }
 
-// The flux work of small FP32 tables split by warp roles: a CTA of 192 threads
+// The flux work of small FP32 tables split by warp roles: a CTA of 256 threads
 // takes the 64 cells of one 2-warp flux CTA; warps 0-1 evaluate their cells'
-// i faces, warps 2-3 the j faces, warps 4-5 the viscous components.  Each
-// thread's dependency chain is about a third of k_split_fluxes' (a small
-// table leaves most of the GPU's warp slots free, and its kernels' times are
-// set by those chains).
+// i faces, warps 2-3 the j faces, warps 4-5 the viscous components and warps
+// 6-7 the k faces (into Fk, which k_split_assemble_kmem reads instead of
+// evaluating them).  Each thread's dependency chain is about a third of
+// k_split_fluxes' (a small table leaves most of the GPU's warp slots free,
+// and its kernels' times are set by those chains).
 template <typename T, bool K_AOS>
-__global__ void __launch_bounds__(192, 5) k_split_fluxes_roles(const Table tab, const Phys ph, const int flags) {
+__global__ void __launch_bounds__(256, 4) k_split_fluxes_roles(const Table tab, const Phys ph, const int flags) {
   const int b = find_block(tab, blockIdx.x);
   if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x, 64);
   grid_dep_wait();
@@ -86,9 +87,27 @@ __global__ void __launch_bounds__(192, 5) k_split_fluxes_roles(const Table tab, 
     if (flags & kRhsInvscd) flux_face_part<T, K_AOS, 0>(B, B.prim, x, ph);
   } else if (warp < 4) {
     if (flags & kRhsInvscd) flux_face_part<T, K_AOS, 1>(B, B.prim, x, ph);
-  } else if (flags & kRhsViscous) {
-    flux_visc_part<T, K_AOS>(B, B.prim, x, ph);
+  } else if (warp < 6) {
+    if (flags & kRhsViscous) flux_visc_part<T, K_AOS>(B, B.prim, x, ph);
+  } else if (flags & kRhsInvscd) {
+    flux_face_part<T, K_AOS, 2>(B, B.prim, x, ph);
   }
+}
+
+// The assembly of small FP32 tables: asm_chunk with the k faces read from Fk
+// (2-warp CTAs of 62 cells; a small table puts about five of them on an SM,
+// so the register cap is loose).
+template <typename T, bool K_AOS>
+__global__ void __launch_bounds__(64, 8) k_split_assemble_kmem(const Table tab, const int flags, const int stage,
+                                                                 const int next_prims, const double gm1,
+                                                                 const double R, const double iR, const Phys ph) {
+  const int b = find_block_asm(tab, blockIdx.x);
+  const Dev& d = tab.b[b];
+  const SplitBlock& B = d.blk;
+  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, 62, B.cta_begin_asm);
+  grid_dep_wait();
+  asm_chunk_kmem<T, K_AOS>(d, TablePtrs{B}, (int64_t)(blockIdx.x - B.cta_begin_asm) * 62, flags, stage, next_prims,
+                           gm1, R, iR, ph);
 }
 
 template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble, int NW = 8>
@@ -529,11 +548,10 @@ int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int fla
     if (nw == 2) {  // a small table: the role-split flux kernel and 2-warp assembly CTAs
       if (!prims_ready)
         pdl_launch(k_split_prims<T, 2>, ctas, 64, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R, K_AOS ? ph.p_ref : 0.0);
-      pdl_launch(k_split_fluxes_roles<T, K_AOS>, ctas, 192, 0, st, tab, ph, flags);
+      pdl_launch(k_split_fluxes_roles<T, K_AOS>, ctas, 256, 0, st, tab, ph, flags);
       if (after_fluxes) cudaEventRecord(after_fluxes, st);
-      constexpr SplitShape sh = kSplitVariants[0];
-      pdl_launch(k_split_assemble<T, K_AOS, sh.asm_occ, 2>, asm_ctas, 64, 0, st, tab, flags, stage, np, ph.gm1,
-                 ph.R, 1.0 / ph.R, ph);
+      pdl_launch(k_split_assemble_kmem<T, K_AOS>, asm_ctas, 64, 0, st, tab, flags, stage, np, ph.gm1, ph.R,
+                 1.0 / ph.R, ph);
       return prims_ready ? 2 : 3;
     }
   }
@@ -660,7 +678,10 @@ static void split_counts(int precision, int& nP, int& nF, int& nG) {
   // the stage input's primitives and the next stage's: the assembly reads the
   // first (its k faces) while writing the second
   nP = rec ? 2 * kRecP : 2 * kRecP64;
-  nF = rec ? kRecFA + kRecFB : 10;  // FP64: the i and j faces, field-major (the k faces stay in the assembly)
+  // FP32: the i/j face records and, for the kernels of small tables, the k
+  // faces (Fk, 5 per cell); FP64: the i and j faces, field-major (the k faces
+  // stay in the assembly)
+  nF = rec ? kRecFA + kRecFB + 5 : 10;
   nG = 9;  // records: kRecG per cell in G, then one per cell in Gz
 }
 
@@ -692,9 +713,11 @@ void split_assign_scratch(int precision, SplitBlock* blocks, int nblocks, void* 
     if (precision == FJ_PREC_F32FLUX) {
       blocks[b].F = F + kRecFA * off * t;
       blocks[b].Fz = F + (kRecFA * total + kRecFB * off) * t;
+      blocks[b].Fk = F + ((kRecFA + kRecFB) * total + 5 * off) * t;
     } else {
       blocks[b].F = F + nF * off * t;
       blocks[b].Fz = nullptr;
+      blocks[b].Fk = nullptr;
     }
     if (precision == FJ_PREC_F32FLUX) {
       blocks[b].G = G + kRecG * off * t;
