@@ -251,7 +251,20 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
   const int variant = o.variant;
   std::vector<fj_block> out(blocks, blocks + nblocks);
   int s;
-  {
+  const bool persist = ctx->pipeline == FJ_PIPELINE_SPLIT && o.persist && p->precision == FJ_PREC_F32FLUX && kmet;
+  const bool fused_fill = ctx->pipeline == FJ_PIPELINE_SPLIT && o.fill && p->precision == FJ_PREC_F32FLUX && kmet;
+  // the copy and the halo fill as one kernel where the step is not in place
+  // (its sources are then the untouched input states); the persistent and
+  // fused-fill paths fill the halo themselves
+  bool filled = false;
+  bool apart = nlinks > 0 && !persist && !fused_fill;
+  for (int b = 0; b < nblocks && apart; ++b) apart = q0p[b] != blocks[b].q;
+  if (apart) {
+    s = copy_fill(ctx, blocks, q0p, nblocks, links, nlinks, p->ghost, st, &filled);
+    if (s != FJ_OK) return s;
+  }
+  for (int b = 0; b < nblocks; ++b) out[b].q = q0p[b];
+  if (!filled) {
     // the step's start state into q0p (where the halo, the BCs and the stages
     // work) by an SM copy kernel: captured into a step graph, a memcpy node
     // made graph replays 2-4 % slower than plain launches
@@ -270,16 +283,17 @@ int step_body(fj_ctx* ctx, const fj_block* blocks, double* const* q0p, double* c
       return cuda_status(ctx, cudaGetLastError(), "state copy");
   }
   // the persistent kernel: halo, BCs and the three stages in one launch
-  if (ctx->pipeline == FJ_PIPELINE_SPLIT && o.persist && p->precision == FJ_PREC_F32FLUX && kmet)
+  if (persist)
     return persist_step(ctx, *o.persist, out.data(), nblocks, q1s, q2s, q_out, p, o.p_ref, mu0_b, dt_b, dt, kmet,
                         tail, o.wait_limit, st);
-  const bool fused_fill = ctx->pipeline == FJ_PIPELINE_SPLIT && o.fill && p->precision == FJ_PREC_F32FLUX && kmet;
   if (fused_fill) {
     s = persist_step(ctx, *o.fill, out.data(), nblocks, q1s, q2s, q_out, p, o.p_ref, mu0_b, dt_b, dt, kmet, tail,
                      o.wait_limit, st, true);
   } else {
-    s = halo_exchange(ctx, out.data(), nblocks, links, nlinks, p->ghost, (double*)tail, tail_b, st);
-    if (s != FJ_OK) return s;
+    if (!filled) {
+      s = halo_exchange(ctx, out.data(), nblocks, links, nlinks, p->ghost, (double*)tail, tail_b, st);
+      if (s != FJ_OK) return s;
+    }
     s = apply_bc(ctx, out.data(), nblocks, bcs, nbcs, p, st);
   }
   if (s != FJ_OK) return s;

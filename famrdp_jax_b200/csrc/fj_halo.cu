@@ -289,6 +289,107 @@ int halo_pack_unpack(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_
   return FJ_OK;
 }
 
+namespace {
+
+// The step's state copy with the halo fill folded in (copy_fill): per block
+// the source and destination state, its dimensions and its links (indices
+// into the HaloTable, grouped by target block, in list order within a block).
+// Block b owns the CTAs [cta_begin[b], cta_begin[b+1]), `cells` cells each
+// (CTAs in proportion to the block's cells): one per thread for tables that
+// would not give every SM 16 CTAs so (their time is the per-thread latency),
+// else four.
+constexpr int kMaxFillBlocks = 64;
+struct CopyFillTable {
+  int nb, ghost, cells;
+  const double* src[kMaxFillBlocks];
+  double* dst[kMaxFillBlocks];
+  int n[kMaxFillBlocks][3];
+  int cta_begin[kMaxFillBlocks + 1];
+  short first[kMaxFillBlocks], count[kMaxFillBlocks];
+  short order[kMaxLinksPerLaunch];
+};
+static_assert(sizeof(HaloTable) + sizeof(CopyFillTable) <= 32000, "kernel parameter space");
+
+// dst[b] := src[b] cell by cell, except the ghost cells a link of block b
+// covers: those take the source cell of the LAST such link (list order), read
+// from the source block's src, i.e. from the pre-exchange states (src is
+// never written here).  The same values as a copy followed by the gather and
+// the ordered scatter.
+__global__ void k_copy_fill(const HaloTable tab, const CopyFillTable ct) {
+  grid_dep_wait();
+  int b = 0;
+  while (b + 1 < ct.nb && ct.cta_begin[b + 1] <= (int)blockIdx.x) ++b;
+  const int ni = ct.n[b][0], nj = ct.n[b][1], nk = ct.n[b][2], g = ct.ghost;
+  const uint32_t N = (uint32_t)ni * nj * nk;  // < 2^31, checked on the host
+  const double* __restrict__ s = ct.src[b];
+  double* __restrict__ d = ct.dst[b];
+  const int e0 = ct.first[b], e1 = ct.first[b] + ct.count[b];
+  const uint32_t c0 = (uint32_t)(blockIdx.x - ct.cta_begin[b]) * (uint32_t)ct.cells;
+  for (uint32_t c = c0 + threadIdx.x; c < N && c < c0 + (uint32_t)ct.cells; c += kThreads) {
+    const uint32_t t = c / (uint32_t)nk;
+    const int k = (int)(c - t * (uint32_t)nk);
+    const int i = (int)(t / (uint32_t)nj), j = (int)(t - (uint32_t)i * (uint32_t)nj);
+    int L = -1;
+    if (i < g || i >= ni - g || j < g || j >= nj - g || k < g || k >= nk - g)
+      for (int e = e1 - 1; e >= e0 && L < 0; --e)
+        if (slab_covers(tab.d[ct.order[e]], i, j, k)) L = ct.order[e];
+    if (L < 0) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) d[(size_t)v * N + c] = s[(size_t)v * N + c];
+    } else {
+      const HaloDesc& h = tab.d[L];
+      const int64_t NS = (int64_t)h.sn[0] * h.sn[1] * h.sn[2];
+      const int64_t si = h.s0 + (i - h.tlo[0]) * h.sstr[0] + (j - h.tlo[1]) * h.sstr[1] + (k - h.tlo[2]) * h.sstr[2];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) d[(size_t)v * N + c] = h.src[v * NS + si];
+    }
+  }
+}
+
+}  // namespace
+
+int copy_fill(fj_ctx* ctx, const fj_block* blocks, double* const* dst, int nblocks, const fj_link* links, int nlinks,
+              int ghost, cudaStream_t st, bool* done) {
+  *done = false;
+  if (nblocks > kMaxFillBlocks || nlinks > kMaxLinksPerLaunch) return FJ_OK;  // the separate copy and fill
+  for (int b = 0; b < nblocks; ++b)
+    if ((int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk >= ((int64_t)1 << 31)) return FJ_OK;
+  std::vector<HaloDesc> descs;
+  size_t nd = 0;
+  int s = build_links(ctx, blocks, nblocks, links, nlinks, ghost, descs, nd);
+  if (s != FJ_OK) return s;
+  HaloTable tab;
+  tab.n = (int)descs.size();
+  for (int L = 0; L < tab.n; ++L) tab.d[L] = descs[(size_t)L];
+  CopyFillTable ct;
+  ct.nb = nblocks;
+  ct.ghost = ghost;
+  int pos = 0;
+  int64_t ctas = 0, narrow = 0;
+  for (int b = 0; b < nblocks; ++b) narrow += ((int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk + kThreads - 1) / kThreads;
+  ct.cells = narrow < 16 * 148 ? kThreads : 4 * kThreads;
+  for (int b = 0; b < nblocks; ++b) {
+    ct.src[b] = blocks[b].q;
+    ct.dst[b] = dst[b];
+    ct.n[b][0] = blocks[b].ni;
+    ct.n[b][1] = blocks[b].nj;
+    ct.n[b][2] = blocks[b].nk;
+    ct.first[b] = (short)pos;
+    for (int L = 0; L < tab.n; ++L)
+      if (tab.d[L].tgt_block == b) ct.order[pos++] = (short)L;
+    ct.count[b] = (short)(pos - ct.first[b]);
+    ct.cta_begin[b] = (int)ctas;
+    ctas += ((int64_t)blocks[b].ni * blocks[b].nj * blocks[b].nk + ct.cells - 1) / ct.cells;
+  }
+  ct.cta_begin[nblocks] = (int)ctas;
+  if (ctas == 0) return FJ_OK;
+  pdl_launch(k_copy_fill, dim3((unsigned)ctas), kThreads, 0, st, tab, ct);
+  ctx->launches += 1;
+  s = launch_status(ctx, "copy-fill launch");
+  if (s == FJ_OK) *done = true;
+  return s;
+}
+
 int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs, int nbcs,
              const fj_params* p, cudaStream_t st) {
   for (int b = 0; b < nbcs; ++b) {

@@ -49,6 +49,12 @@ int halo_exchange(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_lin
                   cudaStream_t st);
 int apply_bc(fj_ctx* ctx, const fj_block* blocks, int nblocks, const fj_bc* bcs, int nbcs,
              const fj_params* p, cudaStream_t st);
+// The step's start state blocks[b].q -> dst[b] with the halo fill of `links`
+// folded in (one kernel over all blocks; dst must not overlap blocks[].q).
+// *done = false, without launching, when the link or block count exceeds one
+// launch's table: the caller then copies and fills separately.
+int copy_fill(fj_ctx* ctx, const fj_block* blocks, double* const* dst, int nblocks, const fj_link* links, int nlinks,
+              int ghost, cudaStream_t st, bool* done);
 // Bytes of scratch the halo gather needs for these links (0 on shape errors).
 size_t halo_ws_bytes(const fj_block* blocks, const fj_link* links, int nlinks, int ghost);
 // One device's part of a halo fill whose blocks live on several devices: the
