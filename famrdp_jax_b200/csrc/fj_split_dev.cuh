@@ -102,10 +102,9 @@ __device__ __forceinline__ bool decode_cell(const Dev& d, int64_t c, Cell& x) {
   return true;
 }
 
-// The cell of this thread in flux / primitive CTA `cta` of the table (CTAs of
-// `cells` threads, one cell each).
-__device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x, int cells = kSplitThreads) {
-  return decode_cell(d, (int64_t)(cta - d.blk.cta_begin) * cells + threadIdx.x, x);
+// The cell of this thread in flux / primitive CTA `cta` of the table.
+__device__ __forceinline__ bool decode(const Dev& d, int cta, Cell& x) {
+  return decode_cell(d, (int64_t)(cta - d.blk.cta_begin) * kSplitThreads + threadIdx.x, x);
 }
 
 // ---- record access -------------------------------------------------------

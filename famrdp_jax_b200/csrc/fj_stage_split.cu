@@ -42,8 +42,8 @@ using namespace sd;
 
 // NW: warps per CTA.  8 normally; 2 for tables too small to give every SM two
 // 256-thread CTAs (the 32^3 block: 183 CTAs of 256 would leave a fifth of the
-// SMs with twice the work), with the same register caps (OCC counts
-// 256-thread CTAs).
+// SMs with twice the work), whose flux and assembly work runs in
+// k_split_fluxes_roles and k_split_assemble_kmem over the same 64-cell ranges.
 template <typename T, int NW = 8>
 __global__ void __launch_bounds__(32 * NW) k_split_prims(const Table tab, const double gm1, const double R,
                                                          const double iR, const double p_ref) {
@@ -56,14 +56,14 @@ __global__ void __launch_bounds__(32 * NW) k_split_prims(const Table tab, const 
   prims_cell<T>(B, c, gm1, R, iR, p_ref);
 }
 
-template <typename T, bool K_AOS, int OCC = SplitOcc<T>::fluxes, int NW = 8>
-__global__ void __launch_bounds__(32 * NW, OCC * 8 / NW) k_split_fluxes(const Table tab, const Phys ph,
-                                                                         const int flags) {
+template <typename T, bool K_AOS, int OCC = SplitOcc<T>::fluxes>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_fluxes(const Table tab, const Phys ph,
+                                                                     const int flags) {
   const int b = find_block(tab, blockIdx.x);
-  if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x, 32 * NW);
+  if (threadIdx.x == 0) prefetch_fluxes<T, K_AOS, false>(tab.b[b], blockIdx.x);
   grid_dep_wait();
   Cell x;
-  if (!decode(tab.b[b], blockIdx.x, x, 32 * NW)) return;
+  if (!decode(tab.b[b], blockIdx.x, x)) return;
   flux_cell<T, K_AOS, true>(tab.b[b].blk, tab.b[b].blk.prim, x, ph, flags);
 }
 
@@ -110,17 +110,17 @@ __global__ void __launch_bounds__(64, 8) k_split_assemble_kmem(const Table tab, 
                            gm1, R, iR, ph);
 }
 
-template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble, int NW = 8>
-__global__ void __launch_bounds__(32 * NW, OCC * 8 / NW) k_split_assemble(const Table tab, const int flags,
-                                                                           const int stage, const int next_prims,
-                                                                           const double gm1, const double R,
-                                                                           const double iR, const Phys ph) {
+template <typename T, bool K_AOS, int OCC = SplitOcc<T>::assemble>
+__global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Table tab, const int flags,
+                                                                       const int stage, const int next_prims,
+                                                                       const double gm1, const double R,
+                                                                       const double iR, const Phys ph) {
   const int b = find_block_asm(tab, blockIdx.x);
   const Dev& d = tab.b[b];
   const SplitBlock& B = d.blk;
-  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, 31 * NW, B.cta_begin_asm);
+  if (threadIdx.x == 0) prefetch_assembly<T, K_AOS, false>(d, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
   grid_dep_wait();
-  asm_chunk<T, K_AOS, true>(d, TablePtrs{B}, (int64_t)(blockIdx.x - B.cta_begin_asm) * (31 * NW), flags, stage,
+  asm_chunk<T, K_AOS, true>(d, TablePtrs{B}, (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells, flags, stage,
                             next_prims, gm1, R, iR, ph);
 }
 
@@ -530,13 +530,13 @@ void launch_pair64(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int
              ph.R, 1.0 / ph.R, ph);
 }
 
-template <typename T, bool K_AOS, int V, int NW = 8>
+template <typename T, bool K_AOS, int V>
 void launch_pair(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int flags, int stage, int np,
                  cudaStream_t st, cudaEvent_t after_fluxes) {
   constexpr SplitShape sh = kSplitVariants[V];
-  pdl_launch(k_split_fluxes<T, K_AOS, sh.flux_occ, NW>, ctas, 32 * NW, 0, st, tab, ph, flags);
+  pdl_launch(k_split_fluxes<T, K_AOS, sh.flux_occ>, ctas, kSplitThreads, 0, st, tab, ph, flags);
   if (after_fluxes) cudaEventRecord(after_fluxes, st);
-  pdl_launch(k_split_assemble<T, K_AOS, sh.asm_occ, NW>, asm_ctas, 32 * NW, 0, st, tab, flags, stage, np, ph.gm1,
+  pdl_launch(k_split_assemble<T, K_AOS, sh.asm_occ>, asm_ctas, kSplitThreads, 0, st, tab, flags, stage, np, ph.gm1,
              ph.R, 1.0 / ph.R, ph);
 }
 
