@@ -131,15 +131,15 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_split_assemble(const Tab
 // lane) and padding bytes than the index arithmetic they save.
 namespace fm {
 
-template <typename T>
-__global__ void __launch_bounds__(kSplitThreads) k_fm_prims(const Table tab, const double gm1,
+template <typename T, int NW = 8>
+__global__ void __launch_bounds__(32 * NW) k_fm_prims(const Table tab, const double gm1,
                                                               const double R, const double iR) {
   const int b = find_block(tab, blockIdx.x);
-  if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x);
+  if (threadIdx.x == 0) prefetch_state(tab.b[b], blockIdx.x, 32 * NW);
   grid_dep_wait();
   const SplitBlock& B = tab.b[b].blk;
   const int64_t N = (int64_t)B.ni * B.nj * B.nk;
-  const int64_t c = (int64_t)(blockIdx.x - B.cta_begin) * kSplitThreads + threadIdx.x;
+  const int64_t c = (int64_t)(blockIdx.x - B.cta_begin) * (32 * NW) + threadIdx.x;
   if (c >= N) return;
   const double* q = B.q;
   const double r = q[c];
@@ -286,6 +286,101 @@ __global__ void __launch_bounds__(kSplitThreads, OCC) k_fm_fluxes(const Table ta
   }
 }
 
+// The FP64 flux work of small tables split by warp roles (192-thread CTAs over
+// the 64 cells of one 2-warp CTA: warps 0-1 the i faces, 2-3 the j faces, 4-5
+// the viscous components), the same arithmetic and stores as k_fm_fluxes.
+template <typename T, int AXIS>
+__device__ __forceinline__ void fm_face_role(const SplitBlock& B, const Cell& x, const Phys& ph) {
+  const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
+  const int ia = AXIS == 0 ? x.i : x.j, na = AXIS == 0 ? x.ni : x.nj;
+  if (ia < 1 || ia > na - 3) return;
+  const int32_t sa = AXIS == 0 ? x.nj * x.nk : x.nk;
+  const T* __restrict__ P = (const T*)B.prim;
+  const Cell6<T> a0 = load_cell<T, false>(P, N, c - sa), a1 = load_cell<T, false>(P, N, c),
+                 a2 = load_cell<T, false>(P, N, c + sa), a3 = load_cell<T, false>(P, N, c + 2 * sa);
+  T kc[3], kn[3], Fo[5];
+  metric_row<T>(B, N, AXIS, c, kc);
+  metric_row<T>(B, N, AXIS, c + sa, kn);
+  face_from_cells<T>(a0, a1, a2, a3, kc, kn, ph, Fo);
+  T* __restrict__ F = (T*)B.F;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) F[(5 * AXIS + v) * N + c] = Fo[v];
+}
+
+template <typename T>
+__device__ __forceinline__ void fm_visc_role(const SplitBlock& B, const Cell& x, const Phys& ph) {
+  using M = FastMath<T>;
+  const int32_t N = (int32_t)x.N, c = (int32_t)x.c;
+  const int32_t si = x.nj * x.nk, sj = x.nk;
+  const T* __restrict__ P = (const T*)B.prim;
+  const int32_t ip = x.i + 1 == x.ni ? c - (x.ni - 1) * si : c + si;
+  const int32_t im = x.i == 0 ? c + (x.ni - 1) * si : c - si;
+  const int32_t jp = x.j + 1 == x.nj ? c - (x.nj - 1) * sj : c + sj;
+  const int32_t jm = x.j == 0 ? c + (x.nj - 1) * sj : c - sj;
+  const int32_t kp = x.k + 1 == x.nk ? c - (x.nk - 1) : c + 1;
+  const int32_t km = x.k == 0 ? c + (x.nk - 1) : c - 1;
+  const Cell6<T> C0 = load_cell<T, true>(P, N, c);
+  const Cell6<T> Im = load_cell<T, true>(P, N, im), Ip = load_cell<T, true>(P, N, ip);
+  const Cell6<T> Jm = load_cell<T, true>(P, N, jm), Jp = load_cell<T, true>(P, N, jp);
+  const Cell6<T> Km = load_cell<T, true>(P, N, km), Kp = load_cell<T, true>(P, N, kp);
+  const T h = T(0.5);
+  const T d[4][3] = {{h * (Ip.u - Im.u), h * (Jp.u - Jm.u), h * (Kp.u - Km.u)},
+                     {h * (Ip.v - Im.v), h * (Jp.v - Jm.v), h * (Kp.v - Km.v)},
+                     {h * (Ip.w - Im.w), h * (Jp.w - Jm.w), h * (Kp.w - Km.w)},
+                     {h * (Ip.t - Im.t), h * (Jp.t - Jm.t), h * (Kp.t - Km.t)}};
+  T kk[9];
+  metric_row<T>(B, N, 0, c, kk);
+  metric_row<T>(B, N, 1, c, kk + 3);
+  metric_row<T>(B, N, 2, c, kk + 6);
+  T g[4][3];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) g[s][m] = d[s][0] * kk[m] + d[s][1] * kk[3 + m] + d[s][2] * kk[6 + m];
+  T mu = (T)B.mu0;
+  if (ph.visc_law == 0) {  // Sutherland (physics/eos.py:24-25)
+    const T r = C0.t * (T)ph.inv_T0;
+    mu = (T)B.mu0 * (r * M::sqrt_pos(r)) * (T)ph.sfac * M::rcp(C0.t + (T)ph.Ts);
+  }
+  const T kappa = (T)ph.kap_fac * mu;
+  const T third = (T)(1.0 / 3.0);
+  const T div_u = g[0][0] + g[1][1] + g[2][2];
+  const T t00 = T(2) * mu * (g[0][0] - div_u * third);
+  const T t01 = mu * (g[0][1] + g[1][0]);
+  const T t02 = mu * (g[0][2] + g[2][0]);
+  const T t11 = T(2) * mu * (g[1][1] - div_u * third);
+  const T t12 = mu * (g[1][2] + g[2][1]);
+  const T t22 = T(2) * mu * (g[2][2] - div_u * third);
+  T* __restrict__ G = (T*)B.G;
+  G[c] = t00;
+  G[N + c] = t01;
+  G[2 * N + c] = t02;
+  G[3 * N + c] = t11;
+  G[4 * N + c] = t12;
+  G[5 * N + c] = t22;
+  G[6 * N + c] = C0.u * t00 + C0.v * t01 + C0.w * t02 + kappa * g[3][0];
+  G[7 * N + c] = C0.u * t01 + C0.v * t11 + C0.w * t12 + kappa * g[3][1];
+  G[8 * N + c] = C0.u * t02 + C0.v * t12 + C0.w * t22 + kappa * g[3][2];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(192, 2) k_fm_fluxes_roles(const Table tab, const Phys ph, const int flags) {
+  const int b = find_block(tab, blockIdx.x);
+  if (threadIdx.x == 0) prefetch_fluxes<T, false, true>(tab.b[b], blockIdx.x, 64);
+  grid_dep_wait();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const SplitBlock& B = tab.b[b].blk;
+  Cell x;
+  if (!decode_cell(tab.b[b], (int64_t)(blockIdx.x - B.cta_begin) * 64 + (warp & 1) * 32 + lane, x)) return;
+  if (warp < 2) {
+    if (flags & kRhsInvscd) fm_face_role<T, 0>(B, x, ph);
+  } else if (warp < 4) {
+    if (flags & kRhsInvscd) fm_face_role<T, 1>(B, x, ph);
+  } else if (flags & kRhsViscous) {
+    fm_visc_role<T>(B, x, ph);
+  }
+}
+
 // The k face c-1 | c (rhs/invscd.py:62-100) of the FP64 path from the
 // primitive records of c-2 .. c+1 and the k rows of kxyz at c-1 and c.
 template <typename T>
@@ -303,20 +398,22 @@ __device__ __forceinline__ void fm_k_face_left(const SplitBlock& B, int32_t N, i
 // left of its cell and takes the one on its right from lane l+1 by shuffle
 // (lane 31's cell is the next warp's first, for which it only supplies the
 // face), as in the FP32 assembly.
-template <typename T, int OCC = 3>
-__global__ void __launch_bounds__(kSplitThreads, OCC) k_fm_assemble(const Table tab, const int flags,
+// NW: warps per CTA (8; 2 for the small tables of launch_tab, with a looser
+// register cap since such a table puts few CTAs on an SM).
+template <typename T, int OCC = 3, int NW = 8>
+__global__ void __launch_bounds__(32 * NW, NW == 8 ? OCC : 8) k_fm_assemble(const Table tab, const int flags,
                                                                  const int stage, const int next_prims,
                                                                  const double gm1, const double R,
                                                                  const double iR, const Phys ph) {
   const int b = find_block_asm(tab, blockIdx.x);
   const Dev& dv = tab.b[b];
   const SplitBlock& B = dv.blk;
-  if (threadIdx.x == 0) prefetch_assembly<T, false, true>(dv, blockIdx.x, flags, stage, kAsmCells, B.cta_begin_asm);
+  if (threadIdx.x == 0) prefetch_assembly<T, false, true>(dv, blockIdx.x, flags, stage, 31 * NW, B.cta_begin_asm);
   grid_dep_wait();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Cell x;
   x.N = (int64_t)B.ni * B.nj * B.nk;
-  x.c = (int64_t)(blockIdx.x - B.cta_begin_asm) * kAsmCells + warp * 31 + lane;
+  x.c = (int64_t)(blockIdx.x - B.cta_begin_asm) * (31 * NW) + warp * 31 + lane;
   const bool alive = x.c < x.N;
   if (alive) {
     const uint32_t t1 = dv.dk.div((uint32_t)x.c);
@@ -556,6 +653,14 @@ int launch_tab(const Table& tab, int ctas, int asm_ctas, const Phys& ph, int fla
     }
   }
   if constexpr (sizeof(T) == 8) {
+    if (nw == 2) {  // a small table: the role-split flux kernel and 2-warp CTAs
+      if (!prims_ready) pdl_launch(fm::k_fm_prims<double, 2>, ctas, 64, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R);
+      pdl_launch(fm::k_fm_fluxes_roles<double>, ctas, 192, 0, st, tab, ph, flags);
+      if (after_fluxes) cudaEventRecord(after_fluxes, st);
+      pdl_launch(fm::k_fm_assemble<double, 3, 2>, asm_ctas, 64, 0, st, tab, flags, stage, np, ph.gm1, ph.R,
+                 1.0 / ph.R, ph);
+      return prims_ready ? 2 : 3;
+    }
     if (!prims_ready) pdl_launch(fm::k_fm_prims<double>, ctas, kSplitThreads, 0, st, tab, ph.gm1, ph.R, 1.0 / ph.R);
     switch (variant) {
       case 1: launch_pair64<1>(tab, ctas, asm_ctas, ph, flags, stage, np, st, after_fluxes); break;
@@ -590,9 +695,9 @@ int launch_split(fj_ctx* ctx, const SplitBlock* blocks, int nblocks, const Phys&
   for (int base = 0; base < nblocks; base += kMaxSplitBlocks) {
     Table tab;
     tab.n = std::min(kMaxSplitBlocks, nblocks - base);
-    // FP32 tables with fewer 256-thread flux CTAs than two per SM run 2-warp CTAs
+    // tables with fewer 256-thread flux CTAs than two per SM run 2-warp CTAs
     int nw = 8;
-    if (sizeof(T) == 4) {
+    {
       int64_t wide = 0;
       for (int t = 0; t < tab.n; ++t) {
         const SplitBlock& sb = blocks[base + t];
